@@ -1,0 +1,144 @@
+/*
+ * magma_b200.h -- public C interface of libmagma_b200.
+ *
+ * libmagma_b200 is a B200 (sm_100a) implementation of MAGMA's batched
+ * small-matrix dense path. Each entry point below keeps the name, argument
+ * order, argument meaning and error behaviour of the MAGMA 2.2 routine it
+ * replaces (cited per declaration as reference file:line), so a caller that
+ * was built against MAGMA relinks against this library unchanged.
+ *
+ * Conventions shared by every batched routine (as in MAGMA):
+ *   - all arrays (pointer arrays, size arrays, ipiv, info, matrices) are
+ *     DEVICE memory owned by the caller; matrices are column-major;
+ *   - ipiv entries are 1-based row indices in LAPACK's swap-sequence form;
+ *   - a negative return value -i means argument i was illegal (reported
+ *     through magma_xerbla); numerical failures are reported per instance in
+ *     info_array (>0: 1-based index of the first zero pivot / non-positive
+ *     leading minor);
+ *   - work is enqueued on the queue's CUDA stream. Unlike the reference these
+ *     routines do not synchronize before returning (no cudaMalloc, no host
+ *     round trip on the call path), so results are visible after
+ *     magma_queue_sync(queue), exactly as after the reference's own return.
+ *   - vbatched size arrays have batchCount+1 entries; the last one is scratch
+ *     (magmablas/zgemm_vbatched.cpp:146-149).
+ */
+#ifndef MAGMA_B200_H
+#define MAGMA_B200_H
+
+#include "magma_b200_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------
+ * Runtime (reference: interface_cuda/interface.cpp, interface_cuda/alloc.cpp,
+ * interface_cuda/copy_v2.cpp, control/xerbla.cpp)
+ * ---------------------------------------------------------------------- */
+
+/* interface_cuda/interface.cpp:168 */
+magma_int_t magma_init(void);
+/* interface_cuda/interface.cpp:246 */
+magma_int_t magma_finalize(void);
+/* interface_cuda/error.cpp:112 */
+const char* magma_strerror(magma_int_t error);
+/* control/xerbla.cpp:51 */
+void magma_xerbla(const char* srname, magma_int_t neg_info);
+
+/* interface_cuda/interface.cpp:546 (magma_getdevice), :567 (magma_setdevice) */
+void magma_getdevice(magma_device_t* dev);
+void magma_setdevice(magma_device_t dev);
+
+/* interface_cuda/alloc.cpp:60 (magma_malloc), :93 (magma_free_internal) */
+magma_int_t magma_malloc(magma_ptr* ptr_ptr, size_t bytes);
+magma_int_t magma_free_internal(magma_ptr ptr, const char* func, const char* file, int line);
+#define magma_free(ptr) magma_free_internal(ptr, __func__, __FILE__, __LINE__)
+
+/* include/magma_auxiliary.h:248-281 (queue support; the public names are
+ * macros over the *_internal symbols, exactly as in MAGMA). */
+void magma_queue_create_internal(magma_device_t device, magma_queue_t* queue_ptr,
+                                 const char* func, const char* file, int line);
+void magma_queue_create_from_cuda_internal(magma_device_t device, cudaStream_t stream,
+                                           cublasHandle_t cublas, cusparseHandle_t cusparse,
+                                           magma_queue_t* queue_ptr,
+                                           const char* func, const char* file, int line);
+void magma_queue_destroy_internal(magma_queue_t queue, const char* func, const char* file, int line);
+void magma_queue_sync_internal(magma_queue_t queue, const char* func, const char* file, int line);
+magma_int_t  magma_queue_get_device(magma_queue_t queue);
+cudaStream_t magma_queue_get_cuda_stream(magma_queue_t queue);
+
+/* No reference counterpart (MAGMA allocates workspace inside every call,
+ * src/zgetrf_batched.cpp:148-170). Reserves at least `bytes` of the queue's
+ * grow-only device workspace now, so that later calls never allocate -- call
+ * it before capturing batched calls into a CUDA graph. */
+magma_int_t  magma_queue_reserve_workspace(magma_queue_t queue, size_t bytes);
+
+#define magma_queue_create(device, queue_ptr) \
+        magma_queue_create_internal(device, queue_ptr, __func__, __FILE__, __LINE__)
+#define magma_queue_create_from_cuda(device, stream, cublas, cusparse, queue_ptr) \
+        magma_queue_create_from_cuda_internal(device, stream, cublas, cusparse, queue_ptr, __func__, __FILE__, __LINE__)
+#define magma_queue_destroy(queue) magma_queue_destroy_internal(queue, __func__, __FILE__, __LINE__)
+#define magma_queue_sync(queue)    magma_queue_sync_internal(queue, __func__, __FILE__, __LINE__)
+
+/* include/magma_copy.h:45-84 (setvector / getvector, sync and async) */
+void magma_setvector_internal(magma_int_t n, magma_int_t elemSize, const void* hx_src, magma_int_t incx,
+                              magma_ptr dy_dst, magma_int_t incy, magma_queue_t queue,
+                              const char* func, const char* file, int line);
+void magma_getvector_internal(magma_int_t n, magma_int_t elemSize, const void* dx_src, magma_int_t incx,
+                              void* hy_dst, magma_int_t incy, magma_queue_t queue,
+                              const char* func, const char* file, int line);
+void magma_setvector_async_internal(magma_int_t n, magma_int_t elemSize, const void* hx_src, magma_int_t incx,
+                                    magma_ptr dy_dst, magma_int_t incy, magma_queue_t queue,
+                                    const char* func, const char* file, int line);
+void magma_getvector_async_internal(magma_int_t n, magma_int_t elemSize, const void* dx_src, magma_int_t incx,
+                                    void* hy_dst, magma_int_t incy, magma_queue_t queue,
+                                    const char* func, const char* file, int line);
+#define magma_setvector(n, es, hx, incx, dy, incy, queue) \
+        magma_setvector_internal(n, es, hx, incx, dy, incy, queue, __func__, __FILE__, __LINE__)
+#define magma_getvector(n, es, dx, incx, hy, incy, queue) \
+        magma_getvector_internal(n, es, dx, incx, hy, incy, queue, __func__, __FILE__, __LINE__)
+#define magma_setvector_async(n, es, hx, incx, dy, incy, queue) \
+        magma_setvector_async_internal(n, es, hx, incx, dy, incy, queue, __func__, __FILE__, __LINE__)
+#define magma_getvector_async(n, es, dx, incx, hy, incy, queue) \
+        magma_getvector_async_internal(n, es, dx, incx, hy, incy, queue, __func__, __FILE__, __LINE__)
+
+/* Pointer-array builders: output_array[i] = input + (batch_offset*i) + row + column*lda.
+ * magmablas/zset_pointer.cu:17-26 (kernel), :87 (magma_zset_pointer);
+ * magmablas/set_pointer.cu:72 (magma_iset_pointer). One launch, no host round trip. */
+void magma_dset_pointer(double** output_array, double* input, magma_int_t lda,
+                        magma_int_t row, magma_int_t column, magma_int_t batch_offset,
+                        magma_int_t batchCount, magma_queue_t queue);
+void magma_sset_pointer(float** output_array, float* input, magma_int_t lda,
+                        magma_int_t row, magma_int_t column, magma_int_t batch_offset,
+                        magma_int_t batchCount, magma_queue_t queue);
+void magma_iset_pointer(magma_int_t** output_array, magma_int_t* input, magma_int_t lda,
+                        magma_int_t row, magma_int_t column, magma_int_t batch_offset,
+                        magma_int_t batchCount, magma_queue_t queue);
+
+/* ------------------------------------------------------------------------
+ * Batched LU (fixed size)
+ * ---------------------------------------------------------------------- */
+
+/* P*A = L*U with partial pivoting (ties -> lowest row, as LAPACK idamax).
+ * src/zgetrf_batched.cpp:83-89; arg checks :96-107 (m:-1, n:-2, ldda:-4). */
+magma_int_t magma_dgetrf_batched(magma_int_t m, magma_int_t n, double** dA_array, magma_int_t ldda,
+                                 magma_int_t** ipiv_array, magma_int_t* info_array,
+                                 magma_int_t batchCount, magma_queue_t queue);
+
+/* Solve op(A) X = B with the factors of magma_dgetrf_batched.
+ * src/zgetrs_batched.cpp:87-118 (trans:-1, n:-2, nrhs:-3, ldda:-5, lddb:-8). */
+magma_int_t magma_dgetrs_batched(magma_trans_t trans, magma_int_t n, magma_int_t nrhs,
+                                 double** dA_array, magma_int_t ldda, magma_int_t** dipiv_array,
+                                 double** dB_array, magma_int_t lddb,
+                                 magma_int_t batchCount, magma_queue_t queue);
+
+/* getrf + getrs. src/zgesv_batched.cpp:93-147 (n:-1, nrhs:-2, ldda:-4, lddb:-6). */
+magma_int_t magma_dgesv_batched(magma_int_t n, magma_int_t nrhs, double** dA_array, magma_int_t ldda,
+                                magma_int_t** dipiv_array, double** dB_array, magma_int_t lddb,
+                                magma_int_t* dinfo_array, magma_int_t batchCount, magma_queue_t queue);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MAGMA_B200_H */

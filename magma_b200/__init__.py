@@ -1,0 +1,20 @@
+"""magma_b200 -- B200-native batched small-matrix dense solvers behind MAGMA's C API.
+
+The product is the shared library ``libmagma_b200.so`` (C ABI in
+``include/magma_b200.h``). This package holds its CUDA/C++ sources
+(``csrc/``), the in-tree build (``build.py``), a ctypes binding (``_lib.py``)
+and thin torch-facing helpers used by the tests, the benchmark and the
+request loop. The helpers only marshal device pointers; every computation
+runs in the library's kernels.
+"""
+from __future__ import annotations
+
+from . import _lib
+from .api import (Queue, ptr_array, dgetrf_batched, dgetrs_batched, dgesv_batched)
+
+__all__ = ["Queue", "ptr_array", "dgetrf_batched", "dgetrs_batched", "dgesv_batched", "load"]
+
+
+def load():
+    """Load libmagma_b200.so (raises if it has not been built)."""
+    return _lib.load()

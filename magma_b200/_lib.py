@@ -1,0 +1,82 @@
+"""ctypes binding of libmagma_b200.so (the C ABI declared in include/magma_b200.h).
+
+The shared library is built in-tree by ``python -m magma_b200.build``. There is
+no fallback: if the library is missing or fails to load, importing the
+bindings raises, so nothing can silently run on another implementation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libmagma_b200.so"
+
+magma_int_t = C.c_int
+_p = C.c_void_p
+_i = C.c_int
+_d = C.c_double
+_f = C.c_float
+_s = C.c_char_p
+_sz = C.c_size_t
+
+MagmaNoTrans, MagmaTrans, MagmaConjTrans = 111, 112, 113
+MagmaUpper, MagmaLower, MagmaFull = 121, 122, 123
+MagmaNonUnit, MagmaUnit = 131, 132
+MagmaLeft, MagmaRight = 141, 142
+
+MAGMA_SUCCESS = 0
+MAGMA_ERR_NOT_SUPPORTED = -103
+MAGMA_ERR_DEVICE_ALLOC = -113
+
+# name -> (restype, argtypes). Every symbol declared in include/magma_b200.h
+# appears here; tests check the two lists agree.
+SIGNATURES: dict[str, tuple] = {
+    # runtime
+    "magma_init": (_i, []),
+    "magma_finalize": (_i, []),
+    "magma_strerror": (_s, [_i]),
+    "magma_xerbla": (None, [_s, _i]),
+    "magma_getdevice": (None, [C.POINTER(_i)]),
+    "magma_setdevice": (None, [_i]),
+    "magma_malloc": (_i, [C.POINTER(_p), _sz]),
+    "magma_free_internal": (_i, [_p, _s, _s, _i]),
+    "magma_queue_create_internal": (None, [_i, C.POINTER(_p), _s, _s, _i]),
+    "magma_queue_create_from_cuda_internal": (None, [_i, _p, _p, _p, C.POINTER(_p), _s, _s, _i]),
+    "magma_queue_destroy_internal": (None, [_p, _s, _s, _i]),
+    "magma_queue_sync_internal": (None, [_p, _s, _s, _i]),
+    "magma_queue_get_device": (_i, [_p]),
+    "magma_queue_get_cuda_stream": (_p, [_p]),
+    "magma_queue_reserve_workspace": (_i, [_p, _sz]),
+    "magma_setvector_internal": (None, [_i, _i, _p, _i, _p, _i, _p, _s, _s, _i]),
+    "magma_getvector_internal": (None, [_i, _i, _p, _i, _p, _i, _p, _s, _s, _i]),
+    "magma_setvector_async_internal": (None, [_i, _i, _p, _i, _p, _i, _p, _s, _s, _i]),
+    "magma_getvector_async_internal": (None, [_i, _i, _p, _i, _p, _i, _p, _s, _s, _i]),
+    "magma_dset_pointer": (None, [_p, _p, _i, _i, _i, _i, _i, _p]),
+    "magma_sset_pointer": (None, [_p, _p, _i, _i, _i, _i, _i, _p]),
+    "magma_iset_pointer": (None, [_p, _p, _i, _i, _i, _i, _i, _p]),
+    # batched LU
+    "magma_dgetrf_batched": (_i, [_i, _i, _p, _i, _p, _p, _i, _p]),
+    "magma_dgetrs_batched": (_i, [_i, _i, _i, _p, _i, _p, _p, _i, _i, _p]),
+    "magma_dgesv_batched": (_i, [_i, _i, _p, _i, _p, _p, _i, _p, _i, _p]),
+}
+
+_lib: C.CDLL | None = None
+
+
+def load() -> C.CDLL:
+    """Load the library once and attach the signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build it with `python -m magma_b200.build` "
+            "(there is no CPU or library fallback)")
+    lib = C.CDLL(str(LIB_PATH), mode=os.RTLD_NOW | C.RTLD_GLOBAL)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib

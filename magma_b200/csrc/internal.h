@@ -1,0 +1,47 @@
+// internal.h -- private runtime state shared by the host side of libmagma_b200.
+//
+// The queue mirrors the role of MAGMA's struct magma_queue
+// (control/magma_internal.h:86-139): a device id plus the CUDA stream all work
+// is enqueued on. Unlike the reference it also owns a grow-only device
+// workspace, so batched routines never call cudaMalloc on their call path
+// (the reference mallocs and frees ~20 buffers per call,
+// src/zgetrf_batched.cpp:148-194 and :356-376).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdio>
+#include "../../include/magma_b200.h"
+
+struct magma_queue {
+    int          device;
+    cudaStream_t stream;
+    bool         own_stream;
+    // grow-only workspace owned by the queue
+    void*        ws;
+    size_t       ws_bytes;
+    // host-pinned staging word used by routines that must read one value back
+    int*         h_flag;
+};
+
+namespace mb200 {
+
+// Returns a device workspace of at least `bytes` on `queue`, growing it when
+// needed. Growing synchronises the queue's stream (the old buffer may still be
+// in use by enqueued work) -- callers that capture CUDA graphs reserve the
+// workspace once before capture with magma_queue_reserve_workspace().
+void* queue_workspace(magma_queue_t queue, size_t bytes);
+
+// Records a CUDA launch error as a MAGMA error code (0 when none).
+inline magma_int_t launch_status() {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        std::fprintf(stderr, "libmagma_b200: CUDA launch failed: %s\n", cudaGetErrorString(e));
+        return MAGMA_ERR_UNKNOWN;
+    }
+    return MAGMA_SUCCESS;
+}
+
+inline int ceildiv(long a, long b) { return (int)((a + b - 1) / b); }
+
+}  // namespace mb200

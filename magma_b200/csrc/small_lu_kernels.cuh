@@ -1,0 +1,262 @@
+// small_lu_kernels.cuh -- kernels of the batched LU factorisation, solve and fused gesv for
+// matrices up to 128 rows x 64 columns, fixed or variable size per instance.
+//
+// Replaces, for these sizes, the reference's getf2 pipeline
+// (src/zgetf2_batched.cpp:98-194: per column an argmax kernel, a swap kernel
+// and a scale/update kernel; then laswp, trsm and gemm launches) and its
+// trsv-based getrs (src/zgetrs_batched.cpp:87-273) by ONE launch each: the
+// matrix is read from HBM once, factored in registers (small_lu.cuh), and
+// written once.
+#include "internal.h"
+#include "small_lu.cuh"
+
+#pragma once
+namespace mb200 {
+
+// Per-instance size lookup: fixed sizes when the array pointer is null.
+struct LuSizes {
+    int m, n, lda, ldb, nrhs;
+    const int* m_arr;
+    const int* n_arr;
+    const int* lda_arr;
+    const int* ldb_arr;
+    const int* nrhs_arr;
+    __device__ __forceinline__ int get_m(int i) const { return m_arr ? m_arr[i] : m; }
+    __device__ __forceinline__ int get_n(int i) const { return n_arr ? n_arr[i] : n; }
+    __device__ __forceinline__ int get_lda(int i) const { return lda_arr ? lda_arr[i] : lda; }
+    __device__ __forceinline__ int get_ldb(int i) const { return ldb_arr ? ldb_arr[i] : ldb; }
+    __device__ __forceinline__ int get_nrhs(int i) const { return nrhs_arr ? nrhs_arr[i] : nrhs; }
+};
+
+// MPB matrices per block when NW == 1 (one warp each); one matrix per block otherwise.
+template <int NW> struct BlockShape { static constexpr int MPB = (NW == 1) ? 4 : 1; };
+
+template <typename T, int NC, int NW>
+__device__ __forceinline__ void load_rows(T (&a)[NC], const T* __restrict__ A, int m, int n, int lda, int tid) {
+#pragma unroll
+    for (int j = 0; j < NC; ++j) a[j] = (tid < m && j < n) ? A[tid + (size_t)j * lda] : T(0);
+}
+
+template <typename T, int NC>
+__device__ __forceinline__ void store_rows(const T (&a)[NC], T* __restrict__ A, int m, int n, int lda, int tid, int pos) {
+    if (tid < m) {
+#pragma unroll
+        for (int j = 0; j < NC; ++j)
+            if (j < n) A[pos + (size_t)j * lda] = a[j];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// getrf
+template <typename T, int NC, int NW>
+__global__ void __launch_bounds__(32 * NW * BlockShape<NW>::MPB)
+getrf_small_kernel(LuSizes sz, T** dA_array, int** ipiv_array, int* info_array, int batch) {
+    constexpr int MPB = BlockShape<NW>::MPB;
+    __shared__ SmallLuShared<T, NC, NW> shm[MPB];
+    const int local = (NW == 1) ? (threadIdx.x >> 5) : 0;
+    const int tid = (NW == 1) ? (threadIdx.x & 31) : threadIdx.x;
+    const int id = blockIdx.x * MPB + local;
+    if (id >= batch) return;   // NW==1: whole warp leaves together; NW>1: whole block
+    const int m = sz.get_m(id), n = sz.get_n(id), lda = sz.get_lda(id);
+    if (m <= 0 || n <= 0) {
+        if (tid == 0) info_array[id] = 0;
+        return;
+    }
+    T* A = dA_array[id];
+    T a[NC];
+    load_rows<T, NC, NW>(a, A, m, n, lda, tid);
+    int pos, my_ipiv, info;
+    small_lu_factor<T, NC, NW>(a, m, n, tid, pos, my_ipiv, info, shm[local]);
+    store_rows<T, NC>(a, A, m, n, lda, tid, pos);
+    if (tid < min(m, n)) ipiv_array[id][tid] = my_ipiv;
+    if (tid == 0) info_array[id] = info;
+}
+
+// ---------------------------------------------------------------------------
+// gesv: getrf + getrs(NoTrans) in one pass. R = RHS columns solved together.
+template <typename T, int NC, int NW, int R>
+__global__ void __launch_bounds__(32 * NW * BlockShape<NW>::MPB)
+gesv_small_kernel(LuSizes sz, T** dA_array, int** ipiv_array, T** dB_array, int* info_array, int batch) {
+    constexpr int MPB = BlockShape<NW>::MPB;
+    __shared__ SmallLuShared<T, NC, NW> shm[MPB];
+    const int local = (NW == 1) ? (threadIdx.x >> 5) : 0;
+    const int tid = (NW == 1) ? (threadIdx.x & 31) : threadIdx.x;
+    const int id = blockIdx.x * MPB + local;
+    if (id >= batch) return;
+    const int n = sz.get_n(id), lda = sz.get_lda(id), ldb = sz.get_ldb(id), nrhs = sz.get_nrhs(id);
+    if (n <= 0) {
+        if (tid == 0) info_array[id] = 0;
+        return;
+    }
+    T* A = dA_array[id];
+    T* B = dB_array[id];
+    T a[NC];
+    load_rows<T, NC, NW>(a, A, n, n, lda, tid);
+    // Prefetch the first RHS chunk before factoring so its latency overlaps.
+    T b[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) b[r] = (tid < n && r < nrhs) ? B[tid + (size_t)r * ldb] : T(0);
+    int pos, my_ipiv, info;
+    small_lu_factor<T, NC, NW>(a, n, n, tid, pos, my_ipiv, info, shm[local]);
+    store_rows<T, NC>(a, A, n, n, lda, tid, pos);
+    if (tid < n) ipiv_array[id][tid] = my_ipiv;
+    if (tid == 0) info_array[id] = info;
+    // Thread tid's b entry (original row tid) belongs at position `pos` of P*b,
+    // the same position its LU row landed at, so no permutation pass is needed.
+    for (int c0 = 0; c0 < nrhs; c0 += R) {
+        if (c0 > 0) {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                b[r] = (tid < n && c0 + r < nrhs) ? B[tid + (size_t)(c0 + r) * ldb] : T(0);
+        }
+        small_lu_solve<T, NC, NW, R>(a, n, pos, b, shm[local]);
+        if (tid < n) {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                if (c0 + r < nrhs) B[pos + (size_t)(c0 + r) * ldb] = b[r];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// getrs, NoTrans. Thread tid loads LU row tid (already in final position) and
+// moves b to P*b by replaying the ipiv swap sequence on indices.
+template <typename T, int NC, int NW, int R>
+__device__ __forceinline__ void permute_rhs(T (&b)[R], const int* ipiv, int n, int tid,
+                                            SmallLuShared<T, NC, NW>& sh, T* xch, bool inverse) {
+    // idx = where the entry of original row tid sits after LAPACK's DLASWP
+    // (forward: k ascending; inverse: k descending).
+    int idx = tid;
+    if (!inverse) {
+        for (int k = 0; k < n; ++k) {
+            int p = ipiv[k] - 1;
+            if (idx == k) idx = p; else if (idx == p) idx = k;
+        }
+    } else {
+        for (int k = n - 1; k >= 0; --k) {
+            int p = ipiv[k] - 1;
+            if (idx == k) idx = p; else if (idx == p) idx = k;
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        if (tid < n) xch[idx] = b[r];
+        mat_sync<NW>();
+        if (tid < n) b[r] = xch[tid];
+        mat_sync<NW>();
+    }
+}
+
+template <typename T, int NC, int NW, int R>
+__global__ void __launch_bounds__(32 * NW * BlockShape<NW>::MPB)
+getrs_small_kernel(LuSizes sz, bool trans, T** dA_array, int** ipiv_array, T** dB_array, int batch) {
+    constexpr int MPB = BlockShape<NW>::MPB;
+    __shared__ SmallLuShared<T, NC, NW> shm[MPB];
+    __shared__ T xch[MPB][32 * NW];
+    const int local = (NW == 1) ? (threadIdx.x >> 5) : 0;
+    const int tid = (NW == 1) ? (threadIdx.x & 31) : threadIdx.x;
+    const int id = blockIdx.x * MPB + local;
+    if (id >= batch) return;
+    const int n = sz.get_n(id), lda = sz.get_lda(id), ldb = sz.get_ldb(id), nrhs = sz.get_nrhs(id);
+    if (n <= 0 || nrhs <= 0) return;
+    const T* A = dA_array[id];
+    T* B = dB_array[id];
+    const int* ipiv = ipiv_array[id];
+    T a[NC];
+    load_rows<T, NC, NW>(a, A, n, n, lda, tid);
+    SmallLuShared<T, NC, NW>& sh = shm[local];
+    const int pos = (tid < n) ? tid : INT_MAX / 2;
+    for (int c0 = 0; c0 < nrhs; c0 += R) {
+        T b[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) b[r] = (tid < n && c0 + r < nrhs) ? B[tid + (size_t)(c0 + r) * ldb] : T(0);
+        if (!trans) {
+            permute_rhs<T, NC, NW, R>(b, ipiv, n, tid, sh, xch[local], false);
+            small_lu_solve<T, NC, NW, R>(a, n, pos, b, sh);
+        } else {
+            // A^T x = b:  U^T y = b (forward, non-unit), L^T z = y (backward, unit),
+            // x = P^T z. Row k of U / L is published through shared memory.
+            static_for<0, NC>([&](auto kc) {
+                constexpr int k = decltype(kc)::value;
+                if (k >= n) return;
+                constexpr int buf = k & 1;
+                if (tid == k) {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) { b[r] = b[r] / a[k]; sh.rhs[buf][r] = b[r]; }
+#pragma unroll
+                    for (int j = k + 1; j < NC; ++j) sh.row[buf][j] = a[j];
+                }
+                mat_sync<NW>();
+                if (tid > k && tid < n) {
+                    const T u = sh.row[buf][tid];   // U(k, tid)
+#pragma unroll
+                    for (int r = 0; r < R; ++r) b[r] = fma_rn(-u, sh.rhs[buf][r], b[r]);
+                }
+            });
+            static_for<0, NC>([&](auto ic) {
+                constexpr int kk = NC - 1 - decltype(ic)::value;
+                if (kk >= n) return;
+                constexpr int buf = (kk + 1) & 1;
+                if (tid == kk) {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) sh.rhs[buf][r] = b[r];
+#pragma unroll
+                    for (int j = 0; j < kk; ++j) sh.row[buf][j] = a[j];
+                }
+                mat_sync<NW>();
+                if (tid < kk) {
+                    const T l = sh.row[buf][tid];   // L(kk, tid)
+#pragma unroll
+                    for (int r = 0; r < R; ++r) b[r] = fma_rn(-l, sh.rhs[buf][r], b[r]);
+                }
+            });
+            permute_rhs<T, NC, NW, R>(b, ipiv, n, tid, sh, xch[local], true);
+        }
+        if (tid < n) {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                if (c0 + r < nrhs) B[pos + (size_t)(c0 + r) * ldb] = b[r];
+        }
+        mat_sync<NW>();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Launchers, explicitly instantiated per (NC, NW) in small_lu_inst_*.cu so the
+// variants compile in parallel.
+template <typename T, int NC, int NW>
+void launch_getrf(const LuSizes& sz, T** A, int** ipiv, int* info, int batch, cudaStream_t s) {
+    constexpr int MPB = BlockShape<NW>::MPB;
+    getrf_small_kernel<T, NC, NW><<<ceildiv(batch, MPB), 32 * NW * MPB, 0, s>>>(sz, A, ipiv, info, batch);
+}
+
+template <typename T, int NC, int NW>
+void launch_gesv(const LuSizes& sz, int max_nrhs, T** A, int** ipiv, T** B, int* info, int batch, cudaStream_t s) {
+    constexpr int MPB = BlockShape<NW>::MPB;
+    if (max_nrhs <= 1)
+        gesv_small_kernel<T, NC, NW, 1><<<ceildiv(batch, MPB), 32 * NW * MPB, 0, s>>>(sz, A, ipiv, B, info, batch);
+    else
+        gesv_small_kernel<T, NC, NW, 4><<<ceildiv(batch, MPB), 32 * NW * MPB, 0, s>>>(sz, A, ipiv, B, info, batch);
+}
+
+template <typename T, int NC, int NW>
+void launch_getrs(const LuSizes& sz, bool trans, int max_nrhs, T** A, int** ipiv, T** B, int batch, cudaStream_t s) {
+    constexpr int MPB = BlockShape<NW>::MPB;
+    if (max_nrhs <= 1)
+        getrs_small_kernel<T, NC, NW, 1><<<ceildiv(batch, MPB), 32 * NW * MPB, 0, s>>>(sz, trans, A, ipiv, B, batch);
+    else
+        getrs_small_kernel<T, NC, NW, 4><<<ceildiv(batch, MPB), 32 * NW * MPB, 0, s>>>(sz, trans, A, ipiv, B, batch);
+}
+
+
+#define MB200_INSTANTIATE_SMALL(T, NC, NW)                                                   \
+    template void launch_getrf<T, NC, NW>(const LuSizes&, T**, int**, int*, int, cudaStream_t); \
+    template void launch_gesv<T, NC, NW>(const LuSizes&, int, T**, int**, T**, int*, int, cudaStream_t); \
+    template void launch_getrs<T, NC, NW>(const LuSizes&, bool, int, T**, int**, T**, int, cudaStream_t);
+
+}  // namespace mb200
+
+// Every (type, column bound, warps per matrix) the dispatcher may select.
+#define MB200_SMALL_VARIANTS(X) \
+    X(double, 8, 1) X(double, 16, 1) X(double, 32, 1) X(double, 64, 1) \
+    X(double, 32, 2) X(double, 64, 2) X(double, 32, 4) X(double, 64, 4)

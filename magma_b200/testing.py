@@ -1,0 +1,145 @@
+"""Seeded input generators and error metrics for the batched solvers.
+
+Inputs come from a project-owned counter-based PRNG (splitmix64 of
+seed + (i+1)*golden), so any element of any stream can be regenerated on any
+machine. Generators produce the synthetic workloads used by the tests and the
+benchmark, with the shapes and value distributions of the reference's
+testers (testing/magma_zgenerate.cpp, testing/testing_z*_batched.cpp):
+
+* ``lu_uniform``      A, B ~ U[-1, 1]                 (plain FP64 LU + solve)
+* ``gemm_vbatched``   M, N, K ~ U{lo..hi}, entries N(0,1), ld = roundup(M, 8)
+* ``svd_logrand``     A = U diag(sigma) V^T, Haar U, V, sigma_i = exp(u_i ln(1/kappa))
+                      (magma_generate_svd + Dist::logrand, magma_zgenerate.cpp:150-156, 197-266)
+* ``spd_gram``        A = G G^T + n I, G ~ N(0,1)    (Cholesky workloads)
+
+Layout: column-major batches of shape (batch, n, ld) (see magma_b200.api).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+_G = np.uint64(0x9E3779B97F4A7C15)
+_M1 = np.uint64(0xBF58476D1CE4E5B9)
+_M2 = np.uint64(0x94D049BB133111EB)
+
+
+def _mix(z: np.ndarray) -> np.ndarray:
+    z = (z ^ (z >> np.uint64(30))) * _M1
+    z = (z ^ (z >> np.uint64(27))) * _M2
+    return z ^ (z >> np.uint64(31))
+
+
+def stream_seed(seed: int, stream: int) -> np.uint64:
+    """Independent sub-stream seed (stream 0 = A, 1 = B, 2.. = auxiliary)."""
+    with np.errstate(over="ignore"):
+        return _mix(np.array([np.uint64(seed) ^ (np.uint64(stream + 1) * _G)], dtype=np.uint64))[0]
+
+
+def uniform01(seed: int, stream: int, count: int) -> np.ndarray:
+    """count doubles in [0, 1) with 53 random bits each."""
+    s = stream_seed(seed, stream)
+    with np.errstate(over="ignore"):
+        idx = np.arange(1, count + 1, dtype=np.uint64)
+        z = _mix(s + idx * _G)
+    return (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+def uniform11(seed: int, stream: int, count: int) -> np.ndarray:
+    return 2.0 * uniform01(seed, stream, count) - 1.0
+
+
+def normal(seed: int, stream: int, count: int) -> np.ndarray:
+    """Box-Muller over two sub-streams."""
+    u1 = uniform01(seed, 2 * stream + 100, count)
+    u2 = uniform01(seed, 2 * stream + 101, count)
+    return np.sqrt(-2.0 * np.log1p(-u1)) * np.cos(2.0 * math.pi * u2)
+
+
+def roundup(x, m):
+    return ((np.asarray(x) + m - 1) // m) * m
+
+
+# ---------------------------------------------------------------------------
+def lu_uniform(batch: int, n: int, nrhs: int = 1, seed: int = 1, lda: int | None = None,
+               ldb: int | None = None, m: int | None = None):
+    """A (batch, n, lda) and B (batch, nrhs, ldb), entries U[-1,1]; padding is zero."""
+    m = n if m is None else m
+    lda = lda or max(1, m)
+    ldb = ldb or max(1, m)
+    A = np.zeros((batch, n, lda))
+    A[:, :, :m] = uniform11(seed, 0, batch * n * m).reshape(batch, n, m)
+    B = np.zeros((batch, nrhs, ldb))
+    B[:, :, :m] = uniform11(seed, 1, batch * nrhs * m).reshape(batch, nrhs, m)
+    return A, B
+
+
+def gemm_sizes(count: int, lo: int = 8, hi: int = 128, seed: int = 2):
+    u = uniform01(seed, 5, 3 * count).reshape(3, count)
+    M, N, K = (lo + np.floor(u * (hi - lo + 1)).astype(np.int64)).clip(lo, hi)
+    return M.astype(np.int32), N.astype(np.int32), K.astype(np.int32)
+
+
+def haar(batch: int, n: int, seed: int, stream: int) -> np.ndarray:
+    """Haar-distributed orthogonal matrices: QR of a Gaussian with R's diagonal made positive."""
+    G = normal(seed, stream, batch * n * n).reshape(batch, n, n)
+    Q, R = np.linalg.qr(G)
+    d = np.sign(np.diagonal(R, axis1=1, axis2=2))
+    d[d == 0] = 1.0
+    return Q * d[:, None, :]
+
+
+def svd_logrand(batch: int, n: int, kappa_lo: float = 1e2, kappa_hi: float = 1e6, nrhs: int = 4,
+                seed: int = 3):
+    """A = U diag(sigma) V^T with per-instance kappa_j log-uniform in [kappa_lo, kappa_hi].
+
+    Returns (A (batch, n, n) column-major, B (batch, nrhs, n) ~ N(0,1), kappa (batch,))."""
+    kap = np.exp(np.log(kappa_lo) + uniform01(seed, 6, batch) * (np.log(kappa_hi) - np.log(kappa_lo)))
+    u = uniform01(seed, 7, batch * n).reshape(batch, n)
+    sigma = np.exp(u * np.log(1.0 / kap)[:, None])
+    U = haar(batch, n, seed, 8)
+    V = haar(batch, n, seed, 9)
+    A_rowmajor = (U * sigma[:, None, :]) @ np.transpose(V, (0, 2, 1))
+    A = np.ascontiguousarray(np.transpose(A_rowmajor, (0, 2, 1)))   # column-major storage
+    B = normal(seed, 10, batch * nrhs * n).reshape(batch, nrhs, n)
+    return A, B, kap
+
+
+def spd_gram(n: int, seed: int, index: int) -> np.ndarray:
+    """A = G G^T + n I (column-major == row-major, symmetric)."""
+    G = normal(seed, 1000 + index, n * n).reshape(n, n)
+    return G @ G.T + n * np.eye(n)
+
+
+# ---------------------------------------------------------------------------
+def backward_error(A_cm: np.ndarray, X_cm: np.ndarray, B_cm: np.ndarray, n: int) -> np.ndarray:
+    """Normwise backward error ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf), per instance and RHS.
+
+    A_cm (batch, n, lda), X_cm and B_cm (batch, nrhs, ld) column-major."""
+    A = np.transpose(A_cm[:, :n, :n], (0, 2, 1))       # row-major (batch, n, n)
+    X = np.transpose(X_cm[:, :, :n], (0, 2, 1))        # (batch, n, nrhs)
+    B = np.transpose(B_cm[:, :, :n], (0, 2, 1))
+    R = B - A @ X
+    anorm = np.abs(A).sum(axis=2).max(axis=1)          # inf-norm
+    rn = np.abs(R).max(axis=1)
+    xn = np.abs(X).max(axis=1)
+    bn = np.abs(B).max(axis=1)
+    return rn / (anorm[:, None] * xn + bn)
+
+
+def lu_residual(A0_cm: np.ndarray, LU_cm: np.ndarray, ipiv: np.ndarray, m: int, n: int) -> np.ndarray:
+    """MAGMA's getrf check ||P A - L U||_F / (||A||_F n) per instance (testing_zgetrf_batched.cpp:30-69)."""
+    out = np.zeros(A0_cm.shape[0])
+    k = min(m, n)
+    for b in range(A0_cm.shape[0]):
+        A = A0_cm[b, :n, :m].T.copy()
+        LU = LU_cm[b, :n, :m].T
+        L = np.tril(LU[:, :k], -1) + np.eye(m, k)
+        U = np.triu(LU[:k, :])
+        for j in range(k):
+            p = ipiv[b, j] - 1
+            if p != j:
+                A[[j, p], :] = A[[p, j], :]
+        out[b] = np.linalg.norm(A - L @ U) / (np.linalg.norm(A) * n)
+    return out

@@ -1,0 +1,153 @@
+/*
+ * lapack_oracle.c -- TEST INFRASTRUCTURE ONLY. CPU restatement of the LAPACK
+ * algorithms that MAGMA's batched testers use as their correctness oracle.
+ * Nothing in the shipped library links or calls this file; only tests/,
+ * __graft_entry__.smoke() and bench.py's CPU-baseline leg do.
+ *
+ * The reference's CPU oracle is host LAPACK, called per instance from the
+ * testers (testing/testing_zgetrf_batched.cpp:188-206 dgetrf,
+ * testing/testing_zgesv_batched.cpp:171 dgesv,
+ * testing/testing_zpotrf_vbatched.cpp:166 dpotrf,
+ * testing/testing_zgemm_vbatched.cpp:293 dgemm). LAPACK is a third-party
+ * dependency absent from the reference tree; in this image it is OpenBLAS
+ * 0.3.30 bundled with scipy 1.18.1 (libscipy_openblas, LP64). This file
+ * restates the published netlib algorithms (LAPACK 3.x dgetf2 / dgetrs /
+ * dpotf2 / dpotrs, reference BLAS dger / dtrsm / dgemm) with every
+ * multiply-add written as an explicit fma(), so that a GPU kernel doing the
+ * same operations in the same order can be compared bit for bit. It is
+ * pinned against the real OpenBLAS on committed golden vectors
+ * (tests/golden/, made by tests/golden/make_golden.py).
+ *
+ * Deliberate, documented departures from netlib:
+ *  - reference BLAS skips updates whose multiplier is exactly zero
+ *    (DGER "IF (Y(JY).NE.ZERO)", DTRSM "IF (B(K,J).NE.ZERO)"); the skip only
+ *    changes the sign of zero results or NaN propagation, so it is omitted;
+ *  - IDAMAX with NaNs: a NaN magnitude ranks below every number (netlib
+ *    returns a leading NaN). Finite inputs are unaffected.
+ *
+ * Compile: make -C oracle   (gcc -O2 -fopenmp -ffp-contract=off)
+ */
+#include <float.h>
+#include <math.h>
+#include <stddef.h>
+#include <string.h>
+
+#define A_(i, j) a[(size_t)(i) + (size_t)(j) * (size_t)lda]
+#define B_(i, j) b[(size_t)(i) + (size_t)(j) * (size_t)ldb]
+
+static double pivot_key(double x) {
+    double v = fabs(x);
+    return (v != v) ? -0.5 : v;
+}
+
+/* LAPACK 3.x dgetf2: unblocked right-looking LU with partial pivoting.
+ * ipiv is 1-based; info = first zero pivot (1-based) or 0. */
+void oracle_dgetf2(int m, int n, double* a, int lda, int* ipiv, int* info) {
+    *info = 0;
+    const int kmax = m < n ? m : n;
+    for (int j = 0; j < kmax; ++j) {
+        int jp = j;
+        double best = pivot_key(A_(j, j));
+        for (int i = j + 1; i < m; ++i) {
+            double v = pivot_key(A_(i, j));
+            if (v > best) { best = v; jp = i; }
+        }
+        ipiv[j] = jp + 1;
+        const double piv = A_(jp, j);
+        if (piv != 0.0) {
+            if (jp != j) {
+                for (int c = 0; c < n; ++c) { double t = A_(j, c); A_(j, c) = A_(jp, c); A_(jp, c) = t; }
+            }
+            if (fabs(piv) >= DBL_MIN) {
+                const double r = 1.0 / piv;
+                for (int i = j + 1; i < m; ++i) A_(i, j) = A_(i, j) * r;
+            } else {
+                for (int i = j + 1; i < m; ++i) A_(i, j) = A_(i, j) / piv;
+            }
+        } else if (*info == 0) {
+            *info = j + 1;
+        }
+        if (j < kmax - 1) {
+            for (int c = j + 1; c < n; ++c) {
+                const double u = A_(j, c);
+                for (int i = j + 1; i < m; ++i) A_(i, c) = fma(A_(i, j), -u, A_(i, c));
+            }
+        }
+    }
+}
+
+/* LAPACK dlaswp on the rows of B: forward (k ascending) or inverse. */
+static void laswp(int n, int nrhs, double* b, int ldb, const int* ipiv, int inverse) {
+    for (int t = 0; t < n; ++t) {
+        const int k = inverse ? n - 1 - t : t;
+        const int p = ipiv[k] - 1;
+        if (p != k)
+            for (int c = 0; c < nrhs; ++c) { double x = B_(k, c); B_(k, c) = B_(p, c); B_(p, c) = x; }
+    }
+}
+
+/* LAPACK dgetrs with reference-BLAS dtrsm loop orders.
+ * trans = 0: A X = B;  trans != 0: A^T X = B. */
+void oracle_dgetrs(int trans, int n, int nrhs, const double* a, int lda, const int* ipiv,
+                   double* b, int ldb) {
+    if (!trans) {
+        laswp(n, nrhs, b, ldb, ipiv, 0);
+        for (int c = 0; c < nrhs; ++c) {
+            /* DTRSM Left Lower NoTrans Unit */
+            for (int k = 0; k < n; ++k)
+                for (int i = k + 1; i < n; ++i) B_(i, c) = fma(-B_(k, c), A_(i, k), B_(i, c));
+            /* DTRSM Left Upper NoTrans NonUnit */
+            for (int k = n - 1; k >= 0; --k) {
+                B_(k, c) = B_(k, c) / A_(k, k);
+                for (int i = 0; i < k; ++i) B_(i, c) = fma(-B_(k, c), A_(i, k), B_(i, c));
+            }
+        }
+    } else {
+        for (int c = 0; c < nrhs; ++c) {
+            /* DTRSM Left Upper Trans NonUnit: dot-product form, k ascending */
+            for (int i = 0; i < n; ++i) {
+                double t = B_(i, c);
+                for (int k = 0; k < i; ++k) t = fma(-A_(k, i), B_(k, c), t);
+                B_(i, c) = t / A_(i, i);
+            }
+            /* DTRSM Left Lower Trans Unit: i descending, k ascending */
+            for (int i = n - 1; i >= 0; --i) {
+                double t = B_(i, c);
+                for (int k = i + 1; k < n; ++k) t = fma(-A_(k, i), B_(k, c), t);
+                B_(i, c) = t;
+            }
+        }
+        laswp(n, nrhs, b, ldb, ipiv, 1);
+    }
+}
+
+/* ---------------------------------------------------------------------------
+ * Batched drivers over contiguous batches (instance i at base + i*stride),
+ * one instance per OpenMP iteration as in testing_zgetrf_batched.cpp:188-206. */
+void oracle_dgetrf_batched(int m, int n, double* A, int lda, long strideA, int* ipiv, long strideP,
+                           int* info, int batch) {
+#pragma omp parallel for schedule(dynamic)
+    for (int i = 0; i < batch; ++i)
+        oracle_dgetf2(m, n, A + (size_t)i * strideA, lda, ipiv + (size_t)i * strideP, info + i);
+}
+
+void oracle_dgetrs_batched(int trans, int n, int nrhs, const double* A, int lda, long strideA,
+                           const int* ipiv, long strideP, double* B, int ldb, long strideB, int batch) {
+#pragma omp parallel for schedule(dynamic)
+    for (int i = 0; i < batch; ++i)
+        oracle_dgetrs(trans, n, nrhs, A + (size_t)i * strideA, lda, ipiv + (size_t)i * strideP,
+                      B + (size_t)i * strideB, ldb);
+}
+
+/* MAGMA's batched gesv solves every instance whatever its info
+ * (src/zgesv_batched.cpp:127-145). */
+void oracle_dgesv_batched(int n, int nrhs, double* A, int lda, long strideA, int* ipiv, long strideP,
+                          double* B, int ldb, long strideB, int* info, int batch) {
+#pragma omp parallel for schedule(dynamic)
+    for (int i = 0; i < batch; ++i) {
+        double* Ai = A + (size_t)i * strideA;
+        int* pi = ipiv + (size_t)i * strideP;
+        oracle_dgetf2(n, n, Ai, lda, pi, info + i);
+        oracle_dgetrs(0, n, nrhs, Ai, lda, pi, B + (size_t)i * strideB, ldb);
+    }
+}

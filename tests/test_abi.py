@@ -1,0 +1,81 @@
+"""CPU tests of the C-ABI boundary: the library loads, exports every symbol the
+public headers declare, and rejects illegal arguments with MAGMA's codes
+without touching the GPU."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import pytest
+
+from magma_b200 import _lib
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def header_functions():
+    names = set()
+    for h in sorted((ROOT / "include").glob("*.h")):
+        text = h.read_text()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)        # drop comments
+        text = re.sub(r"^\s*#.*?(?<!\\)$", "", text, flags=re.M | re.S)  # drop preprocessor lines
+        for m in re.finditer(r"\b(magma\w*|magmablas\w*)\s*\(", text):
+            names.add(m.group(1))
+    return names
+
+
+def test_library_exports_every_header_symbol():
+    lib = _lib.load()
+    declared = header_functions()
+    assert "magma_dgetrf_batched" in declared
+    missing = [n for n in sorted(declared) if not hasattr(lib, n)]
+    assert not missing, f"declared in include/*.h but not exported: {missing}"
+
+
+def test_bindings_cover_the_header():
+    declared = header_functions()
+    assert declared == set(_lib.SIGNATURES), (
+        f"only in header: {sorted(declared - set(_lib.SIGNATURES))}; "
+        f"only in bindings: {sorted(set(_lib.SIGNATURES) - declared)}")
+
+
+@pytest.fixture(scope="module")
+def q():
+    """A queue around the null stream: creating it makes no CUDA call."""
+    lib = _lib.load()
+    h = C.c_void_p()
+    lib.magma_queue_create_from_cuda_internal(0, None, None, None, C.byref(h), b"t", b"t", 0)
+    yield h
+
+
+def test_getrf_argument_errors(q):
+    lib = _lib.load()
+    # batchCount 0 keeps the call off the device; codes follow src/zgetrf_batched.cpp:96-107
+    assert lib.magma_dgetrf_batched(-1, 4, None, 4, None, None, 0, q) == -1
+    assert lib.magma_dgetrf_batched(4, -1, None, 4, None, None, 0, q) == -2
+    assert lib.magma_dgetrf_batched(4, 4, None, 3, None, None, 0, q) == -4
+    assert lib.magma_dgetrf_batched(0, 4, None, 1, None, None, 0, q) == 0
+
+
+def test_getrs_gesv_argument_errors(q):
+    lib = _lib.load()
+    N, T_ = _lib.MagmaNoTrans, _lib.MagmaTrans
+    # src/zgetrs_batched.cpp:99-113
+    assert lib.magma_dgetrs_batched(7, 4, 1, None, 4, None, None, 4, 1, q) == -1
+    assert lib.magma_dgetrs_batched(N, -1, 1, None, 4, None, None, 4, 1, q) == -2
+    assert lib.magma_dgetrs_batched(T_, 4, -1, None, 4, None, None, 4, 1, q) == -3
+    assert lib.magma_dgetrs_batched(N, 4, 1, None, 3, None, None, 4, 1, q) == -5
+    assert lib.magma_dgetrs_batched(N, 4, 1, None, 4, None, None, 3, 1, q) == -8
+    assert lib.magma_dgetrs_batched(N, 0, 1, None, 1, None, None, 1, 1, q) == 0
+    # src/zgesv_batched.cpp:107-118
+    assert lib.magma_dgesv_batched(-1, 1, None, 4, None, None, 4, None, 1, q) == -1
+    assert lib.magma_dgesv_batched(4, -1, None, 4, None, None, 4, None, 1, q) == -2
+    assert lib.magma_dgesv_batched(4, 1, None, 3, None, None, 4, None, 1, q) == -4
+    assert lib.magma_dgesv_batched(4, 1, None, 4, None, None, 3, None, 1, q) == -6
+
+
+def test_strerror_and_xerbla(capfd):
+    lib = _lib.load()
+    assert lib.magma_strerror(-113) == b"cannot allocate memory on GPU device"
+    lib.magma_xerbla(b"magma_dgetrf_batched", 4)
+    err = capfd.readouterr().err
+    assert "On entry to magma_dgetrf_batched, parameter 4 had an illegal value (info = -4)" in err

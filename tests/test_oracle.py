@@ -1,0 +1,111 @@
+"""CPU tests: the oracle restatement is pinned against the reference's LAPACK.
+
+The golden vectors (tests/golden/*.npz, made by make_golden.py with scipy's
+OpenBLAS, the LAPACK MAGMA's testers call) fix pivots and info exactly; the
+factors and solutions of a different summation order must agree to
+c*n*eps*||A||.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from magma_b200 import testing as T
+
+EPS = np.finfo(np.float64).eps
+
+
+def _cm(a):
+    """row-major (m, n) -> column-major storage (1, n, m)."""
+    return np.ascontiguousarray(a.T)[None].copy()
+
+
+def _tags(g, prefix=None):
+    return [t for t in g["tags"] if prefix is None or t.startswith(prefix)]
+
+
+def test_oracle_getrf_matches_lapack_golden(lu_golden):
+    g = lu_golden
+    for tag in _tags(g):
+        m, n = (int(v) for v in g[f"{tag}/mn"])
+        A = _cm(g[f"{tag}/A"])
+        ipiv, info = oracle.dgetrf_batched(A, m)
+        k = min(m, n)
+        assert np.array_equal(ipiv[0, :k], g[f"{tag}/ipiv"][:k]), tag
+        assert info[0] == g[f"{tag}/info"], tag
+        if info[0] == 0:
+            lu = A[0].T
+            anorm = np.abs(g[f"{tag}/A"]).max()
+            assert np.abs(lu - g[f"{tag}/LU"]).max() <= 8 * max(m, n) * EPS * max(anorm, 1.0), tag
+
+
+def test_oracle_getrs_matches_lapack_golden(lu_golden):
+    g = lu_golden
+    for tag in _tags(g):
+        if f"{tag}/B1" not in g:
+            continue
+        n = int(g[f"{tag}/mn"][0])
+        LU = _cm(g[f"{tag}/LU"])
+        ipiv = g[f"{tag}/ipiv"][None].astype(np.int32).copy()
+        for nrhs in (1, 3):
+            for trans, key in ((False, "XN"), (True, "XT")):
+                B = np.ascontiguousarray(g[f"{tag}/B{nrhs}"].T)[None].copy()
+                oracle.dgetrs_batched(LU, ipiv, B, trans=trans)
+                X = g[f"{tag}/{key}{nrhs}"]
+                scale = max(np.abs(X).max(), 1.0)
+                assert np.abs(B[0].T - X).max() <= 64 * n * EPS * scale * 1e2, (tag, nrhs, trans)
+
+
+def test_lapack_loop_is_the_golden_lapack(lu_golden):
+    """The reference CPU loop (oracle.lapack_*) calls the same LAPACK as the fixtures: bit-identical."""
+    g = lu_golden
+    for tag in _tags(g, "uniform_32x32"):
+        A = _cm(g[f"{tag}/A"])
+        ipiv, info = oracle.lapack_dgetrf_batched(A, 32, nthreads=2)
+        assert np.array_equal(A[0].T, g[f"{tag}/LU"])
+        assert np.array_equal(ipiv[0], g[f"{tag}/ipiv"])
+
+
+@pytest.mark.parametrize("n", [8, 32, 64])
+def test_oracle_pivots_match_lapack_on_seeded_batch(n):
+    """On the seeded U[-1,1] workload the restated getf2 and OpenBLAS pick identical pivots."""
+    A, B = T.lu_uniform(1500, n, 2, seed=123 + n)
+    A1, A2 = A.copy(), A.copy()
+    B1, B2 = B.copy(), B.copy()
+    ip1, inf1 = oracle.dgesv_batched(A1, B1)
+    ip2, inf2 = oracle.lapack_dgesv_batched(A2, B2)
+    assert np.array_equal(ip1, ip2)
+    assert np.array_equal(inf1, inf2)
+    assert np.abs(A1 - A2).max() < 64 * n * EPS
+    be = T.backward_error(A, B1, B, n)
+    assert be.max() < 30 * EPS
+
+
+def test_oracle_singular_info():
+    A = np.zeros((3, 8, 8))
+    A[0] = np.eye(8)
+    A[1] = np.eye(8)
+    A[1, 5, :] = 0.0            # column 5 zero -> info 6
+    ipiv, info = oracle.dgetrf_batched(A, 8)
+    assert list(info) == [0, 6, 1]
+    assert list(ipiv[2]) == list(range(1, 9))   # all-zero columns: no swaps, ipiv(k) = k
+
+
+def test_generators_deterministic():
+    a1 = T.uniform11(5, 0, 1000)
+    a2 = T.uniform11(5, 0, 1000)
+    assert np.array_equal(a1, a2)
+    assert a1.min() >= -1 and a1.max() < 1
+    assert abs(a1.mean()) < 0.1
+    z = T.normal(5, 1, 20000)
+    assert abs(z.mean()) < 0.05 and abs(z.std() - 1) < 0.05
+    M, N, K = T.gemm_sizes(5000)
+    assert M.min() == 8 and M.max() == 128 and K.min() == 8 and N.max() == 128
+
+
+def test_svd_logrand_condition():
+    A, B, kap = T.svd_logrand(6, 48, 1e2, 1e6, nrhs=2, seed=9)
+    for i in range(6):
+        s = np.linalg.svd(A[i].T, compute_uv=False)
+        assert s.max() <= 1 + 1e-12
+        assert s.max() / s.min() <= kap[i] * (1 + 1e-8)
+    assert kap.min() >= 1e2 and kap.max() <= 1e6
