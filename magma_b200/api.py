@@ -104,8 +104,11 @@ def dgetrs_batched(A: torch.Tensor, ipiv: torch.Tensor, B: torch.Tensor, trans: 
     q = queue or default_queue()
     batch, n, lda = A.shape
     _, nrhs, ldb = B.shape
-    rc = q.lib.magma_dgetrs_batched(MagmaTrans if trans else MagmaNoTrans, n, nrhs, _vp(ptr_array(A)), lda,
-                                    _vp(ptr_array(ipiv)), _vp(ptr_array(B)), ldb, batch, q.handle)
+    # keep the pointer arrays referenced until the call is enqueued: a temporary
+    # freed early would be handed to the next allocation by torch's caching allocator
+    pA, pP, pB = ptr_array(A), ptr_array(ipiv), ptr_array(B)
+    rc = q.lib.magma_dgetrs_batched(MagmaTrans if trans else MagmaNoTrans, n, nrhs, _vp(pA), lda,
+                                    _vp(pP), _vp(pB), ldb, batch, q.handle)
     _check(rc, "magma_dgetrs_batched")
 
 
@@ -116,7 +119,7 @@ def dgesv_batched(A: torch.Tensor, B: torch.Tensor, queue: Queue | None = None):
     _, nrhs, ldb = B.shape
     ipiv = torch.zeros((batch, n), dtype=torch.int32, device=A.device)
     info = torch.empty(batch, dtype=torch.int32, device=A.device)
-    rc = q.lib.magma_dgesv_batched(n, nrhs, _vp(ptr_array(A)), lda, _vp(ptr_array(ipiv)), _vp(ptr_array(B)), ldb,
-                                   _vp(info), batch, q.handle)
+    pA, pP, pB = ptr_array(A), ptr_array(ipiv), ptr_array(B)
+    rc = q.lib.magma_dgesv_batched(n, nrhs, _vp(pA), lda, _vp(pP), _vp(pB), ldb, _vp(info), batch, q.handle)
     _check(rc, "magma_dgesv_batched")
     return ipiv, info

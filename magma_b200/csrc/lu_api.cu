@@ -28,6 +28,9 @@ magma_int_t magma_dgetrf_batched(magma_int_t m, magma_int_t n, double** dA_array
     if (small_lu_supported(m, n))
         return getrf_small<double>(m, n, nullptr, nullptr, ldda, nullptr, m, n, dA_array,
                                    ipiv_array, info_array, batchCount, queue->stream);
+    if (blocked_lu_supported(m))
+        return getrf_blocked<double>(m, n, nullptr, nullptr, ldda, nullptr, m, n, dA_array,
+                                     ipiv_array, info_array, batchCount, queue->stream);
     return MAGMA_ERR_NOT_SUPPORTED;
 }
 
@@ -52,6 +55,9 @@ magma_int_t magma_dgetrs_batched(magma_trans_t trans, magma_int_t n, magma_int_t
     if (small_lu_supported(n, n))
         return getrs_small<double>(!notran, n, nullptr, nrhs, nullptr, ldda, nullptr, lddb, nullptr, n,
                                    nrhs, dA_array, dipiv_array, dB_array, batchCount, queue->stream);
+    if (blocked_lu_supported(n))
+        return getrs_blocked<double>(!notran, n, nullptr, nrhs, nullptr, ldda, nullptr, lddb, nullptr, n,
+                                     nrhs, dA_array, dipiv_array, dB_array, batchCount, queue->stream);
     return MAGMA_ERR_NOT_SUPPORTED;
 }
 

@@ -57,93 +57,142 @@ __device__ __forceinline__ void mat_sync() {
     if (NW == 1) __syncwarp(); else __syncthreads();
 }
 
-// Pivot key: larger |x| wins, ties -> lower position. NaN magnitudes rank
-// below every number (they are chosen only when nothing else is left), and
-// rows that are no longer candidates carry key -1.
-template <typename T>
-__device__ __forceinline__ bool key_beats(T v2, int p2, T v, int p) {
-    return (v2 > v) || (v2 == v && p2 < p);
+// Pivot key: |x| as an ordered unsigned integer (the bit pattern of a
+// non-negative IEEE number is monotonic in its value), split into two 32-bit
+// halves for the warp REDUX instructions. Order: rows that are not candidates
+// (key 0, position INT_MAX) < NaN (key 0) < 0 (key 1) < ... < +inf. Among
+// equal keys the lowest row position wins, which is IDAMAX's first-maximum rule.
+struct PivotKey { unsigned hi, lo; };
+
+__device__ __forceinline__ PivotKey pivot_key(double x, bool cand) {
+    const double v = fabs(x);
+    unsigned long long b = (cand && v == v) ? (unsigned long long)__double_as_longlong(v) + 1ull : 0ull;
+    return {unsigned(b >> 32), unsigned(b)};
 }
+__device__ __forceinline__ PivotKey pivot_key(float x, bool cand) {
+    const float v = fabsf(x);
+    return {(cand && v == v) ? unsigned(__float_as_uint(v)) + 1u : 0u, 0u};
+}
+
+__device__ __forceinline__ bool key_beats(PivotKey k2, int p2, PivotKey k, int p) {
+    return (k2.hi > k.hi) || (k2.hi == k.hi && (k2.lo > k.lo || (k2.lo == k.lo && p2 < p)));
+}
+
+// Warp-wide argmax: on return every lane holds the winning key and position;
+// the result is the lane that holds the winner.
+__device__ __forceinline__ int warp_argmax(PivotKey& key, int& p, int lane) {
+    (void)lane;
+    const unsigned mhi = __reduce_max_sync(kFullMask, key.hi);
+    const unsigned mlo = __reduce_max_sync(kFullMask, key.hi == mhi ? key.lo : 0u);
+    const bool top = (key.hi == mhi && key.lo == mlo);
+    const int pmin = __reduce_min_sync(kFullMask, top ? p : INT_MAX);
+    const unsigned who = __ballot_sync(kFullMask, top && p == pmin);
+    key.hi = mhi;
+    key.lo = mlo;
+    p = pmin;
+    return __ffs(who) - 1;
+}
+
+template <typename T> struct Vec2;
+template <> struct Vec2<double> { using type = double2; };
+template <> struct Vec2<float> { using type = float2; };
+template <typename T> __device__ __forceinline__ typename Vec2<T>::type make_vec2(T x, T y);
+template <> __device__ __forceinline__ double2 make_vec2<double>(double x, double y) { return make_double2(x, y); }
+template <> __device__ __forceinline__ float2 make_vec2<float>(float x, float y) { return make_float2(x, y); }
 
 // Shared memory one matrix needs.
 template <typename T, int NC, int NW>
 struct SmallLuShared {
-    T     row[2][NC];      // pivot row broadcast (double-buffered)
-    T     rhs[2][4];       // solve broadcast: one value per RHS column in a chunk of 4
-    T     red_v[2][NW];    // cross-warp argmax (only NW > 1)
-    int   red_p[2][NW];
-    int   red_s[2][NW];
-    int   perm[32 * NW];   // scratch for applying ipiv in getrs
+    static_assert(NC % 2 == 0, "the pivot row is broadcast in pairs");
+    alignas(16) T row[2][NC];   // pivot row broadcast (double-buffered)
+    T        rhs[2][4];         // solve broadcast: one value per RHS column in a chunk of 4
+    unsigned red_hi[2][NW];     // cross-warp argmax (only NW > 1)
+    unsigned red_lo[2][NW];
+    int      red_p[2][NW];
+    int      red_s[2][NW];
 };
 
-// Factor the rows held in `a`. tid: thread index within the matrix.
-// On return: `pos` = final row position of this thread's row, the thread with
-// tid == k (k < kmax) holds ipiv(k) in `my_ipiv`, `info` is LAPACK's info.
+// Eliminate register columns 0..nsteps-1 of the rows held in `a` (updating
+// columns up to ncols-1), as global elimination steps g = k0 .. k0+nsteps-1
+// (k0 = 0 for a whole small matrix; the panel offset in the blocked
+// factorisation). tid: thread index within the
+// matrix; `pos` must hold the thread's current row position on entry (tid for
+// live rows, anything < k0 for finished rows, a huge value for tid >= m).
+// On return `pos` is the row's new position, the thread with tid == g holds
+// ipiv(g) (1-based) in `my_ipiv`, and `info` is g+1 of the first zero pivot.
 template <typename T, int NC, int NW>
-__device__ __forceinline__ void small_lu_factor(T (&a)[NC], int m, int n, int tid, int& pos,
-                                                int& my_ipiv, int& info,
-                                                SmallLuShared<T, NC, NW>& sh) {
+__device__ __forceinline__ void lu_panel_steps(T (&a)[NC], int m, int nsteps, int ncols, int k0, int tid, int& pos,
+                                               int& my_ipiv, int& info,
+                                               SmallLuShared<T, NC, NW>& sh) {
+    (void)ncols;   // columns >= ncols hold zeros in every row, so their updates are no-ops
     const int lane = tid & 31;
     const int warp = tid >> 5;
-    const int kmax = min(m, n);
-    pos = (tid < m) ? tid : INT_MAX / 2;
-    info = 0;
-    my_ipiv = 0;
+    using V2 = typename Vec2<T>::type;
     static_for<0, NC>([&](auto kc) {
         constexpr int k = decltype(kc)::value;
-        if (k >= kmax) return;
+        if (k >= nsteps) return;
         constexpr int buf = k & 1;
-        // ---- pivot search over rows still unchosen (pos >= k) ----
-        T v = (pos >= k && tid < m) ? fabs(a[k]) : T(-1);
-        if (v != v) v = T(-0.5);
-        int p = (pos >= k && tid < m) ? pos : INT_MAX;
-        int s = tid;
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            T v2 = __shfl_xor_sync(kFullMask, v, off);
-            int p2 = __shfl_xor_sync(kFullMask, p, off);
-            int s2 = __shfl_xor_sync(kFullMask, s, off);
-            if (key_beats(v2, p2, v, p)) { v = v2; p = p2; s = s2; }
-        }
+        const int g = k0 + k;
+        // ---- pivot search over rows still unchosen (pos >= g) ----
+        const bool cand = (pos >= g && tid < m);
+        PivotKey key = pivot_key(a[k], cand);
+        int p = cand ? pos : INT_MAX;
+        int s = warp_argmax(key, p, lane) + warp * 32;
         if (NW > 1) {
-            if (lane == 0) { sh.red_v[buf][warp] = v; sh.red_p[buf][warp] = p; sh.red_s[buf][warp] = s; }
+            if (lane == 0) { sh.red_hi[buf][warp] = key.hi; sh.red_lo[buf][warp] = key.lo; sh.red_p[buf][warp] = p; sh.red_s[buf][warp] = s; }
             __syncthreads();
-            v = sh.red_v[buf][0]; p = sh.red_p[buf][0]; s = sh.red_s[buf][0];
+            key.hi = sh.red_hi[buf][0]; key.lo = sh.red_lo[buf][0]; p = sh.red_p[buf][0]; s = sh.red_s[buf][0];
 #pragma unroll
             for (int w = 1; w < NW; ++w) {
-                T v2 = sh.red_v[buf][w];
-                int p2 = sh.red_p[buf][w];
-                if (key_beats(v2, p2, v, p)) { v = v2; p = p2; s = sh.red_s[buf][w]; }
+                const PivotKey k2{sh.red_hi[buf][w], sh.red_lo[buf][w]};
+                const int p2 = sh.red_p[buf][w];
+                if (key_beats(k2, p2, key, p)) { key = k2; p = p2; s = sh.red_s[buf][w]; }
             }
         }
-        // ---- the pivot row publishes columns k..n-1 ----
+        // ---- the pivot row publishes columns k..NC-1 (aligned pairs) ----
+        constexpr int jw = k & ~1;
         if (tid == s) {
+            V2* row2 = reinterpret_cast<V2*>(&sh.row[buf][0]);
 #pragma unroll
-            for (int j = k; j < NC; ++j) sh.row[buf][j] = a[j];
+            for (int j = jw; j < NC; j += 2) row2[j / 2] = make_vec2<T>(a[j], a[j + 1]);
         }
         mat_sync<NW>();
         const T piv = sh.row[buf][k];
-        // ---- LAPACK swap bookkeeping: ipiv(k) = current position of the pivot row ----
-        if (tid == k) my_ipiv = p + 1;
+        // ---- LAPACK swap bookkeeping: ipiv(g) = current position of the pivot row ----
+        if (tid == g) my_ipiv = p + 1;
         if (piv != T(0)) {
-            if (pos == k) pos = p;   // row at position k moves to the pivot's old position
-            if (tid == s) pos = k;
+            if (pos == g) pos = p;   // row at position g moves to the pivot's old position
+            if (tid == s) pos = g;
         } else if (info == 0) {
-            info = k + 1;
+            info = g + 1;
         }
         // ---- scale column k below the pivot and apply the rank-1 update ----
-        if (pos > k && tid < m) {
+        if (pos > g && tid < m) {
             if (piv != T(0)) {
                 if (fabs(piv) >= tiny_normal<T>()) a[k] = a[k] * (T(1) / piv);
                 else                               a[k] = a[k] / piv;
             }
             const T l = a[k];
+            const V2* row2 = reinterpret_cast<const V2*>(&sh.row[buf][0]);
 #pragma unroll
-            for (int j = k + 1; j < NC; ++j) {
-                if (j < n) a[j] = fma_rn(l, -sh.row[buf][j], a[j]);
+            for (int j = (k + 1) & ~1; j < NC; j += 2) {
+                const V2 u = row2[j / 2];
+                if (j > k) a[j] = fma_rn(l, -u.x, a[j]);
+                a[j + 1] = fma_rn(l, -u.y, a[j + 1]);
             }
         }
     });
+}
+
+// Whole small matrix (m rows, n <= NC columns): steps 0 .. min(m,n)-1.
+template <typename T, int NC, int NW>
+__device__ __forceinline__ void small_lu_factor(T (&a)[NC], int m, int n, int tid, int& pos,
+                                                int& my_ipiv, int& info,
+                                                SmallLuShared<T, NC, NW>& sh) {
+    pos = (tid < m) ? tid : INT_MAX / 2;
+    info = 0;
+    my_ipiv = 0;
+    lu_panel_steps<T, NC, NW>(a, m, min(m, n), n, 0, tid, pos, my_ipiv, info, sh);
 }
 
 // Solve with the factors held in registers. Each thread holds its LU row at

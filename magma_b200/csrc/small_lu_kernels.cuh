@@ -9,27 +9,15 @@
 // written once.
 #include "internal.h"
 #include "small_lu.cuh"
+#include "lu_sizes.h"
 
 #pragma once
 namespace mb200 {
 
-// Per-instance size lookup: fixed sizes when the array pointer is null.
-struct LuSizes {
-    int m, n, lda, ldb, nrhs;
-    const int* m_arr;
-    const int* n_arr;
-    const int* lda_arr;
-    const int* ldb_arr;
-    const int* nrhs_arr;
-    __device__ __forceinline__ int get_m(int i) const { return m_arr ? m_arr[i] : m; }
-    __device__ __forceinline__ int get_n(int i) const { return n_arr ? n_arr[i] : n; }
-    __device__ __forceinline__ int get_lda(int i) const { return lda_arr ? lda_arr[i] : lda; }
-    __device__ __forceinline__ int get_ldb(int i) const { return ldb_arr ? ldb_arr[i] : ldb; }
-    __device__ __forceinline__ int get_nrhs(int i) const { return nrhs_arr ? nrhs_arr[i] : nrhs; }
-};
-
 // MPB matrices per block when NW == 1 (one warp each); one matrix per block otherwise.
 template <int NW> struct BlockShape { static constexpr int MPB = (NW == 1) ? 4 : 1; };
+// Blocks per SM the register budget is sized for (<= 128 registers a thread for NC <= 32).
+template <int NC, int NW> struct MinBlocks { static constexpr int value = (NC <= 32 && NW == 1) ? 3 : 1; };
 
 template <typename T, int NC, int NW>
 __device__ __forceinline__ void load_rows(T (&a)[NC], const T* __restrict__ A, int m, int n, int lda, int tid) {
@@ -49,7 +37,7 @@ __device__ __forceinline__ void store_rows(const T (&a)[NC], T* __restrict__ A, 
 // ---------------------------------------------------------------------------
 // getrf
 template <typename T, int NC, int NW>
-__global__ void __launch_bounds__(32 * NW * BlockShape<NW>::MPB)
+__global__ void __launch_bounds__(32 * NW * BlockShape<NW>::MPB, MinBlocks<NC, NW>::value)
 getrf_small_kernel(LuSizes sz, T** dA_array, int** ipiv_array, int* info_array, int batch) {
     constexpr int MPB = BlockShape<NW>::MPB;
     __shared__ SmallLuShared<T, NC, NW> shm[MPB];
@@ -75,7 +63,7 @@ getrf_small_kernel(LuSizes sz, T** dA_array, int** ipiv_array, int* info_array, 
 // ---------------------------------------------------------------------------
 // gesv: getrf + getrs(NoTrans) in one pass. R = RHS columns solved together.
 template <typename T, int NC, int NW, int R>
-__global__ void __launch_bounds__(32 * NW * BlockShape<NW>::MPB)
+__global__ void __launch_bounds__(32 * NW * BlockShape<NW>::MPB, MinBlocks<NC, NW>::value)
 gesv_small_kernel(LuSizes sz, T** dA_array, int** ipiv_array, T** dB_array, int* info_array, int batch) {
     constexpr int MPB = BlockShape<NW>::MPB;
     __shared__ SmallLuShared<T, NC, NW> shm[MPB];
@@ -92,10 +80,6 @@ gesv_small_kernel(LuSizes sz, T** dA_array, int** ipiv_array, T** dB_array, int*
     T* B = dB_array[id];
     T a[NC];
     load_rows<T, NC, NW>(a, A, n, n, lda, tid);
-    // Prefetch the first RHS chunk before factoring so its latency overlaps.
-    T b[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) b[r] = (tid < n && r < nrhs) ? B[tid + (size_t)r * ldb] : T(0);
     int pos, my_ipiv, info;
     small_lu_factor<T, NC, NW>(a, n, n, tid, pos, my_ipiv, info, shm[local]);
     store_rows<T, NC>(a, A, n, n, lda, tid, pos);
@@ -103,12 +87,13 @@ gesv_small_kernel(LuSizes sz, T** dA_array, int** ipiv_array, T** dB_array, int*
     if (tid == 0) info_array[id] = info;
     // Thread tid's b entry (original row tid) belongs at position `pos` of P*b,
     // the same position its LU row landed at, so no permutation pass is needed.
+    // (Every read of B happens before the first barrier of the solve, every
+    // write after its last one, so rows may move between threads in place.)
     for (int c0 = 0; c0 < nrhs; c0 += R) {
-        if (c0 > 0) {
+        T b[R];
 #pragma unroll
-            for (int r = 0; r < R; ++r)
-                b[r] = (tid < n && c0 + r < nrhs) ? B[tid + (size_t)(c0 + r) * ldb] : T(0);
-        }
+        for (int r = 0; r < R; ++r)
+            b[r] = (tid < n && c0 + r < nrhs) ? B[tid + (size_t)(c0 + r) * ldb] : T(0);
         small_lu_solve<T, NC, NW, R>(a, n, pos, b, shm[local]);
         if (tid < n) {
 #pragma unroll
@@ -147,9 +132,9 @@ __device__ __forceinline__ void permute_rhs(T (&b)[R], const int* ipiv, int n, i
     }
 }
 
-template <typename T, int NC, int NW, int R>
-__global__ void __launch_bounds__(32 * NW * BlockShape<NW>::MPB)
-getrs_small_kernel(LuSizes sz, bool trans, T** dA_array, int** ipiv_array, T** dB_array, int batch) {
+template <typename T, int NC, int NW, int R, bool trans>
+__global__ void __launch_bounds__(32 * NW * BlockShape<NW>::MPB, MinBlocks<NC, NW>::value)
+getrs_small_kernel(LuSizes sz, T** dA_array, int** ipiv_array, T** dB_array, int batch) {
     constexpr int MPB = BlockShape<NW>::MPB;
     __shared__ SmallLuShared<T, NC, NW> shm[MPB];
     __shared__ T xch[MPB][32 * NW];
@@ -170,7 +155,7 @@ getrs_small_kernel(LuSizes sz, bool trans, T** dA_array, int** ipiv_array, T** d
         T b[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) b[r] = (tid < n && c0 + r < nrhs) ? B[tid + (size_t)(c0 + r) * ldb] : T(0);
-        if (!trans) {
+        if constexpr (!trans) {
             permute_rhs<T, NC, NW, R>(b, ipiv, n, tid, sh, xch[local], false);
             small_lu_solve<T, NC, NW, R>(a, n, pos, b, sh);
         } else {
@@ -242,10 +227,14 @@ void launch_gesv(const LuSizes& sz, int max_nrhs, T** A, int** ipiv, T** B, int*
 template <typename T, int NC, int NW>
 void launch_getrs(const LuSizes& sz, bool trans, int max_nrhs, T** A, int** ipiv, T** B, int batch, cudaStream_t s) {
     constexpr int MPB = BlockShape<NW>::MPB;
-    if (max_nrhs <= 1)
-        getrs_small_kernel<T, NC, NW, 1><<<ceildiv(batch, MPB), 32 * NW * MPB, 0, s>>>(sz, trans, A, ipiv, B, batch);
-    else
-        getrs_small_kernel<T, NC, NW, 4><<<ceildiv(batch, MPB), 32 * NW * MPB, 0, s>>>(sz, trans, A, ipiv, B, batch);
+    const dim3 grid(ceildiv(batch, MPB)), block(32 * NW * MPB);
+    if (trans) {
+        if (max_nrhs <= 1) getrs_small_kernel<T, NC, NW, 1, true><<<grid, block, 0, s>>>(sz, A, ipiv, B, batch);
+        else getrs_small_kernel<T, NC, NW, 4, true><<<grid, block, 0, s>>>(sz, A, ipiv, B, batch);
+    } else {
+        if (max_nrhs <= 1) getrs_small_kernel<T, NC, NW, 1, false><<<grid, block, 0, s>>>(sz, A, ipiv, B, batch);
+        else getrs_small_kernel<T, NC, NW, 4, false><<<grid, block, 0, s>>>(sz, A, ipiv, B, batch);
+    }
 }
 
 

@@ -154,3 +154,64 @@ def test_config1_full_size(cuda):
     assert np.array_equal(B.cpu().numpy(), OB)
     be = T.backward_error(A_np, B.cpu().numpy(), B_np, 32)
     assert be.max() <= 1e-14
+
+
+# ------------------------------------------------------------------ blocked path (n > 64)
+@pytest.mark.parametrize("n,nrhs,batch", [(65, 1, 64), (96, 3, 64), (100, 4, 48), (128, 1, 48), (129, 5, 32),
+                                          (200, 2, 24), (256, 4, 32), (300, 1, 12), (512, 4, 6), (700, 2, 3),
+                                          (1024, 1, 2)])
+def test_blocked_gesv_bit_identical(cuda, n, nrhs, batch):
+    import magma_b200 as mb
+    A_np, B_np = T.lu_uniform(batch, n, nrhs, seed=4000 + n + nrhs)
+    A, B = to_dev(A_np, cuda), to_dev(B_np, cuda)
+    ipiv, info = mb.dgesv_batched(A, B)
+    OA, OB = A_np.copy(), B_np.copy()
+    oip, oinf = oracle.dgesv_batched(OA, OB)
+    assert np.array_equal(ipiv.cpu().numpy(), oip)
+    assert np.array_equal(info.cpu().numpy(), oinf)
+    assert np.array_equal(A.cpu().numpy(), OA)
+    assert np.array_equal(B.cpu().numpy(), OB)
+    assert T.backward_error(A_np, OB, B_np, n).max() < 30 * EPS
+
+
+@pytest.mark.parametrize("m,n", [(200, 80), (80, 200), (256, 255), (500, 33), (129, 1000), (1024, 64)])
+def test_blocked_getrf_rectangular(cuda, m, n):
+    batch = 5
+    A_np, _ = T.lu_uniform(batch, n, 1, seed=55 + m + n, m=m)
+    LU, ipiv, info = gpu_getrf(A_np, m, cuda)
+    O = A_np.copy()
+    oip, oinf = oracle.dgetrf_batched(O, m)
+    assert np.array_equal(ipiv, oip)
+    assert np.array_equal(info, oinf)
+    assert np.array_equal(LU, O)
+
+
+@pytest.mark.parametrize("n", [90, 256, 333])
+def test_blocked_getrs_trans(cuda, n):
+    import magma_b200 as mb
+    batch, nrhs = 6, 3
+    A_np, B_np = T.lu_uniform(batch, n, nrhs, seed=99 + n)
+    O = A_np.copy()
+    oip, _ = oracle.dgetrf_batched(O, n)
+    for trans in (False, True):
+        Bd = to_dev(B_np, cuda)
+        mb.dgetrs_batched(to_dev(O, cuda), to_dev(oip, cuda), Bd, trans=trans)
+        X = Bd.cpu().numpy()
+        OB = B_np.copy()
+        oracle.dgetrs_batched(O.copy(), oip, OB, trans=trans)
+        if not trans:
+            assert np.array_equal(X, OB)
+        assert np.abs(X - OB).max() <= 64 * n * EPS * max(np.abs(OB).max(), 1.0)
+
+
+def test_blocked_singular(cuda):
+    n = 150
+    A_np, _ = T.lu_uniform(4, n, 1, seed=3)
+    A_np[1, 77, :] = 0.0   # zero column 77 -> info 78
+    A_np[2] = 0.0
+    LU, ipiv, info = gpu_getrf(A_np, n, cuda)
+    O = A_np.copy()
+    oip, oinf = oracle.dgetrf_batched(O, n)
+    assert info[1] == 78 and info[2] == 1
+    assert np.array_equal(info, oinf) and np.array_equal(ipiv, oip)
+    assert np.array_equal(np.nan_to_num(LU), np.nan_to_num(O))
