@@ -137,6 +137,80 @@ magma_int_t magma_dgesv_batched(magma_int_t n, magma_int_t nrhs, double** dA_arr
                                 magma_int_t** dipiv_array, double** dB_array, magma_int_t lddb,
                                 magma_int_t* dinfo_array, magma_int_t batchCount, magma_queue_t queue);
 
+
+/* Mixed precision: FP32 LU + FP64 iterative refinement with FP64 fallback.
+ * No batched counterpart in MAGMA 2.2; per instance it is magma_dsgesv_gpu
+ * (src/zcgesv_gpu.cpp:144-365): stopping test max|R_j| <= max|X_j| ||A||_inf
+ * eps sqrt(n), ITERMAX 30. iter_array[i]: >= 0 iterations used; -2 overflow in
+ * the conversion to single; -3 singular in single; -31 no convergence (also
+ * reported early when the residual stops halving). Negative iter means the
+ * instance was re-solved in double (A then holds the double LU factors and
+ * ipiv the double pivots; info its getrf info). Checks: n -1, nrhs -2,
+ * ldda -4, lddb -7, lddx -9. B is not modified. n <= 512. */
+magma_int_t magma_dsgesv_batched(magma_int_t n, magma_int_t nrhs, double** dA_array, magma_int_t ldda,
+                                 magma_int_t** dipiv_array, double** dB_array, magma_int_t lddb, double** dX_array,
+                                 magma_int_t lddx, magma_int_t* iter_array, magma_int_t* dinfo_array,
+                                 magma_int_t batchCount, magma_queue_t queue);
+
+/* ------------------------------------------------------------------------
+ * Batched Cholesky (fixed size). Lower and Upper are both supported (the
+ * reference's batched potrf handles Lower only, src/zpotf2_vbatched.cpp:32-34).
+ * ---------------------------------------------------------------------- */
+
+/* A = L L^T (or U^T U). src/zpotrf_batched.cpp:291-320: info zeroed first;
+ * uplo -1, n -2, ldda -4. info_array[i] = order of the first non-positive
+ * (or NaN) leading minor, as LAPACK dpotrf. */
+magma_int_t magma_dpotrf_batched(magma_uplo_t uplo, magma_int_t n, double** dA_array, magma_int_t ldda,
+                                 magma_int_t* info_array, magma_int_t batchCount, magma_queue_t queue);
+
+/* src/zpotrs_batched.cpp:71-94 (last failing argument wins: uplo -1, n -2,
+ * nrhs -3, ldda -5, lddb -7). */
+magma_int_t magma_dpotrs_batched(magma_uplo_t uplo, magma_int_t n, magma_int_t nrhs, double** dA_array,
+                                 magma_int_t ldda, double** dB_array, magma_int_t lddb, magma_int_t batchCount,
+                                 magma_queue_t queue);
+
+/* potrf + potrs. src/zposv_batched.cpp:89-141. */
+magma_int_t magma_dposv_batched(magma_uplo_t uplo, magma_int_t n, magma_int_t nrhs, double** dA_array,
+                                magma_int_t ldda, double** dB_array, magma_int_t lddb, magma_int_t* dinfo_array,
+                                magma_int_t batchCount, magma_queue_t queue);
+
+/* ------------------------------------------------------------------------
+ * Variable-size batched Cholesky. n, nrhs, ldda, lddb are device arrays of
+ * batchCount+1 entries. The checked forms reduce the sizes on the device and
+ * read the maxima back (one host synchronisation, as the reference);
+ * _max_nocheck forms take the maxima from the caller and never synchronise.
+ * ---------------------------------------------------------------------- */
+
+/* include/magma_zvbatched.h:66-70, src/zpotrf_vbatched.cpp:335-356; checks as
+ * magmablas/vbatched_check.cu:840-892 (uplo -1, n -2, ldda -4, batchCount -6). */
+magma_int_t magma_dpotrf_vbatched(magma_uplo_t uplo, magma_int_t* n, double** dA_array, magma_int_t* ldda,
+                                  magma_int_t* info_array, magma_int_t batchCount, magma_queue_t queue);
+/* include/magma_zvbatched.h:59-64, src/zpotrf_vbatched.cpp:251-267. */
+magma_int_t magma_dpotrf_vbatched_max_nocheck(magma_uplo_t uplo, magma_int_t* n, double** dA_array,
+                                              magma_int_t* ldda, magma_int_t* info_array, magma_int_t batchCount,
+                                              magma_int_t max_n, magma_queue_t queue);
+
+/* No counterpart in MAGMA 2.2 (potrs is fixed-size only, src/zpotrs_batched.cpp:71);
+ * defined by analogy with magma_dpotrf_vbatched. Checks: uplo -1, n -2, nrhs -3,
+ * ldda -5, lddb -7, batchCount -9. */
+magma_int_t magma_dpotrs_vbatched(magma_uplo_t uplo, magma_int_t* n, magma_int_t* nrhs, double** dA_array,
+                                  magma_int_t* ldda, double** dB_array, magma_int_t* lddb, magma_int_t batchCount,
+                                  magma_queue_t queue);
+magma_int_t magma_dpotrs_vbatched_max_nocheck(magma_uplo_t uplo, magma_int_t* n, magma_int_t* nrhs,
+                                              double** dA_array, magma_int_t* ldda, double** dB_array,
+                                              magma_int_t* lddb, magma_int_t batchCount, magma_int_t max_n,
+                                              magma_int_t max_nrhs, magma_queue_t queue);
+
+/* No counterpart in MAGMA 2.2: potrf + potrs on variable sizes (checks as potrs,
+ * batchCount -10). */
+magma_int_t magma_dposv_vbatched(magma_uplo_t uplo, magma_int_t* n, magma_int_t* nrhs, double** dA_array,
+                                 magma_int_t* ldda, double** dB_array, magma_int_t* lddb, magma_int_t* dinfo_array,
+                                 magma_int_t batchCount, magma_queue_t queue);
+magma_int_t magma_dposv_vbatched_max_nocheck(magma_uplo_t uplo, magma_int_t* n, magma_int_t* nrhs,
+                                             double** dA_array, magma_int_t* ldda, double** dB_array,
+                                             magma_int_t* lddb, magma_int_t* dinfo_array, magma_int_t batchCount,
+                                             magma_int_t max_n, magma_int_t max_nrhs, magma_queue_t queue);
+
 #ifdef __cplusplus
 }
 #endif

@@ -10,9 +10,11 @@ runs in the library's kernels.
 from __future__ import annotations
 
 from . import _lib
-from .api import (Queue, ptr_array, dgetrf_batched, dgetrs_batched, dgesv_batched)
+from .api import (Queue, VarBatch, ptr_array, dgetrf_batched, dgetrs_batched, dgesv_batched, dpotrf_batched,
+                  dpotrs_batched, dposv_batched, dposv_vbatched, dsgesv_batched)
 
-__all__ = ["Queue", "ptr_array", "dgetrf_batched", "dgetrs_batched", "dgesv_batched", "load"]
+__all__ = ["Queue", "VarBatch", "ptr_array", "dgetrf_batched", "dgetrs_batched", "dgesv_batched", "dpotrf_batched",
+           "dpotrs_batched", "dposv_batched", "dposv_vbatched", "dsgesv_batched", "load"]
 
 
 def load():

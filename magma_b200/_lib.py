@@ -59,6 +59,17 @@ SIGNATURES: dict[str, tuple] = {
     "magma_dgetrf_batched": (_i, [_i, _i, _p, _i, _p, _p, _i, _p]),
     "magma_dgetrs_batched": (_i, [_i, _i, _i, _p, _i, _p, _p, _i, _i, _p]),
     "magma_dgesv_batched": (_i, [_i, _i, _p, _i, _p, _p, _i, _p, _i, _p]),
+    "magma_dsgesv_batched": (_i, [_i, _i, _p, _i, _p, _p, _i, _p, _i, _p, _p, _i, _p]),
+    # batched Cholesky
+    "magma_dpotrf_batched": (_i, [_i, _i, _p, _i, _p, _i, _p]),
+    "magma_dpotrs_batched": (_i, [_i, _i, _i, _p, _i, _p, _i, _i, _p]),
+    "magma_dposv_batched": (_i, [_i, _i, _i, _p, _i, _p, _i, _p, _i, _p]),
+    "magma_dpotrf_vbatched": (_i, [_i, _p, _p, _p, _p, _i, _p]),
+    "magma_dpotrf_vbatched_max_nocheck": (_i, [_i, _p, _p, _p, _p, _i, _i, _p]),
+    "magma_dpotrs_vbatched": (_i, [_i, _p, _p, _p, _p, _p, _p, _i, _p]),
+    "magma_dpotrs_vbatched_max_nocheck": (_i, [_i, _p, _p, _p, _p, _p, _p, _i, _i, _i, _p]),
+    "magma_dposv_vbatched": (_i, [_i, _p, _p, _p, _p, _p, _p, _p, _i, _p]),
+    "magma_dposv_vbatched_max_nocheck": (_i, [_i, _p, _p, _p, _p, _p, _p, _p, _i, _i, _i, _p]),
 }
 
 _lib: C.CDLL | None = None
@@ -73,7 +84,10 @@ def load() -> C.CDLL:
         raise RuntimeError(
             f"{LIB_PATH} is missing: build it with `python -m magma_b200.build` "
             "(there is no CPU or library fallback)")
-    lib = C.CDLL(str(LIB_PATH), mode=os.RTLD_NOW | C.RTLD_GLOBAL)
+    # RTLD_LOCAL: the library exports MAGMA's C names; another MAGMA in the
+    # process (torch bundles one in libtorch_cuda_linalg.so) must not resolve
+    # its own calls to these definitions.
+    lib = C.CDLL(str(LIB_PATH), mode=os.RTLD_NOW | os.RTLD_LOCAL)
     for name, (res, args) in SIGNATURES.items():
         fn = getattr(lib, name)
         fn.restype = res

@@ -123,3 +123,138 @@ def dgesv_batched(A: torch.Tensor, B: torch.Tensor, queue: Queue | None = None):
     rc = q.lib.magma_dgesv_batched(n, nrhs, _vp(pA), lda, _vp(pP), _vp(pB), ldb, _vp(info), batch, q.handle)
     _check(rc, "magma_dgesv_batched")
     return ipiv, info
+
+
+# ---------------------------------------------------------------------------- Cholesky
+from ._lib import MagmaLower, MagmaUpper  # noqa: E402
+
+
+def _uplo(upper: bool) -> int:
+    return MagmaUpper if upper else MagmaLower
+
+
+def dpotrf_batched(A: torch.Tensor, upper: bool = False, queue: Queue | None = None) -> torch.Tensor:
+    """Cholesky of each instance of A (batch, n, lda) in place. Returns info (batch,)."""
+    q = queue or default_queue()
+    batch, n, lda = A.shape
+    info = torch.empty(batch, dtype=torch.int32, device=A.device)
+    pA = ptr_array(A)
+    _check(q.lib.magma_dpotrf_batched(_uplo(upper), n, _vp(pA), lda, _vp(info), batch, q.handle),
+           "magma_dpotrf_batched")
+    return info
+
+
+def dpotrs_batched(A: torch.Tensor, B: torch.Tensor, upper: bool = False, queue: Queue | None = None) -> None:
+    q = queue or default_queue()
+    batch, n, lda = A.shape
+    _, nrhs, ldb = B.shape
+    pA, pB = ptr_array(A), ptr_array(B)
+    _check(q.lib.magma_dpotrs_batched(_uplo(upper), n, nrhs, _vp(pA), lda, _vp(pB), ldb, batch, q.handle),
+           "magma_dpotrs_batched")
+
+
+def dposv_batched(A: torch.Tensor, B: torch.Tensor, upper: bool = False, queue: Queue | None = None) -> torch.Tensor:
+    q = queue or default_queue()
+    batch, n, lda = A.shape
+    _, nrhs, ldb = B.shape
+    info = torch.empty(batch, dtype=torch.int32, device=A.device)
+    pA, pB = ptr_array(A), ptr_array(B)
+    _check(q.lib.magma_dposv_batched(_uplo(upper), n, nrhs, _vp(pA), lda, _vp(pB), ldb, _vp(info), batch, q.handle),
+           "magma_dposv_batched")
+    return info
+
+
+class VarBatch:
+    """Variable-size batch packed into one device buffer, with MAGMA's pointer
+    array and per-instance size arrays (batchCount+1 entries, last one scratch).
+
+    ``mats`` are column-major host arrays of shape (cols_i, ld_i)."""
+
+    def __init__(self, mats, device, dtype=torch.float64, align: int = 32):
+        import numpy as np
+
+        self.batch = len(mats)
+        self.shapes = [tuple(m.shape) for m in mats]
+        esz = torch.tensor([], dtype=dtype).element_size()
+        step = max(1, align // esz)
+        sizes = [((m.size + step - 1) // step) * step for m in mats]
+        self.offsets = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64) if mats else np.zeros(0, np.int64)
+        total = int(sum(sizes)) if mats else 1
+        flat = np.zeros(max(total, 1), dtype=np.float64 if dtype == torch.float64 else np.float32)
+        for m, o in zip(mats, self.offsets):
+            flat[o:o + m.size] = m.reshape(-1)
+        self.buf = torch.from_numpy(flat).to(device)
+        self.ptrs = self.buf.data_ptr() + torch.from_numpy(self.offsets * esz).to(device)
+        self.device = device
+
+    def ints(self, values) -> torch.Tensor:
+        """Device int32 array of batch+1 entries (the extra slot is scratch)."""
+        import numpy as np
+
+        v = np.zeros(self.batch + 1, np.int32)
+        v[:self.batch] = values
+        return torch.from_numpy(v).to(self.device)
+
+    def unpack(self):
+        flat = self.buf.cpu().numpy()
+        return [flat[o:o + s[0] * s[1]].reshape(s).copy() for o, s in zip(self.offsets, self.shapes)]
+
+
+def dposv_vbatched(A: VarBatch, B: VarBatch | None, n, nrhs=None, lda=None, ldb=None, upper=False,
+                   factor=True, solve=True, max_sizes=None, queue: Queue | None = None):
+    """Variable-size potrf / potrs / posv through the C ABI. Returns info (device) or None for potrs.
+
+    max_sizes=(max_n, max_nrhs) selects the _max_nocheck entry points."""
+    q = queue or default_queue()
+    batch = A.batch
+    dn = A.ints(n)
+    dlda = A.ints(lda if lda is not None else [s[1] for s in A.shapes])
+    dB = B.ptrs if B is not None else None
+    dnr = A.ints(nrhs) if nrhs is not None else None
+    dldb = A.ints(ldb if ldb is not None else [s[1] for s in B.shapes]) if B is not None else None
+    info = torch.empty(batch + 1, dtype=torch.int32, device=A.device)
+    L = q.lib
+    u = _uplo(upper)
+    if factor and not solve:
+        if max_sizes:
+            rc = L.magma_dpotrf_vbatched_max_nocheck(u, _vp(dn), _vp(A.ptrs), _vp(dlda), _vp(info), batch,
+                                                     max_sizes[0], q.handle)
+        else:
+            rc = L.magma_dpotrf_vbatched(u, _vp(dn), _vp(A.ptrs), _vp(dlda), _vp(info), batch, q.handle)
+        _check(rc, "magma_dpotrf_vbatched")
+        return info[:batch]
+    if solve and not factor:
+        if max_sizes:
+            rc = L.magma_dpotrs_vbatched_max_nocheck(u, _vp(dn), _vp(dnr), _vp(A.ptrs), _vp(dlda), _vp(dB),
+                                                     _vp(dldb), batch, max_sizes[0], max_sizes[1], q.handle)
+        else:
+            rc = L.magma_dpotrs_vbatched(u, _vp(dn), _vp(dnr), _vp(A.ptrs), _vp(dlda), _vp(dB), _vp(dldb), batch,
+                                         q.handle)
+        _check(rc, "magma_dpotrs_vbatched")
+        return None
+    if max_sizes:
+        rc = L.magma_dposv_vbatched_max_nocheck(u, _vp(dn), _vp(dnr), _vp(A.ptrs), _vp(dlda), _vp(dB), _vp(dldb),
+                                                _vp(info), batch, max_sizes[0], max_sizes[1], q.handle)
+    else:
+        rc = L.magma_dposv_vbatched(u, _vp(dn), _vp(dnr), _vp(A.ptrs), _vp(dlda), _vp(dB), _vp(dldb), _vp(info),
+                                    batch, q.handle)
+    _check(rc, "magma_dposv_vbatched")
+    return info[:batch]
+
+
+# -------------------------------------------------------------------- mixed precision
+def dsgesv_batched(A: torch.Tensor, B: torch.Tensor, queue: Queue | None = None):
+    """Mixed-precision solve A_i X_i = B_i (FP32 LU, FP64 refinement, FP64 fallback).
+
+    Returns (X, ipiv, iter, info); A is left unchanged unless iter < 0."""
+    q = queue or default_queue()
+    batch, n, lda = A.shape
+    _, nrhs, ldb = B.shape
+    X = torch.empty((batch, nrhs, n), dtype=torch.float64, device=A.device)
+    ipiv = torch.zeros((batch, n), dtype=torch.int32, device=A.device)
+    it = torch.empty(batch, dtype=torch.int32, device=A.device)
+    info = torch.empty(batch, dtype=torch.int32, device=A.device)
+    pA, pP, pB, pX = ptr_array(A), ptr_array(ipiv), ptr_array(B), ptr_array(X)
+    _check(q.lib.magma_dsgesv_batched(n, nrhs, _vp(pA), lda, _vp(pP), _vp(pB), ldb, _vp(pX), n, _vp(it), _vp(info),
+                                      batch, q.handle), "magma_dsgesv_batched")
+    return X, ipiv, it, info

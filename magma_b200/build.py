@@ -56,7 +56,10 @@ def build(force: bool = False, jobs: int | None = None, extra: list[str] | None 
     with cf.ThreadPoolExecutor(max_workers=jobs or os.cpu_count()) as ex:
         objs = list(ex.map(lambda s: _compile(s, extra), srcs))
     if force or not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
-        cmd = [NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-cudart", "static", "-lpthread"]
+        # -Bsymbolic: calls between the library's own exported MAGMA functions bind
+        # inside the library even when another MAGMA is loaded in the process.
+        cmd = [NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-cudart", "static", "-lpthread",
+               "-Xlinker", "-Bsymbolic"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)

@@ -1,0 +1,266 @@
+// chol.cuh -- Cholesky factorisation (potrf) and solve (potrs) device code.
+//
+// Thread i owns row i of the lower triangle (for uplo = Upper: column i of
+// the upper triangle, i.e. the same numbers transposed). Step k:
+//   every live row publishes its raw column-k entry to shared memory; after
+//   ONE barrier each thread reads d = A(k,k), checks d > 0 (NaN fails, as
+//   LAPACK's "AJJ.LE.ZERO.OR.DISNAN(AJJ)"), forms r = 1/sqrt(d) and applies
+//   A(i,j) = fma(-A(i,k)*r, A(j,k)*r, A(i,j)) for k < j <= i,
+// recomputing the scaled multiplier A(j,k)*r itself instead of waiting for
+// its owner (same operands, same rounding). Every element sees the oracle's
+// operations in the oracle's order, so factors are bit-identical.
+//
+// Replaces the reference's lpout Cholesky (magmablas/zpotf2_kernels_var.cu:80-111:
+// one launch per 8 columns of the largest matrix) and its large-size path
+// (src/zpotrf_vbatched.cpp:19-247: panel + trsm + herk launches, or a host
+// loop over cuBLAS dsyrk on 32 streams).
+#pragma once
+
+#include "small_lu.cuh"
+
+namespace mb200 {
+
+template <typename T> __device__ __forceinline__ T sqrt_rn(T x);
+template <> __device__ __forceinline__ double sqrt_rn<double>(double x) { return __dsqrt_rn(x); }
+template <> __device__ __forceinline__ float sqrt_rn<float>(float x) { return __fsqrt_rn(x); }
+
+template <typename T, int NC>
+struct CholShared {
+    alignas(16) T col[2][NC];   // raw column k (double-buffered)
+    alignas(16) T row[2][NC];   // row broadcast for the transposed solve
+    T rhs[2][4];
+};
+
+// Factor steps k0 .. k0+nsteps-1 on register columns 0..nsteps-1. `a` holds
+// this thread's row (entries of columns k0..k0+NC-1); rows are live when
+// k0 <= tid < n. Returns the 1-based failing step or 0; `done` gets the number
+// of completed steps.
+template <typename T, int NC, int NW>
+__device__ __forceinline__ int chol_panel_steps(T (&a)[NC], int n, int nsteps, int k0, int tid,
+                                                CholShared<T, NC>& sh) {
+    int info = 0;
+    static_for<0, NC>([&](auto kc) {
+        constexpr int k = decltype(kc)::value;
+        if (k >= nsteps || info != 0) return;
+        constexpr int buf = k & 1;
+        const int g = k0 + k;
+        if (tid >= g && tid < n && tid < k0 + NC) sh.col[buf][tid - k0] = a[k];
+        mat_sync<NW>();
+        const T d = sh.col[buf][k];
+        if (!(d > T(0))) {          // not positive definite (or NaN): stop, A(g,g) keeps d
+            info = g + 1;
+            return;
+        }
+        const T s = sqrt_rn(d);
+        const T r = T(1) / s;
+        if (tid == g) a[k] = s;
+        if (tid > g && tid < n) {
+            const T l = a[k] * r;
+            a[k] = l;
+#pragma unroll
+            for (int j = k + 1; j < NC; ++j) a[j] = fma_rn(-l, sh.col[buf][j] * r, a[j]);
+        }
+    });
+    return info;
+}
+
+// Solve L L^T x = b for register-resident rows of L (thread = row, `a` = row).
+// Forward: b(k) /= L(k,k); b(i) = fma(-b(k), L(i,k), b(i)) for i > k.
+// Backward (column sweep of U = L^T): b(k) /= L(k,k); b(i) = fma(-b(k), L(k,i), b(i)) for i < k,
+// with row k of L published through shared memory.
+template <typename T, int NC, int NW, int R>
+__device__ __forceinline__ void chol_solve(const T (&a)[NC], int n, int tid, T (&b)[R], CholShared<T, NC>& sh) {
+    static_for<0, NC>([&](auto kc) {
+        constexpr int k = decltype(kc)::value;
+        if (k >= n) return;
+        constexpr int buf = k & 1;
+        if (tid == k) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) { b[r] = b[r] / a[k]; sh.rhs[buf][r] = b[r]; }
+        }
+        mat_sync<NW>();
+        if (tid > k && tid < n) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) b[r] = fma_rn(-sh.rhs[buf][r], a[k], b[r]);
+        }
+    });
+    static_for<0, NC>([&](auto ic) {
+        constexpr int k = NC - 1 - decltype(ic)::value;
+        if (k >= n) return;
+        constexpr int buf = (k + 1) & 1;
+        if (tid == k) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) { b[r] = b[r] / a[k]; sh.rhs[buf][r] = b[r]; }
+#pragma unroll
+            for (int j = 0; j < k; ++j) sh.row[buf][j] = a[j];
+        }
+        mat_sync<NW>();
+        if (tid < k) {
+            const T lki = sh.row[buf][tid];
+#pragma unroll
+            for (int r = 0; r < R; ++r) b[r] = fma_rn(-sh.rhs[buf][r], lki, b[r]);
+        }
+    });
+}
+
+// Element (i, j) of the stored triangle: lower -> A(i, j), upper -> A(j, i).
+template <typename T>
+__device__ __forceinline__ T& tri(T* A, int lda, bool upper, int i, int j) {
+    return upper ? A[j + (size_t)i * lda] : A[i + (size_t)j * lda];
+}
+
+// ---------------------------------------------------------------------------
+// Blocked right-looking Cholesky of one matrix per thread block (n <= NT).
+template <typename T, int NB, int NT, int CW>
+struct BlockedCholShared {
+    CholShared<T, NB> p;
+    T L[CW][NB + 1];     // panel rows j0..j0+CW-1 for the trailing update
+};
+
+template <typename T, int NB, int NT, int CW, int CB>
+__device__ int blocked_potrf(T* __restrict__ A, int n, int lda, bool upper, BlockedCholShared<T, NB, NT, CW>& sh) {
+    constexpr int NW = NT / 32;
+    const int tid = threadIdx.x;
+    for (int k0 = 0; k0 < n; k0 += NB) {
+        const int nbp = min(NB, n - k0);
+        const bool live = (tid >= k0 && tid < n);
+        T a[NB];
+#pragma unroll
+        for (int c = 0; c < NB; ++c)
+            a[c] = (live && c < nbp && k0 + c <= tid) ? tri(A, lda, upper, tid, k0 + c) : T(0);
+        const int info = chol_panel_steps<T, NB, NW>(a, n, nbp, k0, tid, sh.p);
+        if (live) {
+#pragma unroll
+            for (int c = 0; c < NB; ++c)
+                if (c < nbp && k0 + c <= tid) tri(A, lda, upper, tid, k0 + c) = a[c];
+        }
+        if (info) return info;
+        // trailing update of the lower triangle: A(i, j) -= sum_r L(i, r) L(j, r), j <= i
+        for (int j0 = k0 + nbp; j0 < n; j0 += CW) {
+            const int cw = min(CW, n - j0);
+            __syncthreads();   // previous readers of sh.L done
+            if (tid >= j0 && tid < j0 + cw) {
+#pragma unroll
+                for (int r = 0; r < NB; ++r) sh.L[tid - j0][r] = a[r];
+            }
+            __syncthreads();
+            if (tid >= j0 && tid < n) {
+                const int cmax = min(cw, tid - j0 + 1);   // columns j0 .. min(j0+cw-1, tid)
+                for (int c0 = 0; c0 < cmax; c0 += CB) {
+                    T acc[CB];
+#pragma unroll
+                    for (int c = 0; c < CB; ++c) acc[c] = (c0 + c < cmax) ? tri(A, lda, upper, tid, j0 + c0 + c) : T(0);
+                    static_for<0, NB>([&](auto rc) {
+                        constexpr int r = decltype(rc)::value;
+                        if (r < nbp) {
+                            const T l = a[r];
+#pragma unroll
+                            for (int c = 0; c < CB; ++c) acc[c] = fma_rn(-l, sh.L[c0 + c][r], acc[c]);
+                        }
+                    });
+#pragma unroll
+                    for (int c = 0; c < CB; ++c)
+                        if (c0 + c < cmax) tri(A, lda, upper, tid, j0 + c0 + c) = acc[c];
+                }
+            }
+        }
+        __syncthreads();
+    }
+    return 0;
+}
+
+// Blocked L L^T x = b for one matrix per thread block (n <= NT), R RHS at a time.
+template <typename T, int NT, int R>
+struct BlockedCholRsShared {
+    T sb[32][R];
+    T D[32][33];
+};
+
+template <typename T, int NT, int R>
+__device__ void blocked_potrs(const T* __restrict__ A, int n, int lda, bool upper, T* __restrict__ B, int nrhs,
+                              int ldb, BlockedCholRsShared<T, NT, R>& sh) {
+    const int t = threadIdx.x, lane = t & 31;
+    const int nblk = (n + 31) / 32;
+    auto L = [&](int i, int j) -> T { return upper ? A[j + (size_t)i * lda] : A[i + (size_t)j * lda]; };
+    for (int c0 = 0; c0 < nrhs; c0 += R) {
+        T b[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) b[r] = (t < n && c0 + r < nrhs) ? B[t + (size_t)(c0 + r) * ldb] : T(0);
+        // forward: L y = b, blocks ascending
+        for (int J = 0; J < nblk; ++J) {
+            const int j0 = J * 32, j1 = min(n, j0 + 32);
+            __syncthreads();
+            if ((t >> 5) == J) {
+#pragma unroll
+                for (int c = 0; c < 32; ++c)
+                    if (j0 + c < j1 && j0 + lane < j1 && c <= lane) sh.D[lane][c] = L(j0 + lane, j0 + c);
+                __syncwarp();
+                for (int k = j0; k < j1; ++k) {
+                    if (t == k) {
+#pragma unroll
+                        for (int r = 0; r < R; ++r) { b[r] = b[r] / sh.D[k - j0][k - j0]; sh.sb[k - j0][r] = b[r]; }
+                    }
+                    __syncwarp();
+                    if (t > k && t < j1) {
+                        const T l = sh.D[t - j0][k - j0];
+#pragma unroll
+                        for (int r = 0; r < R; ++r) b[r] = fma_rn(-sh.sb[k - j0][r], l, b[r]);
+                    }
+                }
+            }
+            __syncthreads();
+            if (t >= j1 && t < n) {
+#pragma unroll
+                for (int kk = 0; kk < 32; ++kk) {
+                    if (j0 + kk < j1) {
+                        const T l = L(t, j0 + kk);
+#pragma unroll
+                        for (int r = 0; r < R; ++r) b[r] = fma_rn(-sh.sb[kk][r], l, b[r]);
+                    }
+                }
+            }
+        }
+        // backward: L^T x = y, blocks descending (column sweep of U = L^T)
+        for (int J = nblk - 1; J >= 0; --J) {
+            const int j0 = J * 32, j1 = min(n, j0 + 32);
+            __syncthreads();
+            if ((t >> 5) == J) {
+#pragma unroll
+                for (int c = 0; c < 32; ++c)
+                    if (j0 + c < j1 && j0 + lane < j1 && c <= lane) sh.D[lane][c] = L(j0 + lane, j0 + c);
+                __syncwarp();
+                for (int k = j1 - 1; k >= j0; --k) {
+                    if (t == k) {
+#pragma unroll
+                        for (int r = 0; r < R; ++r) { b[r] = b[r] / sh.D[k - j0][k - j0]; sh.sb[k - j0][r] = b[r]; }
+                    }
+                    __syncwarp();
+                    if (t >= j0 && t < k) {
+                        const T u = sh.D[k - j0][t - j0];   // U(t, k) = L(k, t)
+#pragma unroll
+                        for (int r = 0; r < R; ++r) b[r] = fma_rn(-sh.sb[k - j0][r], u, b[r]);
+                    }
+                }
+            }
+            __syncthreads();
+            if (t < j0) {
+#pragma unroll
+                for (int kk = 31; kk >= 0; --kk) {
+                    if (j0 + kk < j1) {
+                        const T u = L(j0 + kk, t);
+#pragma unroll
+                        for (int r = 0; r < R; ++r) b[r] = fma_rn(-sh.sb[kk][r], u, b[r]);
+                    }
+                }
+            }
+        }
+        if (t < n) {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                if (c0 + r < nrhs) B[t + (size_t)(c0 + r) * ldb] = b[r];
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace mb200

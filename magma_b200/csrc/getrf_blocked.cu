@@ -1,78 +1,95 @@
 // getrf_blocked.cu -- kernels and host dispatch of the blocked batched LU
-// (one matrix per thread block, up to 1024 rows): getrf, getrs, and the
-// fixed/variable-size drivers' entry into them.
+// (one matrix per thread block, up to 1024 rows): getrf and getrs.
 #include "internal.h"
 #include "blocked_lu.cuh"
 #include "getrs_blocked.cuh"
 #include "batched_kernels.h"
 #include "lu_sizes.h"
+#include "vbatched.h"
 
 namespace mb200 {
 
 template <typename T, int NB, int NT, int CW, int CB>
 __global__ void __launch_bounds__(NT)
-getrf_blocked_kernel(LuSizes sz, T** dA_array, int** ipiv_array, int* info_array, int batch) {
+getrf_blocked_kernel(WorkList wl, LuSizes sz, T** dA_array, int** ipiv_array, int* info_array) {
     __shared__ BlockedLuShared<T, NB, NT, CW> sh;
-    const int id = blockIdx.x;
-    if (id >= batch) return;
-    const int m = sz.get_m(id), n = sz.get_n(id), lda = sz.get_lda(id);
-    if (m <= 0 || n <= 0) {
-        if (threadIdx.x == 0) info_array[id] = 0;
-        return;
+    for (int w = blockIdx.x; w < wl.size(); w += gridDim.x) {
+        const int id = wl.at(w);
+        const int m = sz.get_m(id), n = sz.get_n(id), lda = sz.get_lda(id);
+        int info = 0;
+        if (m > 0 && n > 0) blocked_getrf<T, NB, NT, CW, CB>(dA_array[id], m, n, lda, ipiv_array[id], info, sh);
+        if (threadIdx.x == 0) info_array[id] = info;
+        __syncthreads();
     }
-    int info;
-    blocked_getrf<T, NB, NT, CW, CB>(dA_array[id], m, n, lda, ipiv_array[id], info, sh);
-    if (threadIdx.x == 0) info_array[id] = info;
 }
 
 template <typename T, int NT, int R>
 __global__ void __launch_bounds__(NT)
-getrs_blocked_kernel(LuSizes sz, bool trans, T** dA_array, int** ipiv_array, T** dB_array, int batch) {
+getrs_blocked_kernel(WorkList wl, LuSizes sz, bool trans, T** dA_array, int** ipiv_array, T** dB_array) {
     __shared__ BlockedRsShared<T, NT, R> sh;
-    const int id = blockIdx.x;
-    if (id >= batch) return;
-    const int n = sz.get_n(id), lda = sz.get_lda(id), ldb = sz.get_ldb(id), nrhs = sz.get_nrhs(id);
-    if (n <= 0 || nrhs <= 0) return;
-    blocked_getrs<T, NT, R>(trans, dA_array[id], n, lda, ipiv_array[id], dB_array[id], nrhs, ldb, sh);
+    for (int w = blockIdx.x; w < wl.size(); w += gridDim.x) {
+        const int id = wl.at(w);
+        const int n = sz.get_n(id), lda = sz.get_lda(id), ldb = sz.get_ldb(id), nrhs = sz.get_nrhs(id);
+        if (n > 0 && nrhs > 0)
+            blocked_getrs<T, NT, R>(trans, dA_array[id], n, lda, ipiv_array[id], dB_array[id], nrhs, ldb, sh);
+        __syncthreads();
+    }
 }
 
 bool blocked_lu_supported(int max_m) { return max_m <= 1024; }
 
-template <typename T>
-magma_int_t getrf_blocked(int m, int n, const int* m_arr, const int* n_arr, int lda, const int* lda_arr,
-                          int max_m, int max_n, T** A, int** ipiv, int* info, int batch, cudaStream_t s) {
-    (void)max_n;
-    LuSizes sz{m, n, lda, 0, 0, m_arr, n_arr, lda_arr, nullptr, nullptr};
-    if (max_m <= 128)
-        getrf_blocked_kernel<T, 32, 128, 128, 16><<<batch, 128, 0, s>>>(sz, A, ipiv, info, batch);
-    else if (max_m <= 256)
-        getrf_blocked_kernel<T, 32, 256, 128, 8><<<batch, 256, 0, s>>>(sz, A, ipiv, info, batch);
-    else if (max_m <= 512)
-        getrf_blocked_kernel<T, 32, 512, 128, 8><<<batch, 512, 0, s>>>(sz, A, ipiv, info, batch);
-    else
-        getrf_blocked_kernel<T, 16, 1024, 128, 4><<<batch, 1024, 0, s>>>(sz, A, ipiv, info, batch);
-    return launch_status();
+template <typename K>
+static int blocked_grid(K kernel, int threads, int bound, bool persistent) {
+    if (!persistent) return std::max(1, bound);
+    return std::max(1, std::min(bound, resident_blocks((const void*)kernel, threads, 0)));
+}
+
+template <typename T, int NB, int NT, int CW, int CB>
+static void launch_getrf_blocked(const WorkList& wl, int bound, bool persistent, const LuSizes& sz, T** A, int** ipiv,
+                                 int* info, cudaStream_t s) {
+    auto k = getrf_blocked_kernel<T, NB, NT, CW, CB>;
+    k<<<blocked_grid(k, NT, bound, persistent), NT, 0, s>>>(wl, sz, A, ipiv, info);
 }
 
 template <typename T>
-magma_int_t getrs_blocked(bool trans, int n, const int* n_arr, int nrhs, const int* nrhs_arr, int lda,
-                          const int* lda_arr, int ldb, const int* ldb_arr, int max_n, int max_nrhs,
-                          T** A, int** ipiv, T** B, int batch, cudaStream_t s) {
-    LuSizes sz{n, n, lda, ldb, nrhs, n_arr, n_arr, lda_arr, ldb_arr, nrhs_arr};
-#define MB200_RS(NT_)                                                                                  \
-    if (max_nrhs <= 1) getrs_blocked_kernel<T, NT_, 1><<<batch, NT_, 0, s>>>(sz, trans, A, ipiv, B, batch); \
-    else getrs_blocked_kernel<T, NT_, 4><<<batch, NT_, 0, s>>>(sz, trans, A, ipiv, B, batch);
-    if (max_n <= 128) { MB200_RS(128) }
-    else if (max_n <= 256) { MB200_RS(256) }
-    else if (max_n <= 512) { MB200_RS(512) }
-    else { MB200_RS(1024) }
-#undef MB200_RS
+magma_int_t getrf_blocked(const WorkList& wl, int bound, bool persistent, const LuSizes& sz, int max_m, T** A,
+                          int** ipiv, int* info, cudaStream_t s) {
+    if (max_m <= 128) launch_getrf_blocked<T, 32, 128, 128, 16>(wl, bound, persistent, sz, A, ipiv, info, s);
+    else if (max_m <= 256) launch_getrf_blocked<T, 32, 256, 128, 8>(wl, bound, persistent, sz, A, ipiv, info, s);
+    else if (max_m <= 512) launch_getrf_blocked<T, 32, 512, 128, 8>(wl, bound, persistent, sz, A, ipiv, info, s);
+    else launch_getrf_blocked<T, 16, 1024, 128, 4>(wl, bound, persistent, sz, A, ipiv, info, s);
     return launch_status();
 }
 
-template magma_int_t getrf_blocked<double>(int, int, const int*, const int*, int, const int*, int, int, double**, int**, int*, int, cudaStream_t);
-template magma_int_t getrf_blocked<float>(int, int, const int*, const int*, int, const int*, int, int, float**, int**, int*, int, cudaStream_t);
-template magma_int_t getrs_blocked<double>(bool, int, const int*, int, const int*, int, const int*, int, const int*, int, int, double**, int**, double**, int, cudaStream_t);
-template magma_int_t getrs_blocked<float>(bool, int, const int*, int, const int*, int, const int*, int, const int*, int, int, float**, int**, float**, int, cudaStream_t);
+template <typename T, int NT>
+static void launch_getrs_blocked(const WorkList& wl, int bound, bool persistent, const LuSizes& sz, bool trans,
+                                 int max_nrhs, T** A, int** ipiv, T** B, cudaStream_t s) {
+    if (max_nrhs <= 1) {
+        auto k = getrs_blocked_kernel<T, NT, 1>;
+        k<<<blocked_grid(k, NT, bound, persistent), NT, 0, s>>>(wl, sz, trans, A, ipiv, B);
+    } else {
+        auto k = getrs_blocked_kernel<T, NT, 4>;
+        k<<<blocked_grid(k, NT, bound, persistent), NT, 0, s>>>(wl, sz, trans, A, ipiv, B);
+    }
+}
+
+template <typename T>
+magma_int_t getrs_blocked(const WorkList& wl, int bound, bool persistent, bool trans, const LuSizes& sz, int max_n,
+                          int max_nrhs, T** A, int** ipiv, T** B, cudaStream_t s) {
+    if (max_n <= 128) launch_getrs_blocked<T, 128>(wl, bound, persistent, sz, trans, max_nrhs, A, ipiv, B, s);
+    else if (max_n <= 256) launch_getrs_blocked<T, 256>(wl, bound, persistent, sz, trans, max_nrhs, A, ipiv, B, s);
+    else if (max_n <= 512) launch_getrs_blocked<T, 512>(wl, bound, persistent, sz, trans, max_nrhs, A, ipiv, B, s);
+    else launch_getrs_blocked<T, 1024>(wl, bound, persistent, sz, trans, max_nrhs, A, ipiv, B, s);
+    return launch_status();
+}
+
+template magma_int_t getrf_blocked<double>(const WorkList&, int, bool, const LuSizes&, int, double**, int**, int*,
+                                           cudaStream_t);
+template magma_int_t getrf_blocked<float>(const WorkList&, int, bool, const LuSizes&, int, float**, int**, int*,
+                                          cudaStream_t);
+template magma_int_t getrs_blocked<double>(const WorkList&, int, bool, bool, const LuSizes&, int, int, double**, int**,
+                                           double**, cudaStream_t);
+template magma_int_t getrs_blocked<float>(const WorkList&, int, bool, bool, const LuSizes&, int, int, float**, int**,
+                                          float**, cudaStream_t);
 
 }  // namespace mb200

@@ -25,12 +25,12 @@ magma_int_t magma_dgetrf_batched(magma_int_t m, magma_int_t n, double** dA_array
         return arginfo;
     }
     if (m == 0 || n == 0 || batchCount <= 0) return 0;
+    const WorkList wl{nullptr, nullptr, batchCount};
+    const LuSizes sz{m, n, ldda, 0, 0, nullptr, nullptr, nullptr, nullptr, nullptr};
     if (small_lu_supported(m, n))
-        return getrf_small<double>(m, n, nullptr, nullptr, ldda, nullptr, m, n, dA_array,
-                                   ipiv_array, info_array, batchCount, queue->stream);
+        return getrf_small<double>(wl, batchCount, false, sz, m, n, dA_array, ipiv_array, info_array, queue->stream);
     if (blocked_lu_supported(m))
-        return getrf_blocked<double>(m, n, nullptr, nullptr, ldda, nullptr, m, n, dA_array,
-                                     ipiv_array, info_array, batchCount, queue->stream);
+        return getrf_blocked<double>(wl, batchCount, false, sz, m, dA_array, ipiv_array, info_array, queue->stream);
     return MAGMA_ERR_NOT_SUPPORTED;
 }
 
@@ -52,12 +52,14 @@ magma_int_t magma_dgetrs_batched(magma_trans_t trans, magma_int_t n, magma_int_t
         return info;
     }
     if (n == 0 || nrhs == 0 || batchCount <= 0) return 0;
+    const WorkList wl{nullptr, nullptr, batchCount};
+    const LuSizes sz{n, n, ldda, lddb, nrhs, nullptr, nullptr, nullptr, nullptr, nullptr};
     if (small_lu_supported(n, n))
-        return getrs_small<double>(!notran, n, nullptr, nrhs, nullptr, ldda, nullptr, lddb, nullptr, n,
-                                   nrhs, dA_array, dipiv_array, dB_array, batchCount, queue->stream);
+        return getrs_small<double>(wl, batchCount, false, !notran, sz, n, nrhs, dA_array, dipiv_array, dB_array,
+                                   queue->stream);
     if (blocked_lu_supported(n))
-        return getrs_blocked<double>(!notran, n, nullptr, nrhs, nullptr, ldda, nullptr, lddb, nullptr, n,
-                                     nrhs, dA_array, dipiv_array, dB_array, batchCount, queue->stream);
+        return getrs_blocked<double>(wl, batchCount, false, !notran, sz, n, nrhs, dA_array, dipiv_array, dB_array,
+                                     queue->stream);
     return MAGMA_ERR_NOT_SUPPORTED;
 }
 
@@ -76,13 +78,43 @@ magma_int_t magma_dgesv_batched(magma_int_t n, magma_int_t nrhs, double** dA_arr
         return info;
     }
     if (n == 0 || nrhs == 0 || batchCount <= 0) return 0;
-    if (small_lu_supported(n, n))
-        return gesv_small<double>(n, nullptr, nrhs, nullptr, ldda, nullptr, lddb, nullptr, n, nrhs,
-                                  dA_array, dipiv_array, dB_array, dinfo_array, batchCount, queue->stream);
+    if (small_lu_supported(n, n)) {
+        const WorkList wl{nullptr, nullptr, batchCount};
+        const LuSizes sz{n, n, ldda, lddb, nrhs, nullptr, nullptr, nullptr, nullptr, nullptr};
+        return gesv_small<double>(wl, batchCount, false, sz, n, nrhs, dA_array, dipiv_array, dB_array, dinfo_array,
+                                  queue->stream);
+    }
     info = magma_dgetrf_batched(n, n, dA_array, ldda, dipiv_array, dinfo_array, batchCount, queue);
     if (info != MAGMA_SUCCESS) return info;
     return magma_dgetrs_batched(MagmaNoTrans, n, nrhs, dA_array, ldda, dipiv_array, dB_array, lddb,
                                 batchCount, queue);
+}
+
+// No batched counterpart in MAGMA 2.2 (mixed precision exists only for one
+// matrix, magma_dsgesv_gpu, src/zcgesv_gpu.cpp:144). Arguments follow
+// magma_dgesv_batched plus the solution and iteration arrays; checks:
+// n -1, nrhs -2, ldda -4, lddb -7, lddx -9. iter_array[i] as magma_dsgesv_gpu:
+// >= 0 refinement iterations used, -2 overflow converting to single, -3
+// singular in single precision, -31 refinement did not converge; for negative
+// iter the solve was redone in double precision (A then holds the double
+// factors, info the double getrf info).
+magma_int_t magma_dsgesv_batched(magma_int_t n, magma_int_t nrhs, double** dA_array, magma_int_t ldda,
+                                 magma_int_t** dipiv_array, double** dB_array, magma_int_t lddb, double** dX_array,
+                                 magma_int_t lddx, magma_int_t* iter_array, magma_int_t* dinfo_array,
+                                 magma_int_t batchCount, magma_queue_t queue) {
+    magma_int_t info = 0;
+    if (n < 0) info = -1;
+    else if (nrhs < 0) info = -2;
+    else if (ldda < std::max(1, n)) info = -4;
+    else if (lddb < std::max(1, n)) info = -7;
+    else if (lddx < std::max(1, n)) info = -9;
+    if (info != 0) {
+        magma_xerbla(__func__, -info);
+        return info;
+    }
+    if (n == 0 || nrhs == 0 || batchCount <= 0) return 0;
+    return dsgesv_batched(n, nrhs, dA_array, ldda, dipiv_array, dB_array, lddb, dX_array, lddx, iter_array,
+                          dinfo_array, batchCount, queue);
 }
 
 }  // extern "C"

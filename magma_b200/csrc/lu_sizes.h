@@ -19,3 +19,19 @@ struct LuSizes {
 };
 
 }  // namespace mb200
+
+namespace mb200 {
+
+// The instances a launch works on: either 0..total-1, or the entries of a
+// device list (one size bucket of a variable-size batch) whose length the
+// device holds in *count. Kernels walk it with a grid-stride loop, so a
+// launch never needs the length on the host.
+struct WorkList {
+    const int* list;
+    const int* count;
+    int total;
+    __device__ __forceinline__ int size() const { return count ? *count : total; }
+    __device__ __forceinline__ int at(int w) const { return list ? list[w] : w; }
+};
+
+}  // namespace mb200

@@ -38,43 +38,46 @@ __device__ __forceinline__ void store_rows(const T (&a)[NC], T* __restrict__ A, 
 // getrf
 template <typename T, int NC, int NW>
 __global__ void __launch_bounds__(32 * NW * BlockShape<NW>::MPB, MinBlocks<NC, NW>::value)
-getrf_small_kernel(LuSizes sz, T** dA_array, int** ipiv_array, int* info_array, int batch) {
+getrf_small_kernel(WorkList wl, LuSizes sz, T** dA_array, int** ipiv_array, int* info_array) {
     constexpr int MPB = BlockShape<NW>::MPB;
     __shared__ SmallLuShared<T, NC, NW> shm[MPB];
     const int local = (NW == 1) ? (threadIdx.x >> 5) : 0;
     const int tid = (NW == 1) ? (threadIdx.x & 31) : threadIdx.x;
-    const int id = blockIdx.x * MPB + local;
-    if (id >= batch) return;   // NW==1: whole warp leaves together; NW>1: whole block
-    const int m = sz.get_m(id), n = sz.get_n(id), lda = sz.get_lda(id);
-    if (m <= 0 || n <= 0) {
-        if (tid == 0) info_array[id] = 0;
-        return;
+    // NW == 1: each warp walks its own items; NW > 1: the block walks them together
+    for (int w = blockIdx.x * MPB + local; w < wl.size(); w += gridDim.x * MPB) {
+        const int id = wl.at(w);
+        const int m = sz.get_m(id), n = sz.get_n(id), lda = sz.get_lda(id);
+        if (m <= 0 || n <= 0) {
+            if (tid == 0) info_array[id] = 0;
+            continue;
+        }
+        T* A = dA_array[id];
+        T a[NC];
+        load_rows<T, NC, NW>(a, A, m, n, lda, tid);
+        int pos, my_ipiv, info;
+        small_lu_factor<T, NC, NW>(a, m, n, tid, pos, my_ipiv, info, shm[local]);
+        store_rows<T, NC>(a, A, m, n, lda, tid, pos);
+        if (tid < min(m, n)) ipiv_array[id][tid] = my_ipiv;
+        if (tid == 0) info_array[id] = info;
+        mat_sync<NW>();
     }
-    T* A = dA_array[id];
-    T a[NC];
-    load_rows<T, NC, NW>(a, A, m, n, lda, tid);
-    int pos, my_ipiv, info;
-    small_lu_factor<T, NC, NW>(a, m, n, tid, pos, my_ipiv, info, shm[local]);
-    store_rows<T, NC>(a, A, m, n, lda, tid, pos);
-    if (tid < min(m, n)) ipiv_array[id][tid] = my_ipiv;
-    if (tid == 0) info_array[id] = info;
 }
 
 // ---------------------------------------------------------------------------
 // gesv: getrf + getrs(NoTrans) in one pass. R = RHS columns solved together.
 template <typename T, int NC, int NW, int R>
 __global__ void __launch_bounds__(32 * NW * BlockShape<NW>::MPB, MinBlocks<NC, NW>::value)
-gesv_small_kernel(LuSizes sz, T** dA_array, int** ipiv_array, T** dB_array, int* info_array, int batch) {
+gesv_small_kernel(WorkList wl, LuSizes sz, T** dA_array, int** ipiv_array, T** dB_array, int* info_array) {
     constexpr int MPB = BlockShape<NW>::MPB;
     __shared__ SmallLuShared<T, NC, NW> shm[MPB];
     const int local = (NW == 1) ? (threadIdx.x >> 5) : 0;
     const int tid = (NW == 1) ? (threadIdx.x & 31) : threadIdx.x;
-    const int id = blockIdx.x * MPB + local;
-    if (id >= batch) return;
+    for (int w = blockIdx.x * MPB + local; w < wl.size(); w += gridDim.x * MPB) {
+    const int id = wl.at(w);
     const int n = sz.get_n(id), lda = sz.get_lda(id), ldb = sz.get_ldb(id), nrhs = sz.get_nrhs(id);
     if (n <= 0) {
         if (tid == 0) info_array[id] = 0;
-        return;
+        continue;
     }
     T* A = dA_array[id];
     T* B = dB_array[id];
@@ -100,6 +103,8 @@ gesv_small_kernel(LuSizes sz, T** dA_array, int** ipiv_array, T** dB_array, int*
             for (int r = 0; r < R; ++r)
                 if (c0 + r < nrhs) B[pos + (size_t)(c0 + r) * ldb] = b[r];
         }
+    }
+    mat_sync<NW>();
     }
 }
 
@@ -134,16 +139,16 @@ __device__ __forceinline__ void permute_rhs(T (&b)[R], const int* ipiv, int n, i
 
 template <typename T, int NC, int NW, int R, bool trans>
 __global__ void __launch_bounds__(32 * NW * BlockShape<NW>::MPB, MinBlocks<NC, NW>::value)
-getrs_small_kernel(LuSizes sz, T** dA_array, int** ipiv_array, T** dB_array, int batch) {
+getrs_small_kernel(WorkList wl, LuSizes sz, T** dA_array, int** ipiv_array, T** dB_array) {
     constexpr int MPB = BlockShape<NW>::MPB;
     __shared__ SmallLuShared<T, NC, NW> shm[MPB];
     __shared__ T xch[MPB][32 * NW];
     const int local = (NW == 1) ? (threadIdx.x >> 5) : 0;
     const int tid = (NW == 1) ? (threadIdx.x & 31) : threadIdx.x;
-    const int id = blockIdx.x * MPB + local;
-    if (id >= batch) return;
+    for (int w = blockIdx.x * MPB + local; w < wl.size(); w += gridDim.x * MPB) {
+    const int id = wl.at(w);
     const int n = sz.get_n(id), lda = sz.get_lda(id), ldb = sz.get_ldb(id), nrhs = sz.get_nrhs(id);
-    if (n <= 0 || nrhs <= 0) return;
+    if (n <= 0 || nrhs <= 0) continue;
     const T* A = dA_array[id];
     T* B = dB_array[id];
     const int* ipiv = ipiv_array[id];
@@ -204,48 +209,54 @@ getrs_small_kernel(LuSizes sz, T** dA_array, int** ipiv_array, T** dB_array, int
         }
         mat_sync<NW>();
     }
+    }
 }
 
 // ---------------------------------------------------------------------------
 // Launchers, explicitly instantiated per (NC, NW) in small_lu_inst_*.cu so the
 // variants compile in parallel.
 template <typename T, int NC, int NW>
-void launch_getrf(const LuSizes& sz, T** A, int** ipiv, int* info, int batch, cudaStream_t s) {
+void launch_getrf(const WorkList& wl, int grid, const LuSizes& sz, T** A, int** ipiv, int* info, cudaStream_t s) {
     constexpr int MPB = BlockShape<NW>::MPB;
-    getrf_small_kernel<T, NC, NW><<<ceildiv(batch, MPB), 32 * NW * MPB, 0, s>>>(sz, A, ipiv, info, batch);
+    getrf_small_kernel<T, NC, NW><<<grid, 32 * NW * MPB, 0, s>>>(wl, sz, A, ipiv, info);
 }
 
 template <typename T, int NC, int NW>
-void launch_gesv(const LuSizes& sz, int max_nrhs, T** A, int** ipiv, T** B, int* info, int batch, cudaStream_t s) {
+void launch_gesv(const WorkList& wl, int grid, const LuSizes& sz, int max_nrhs, T** A, int** ipiv, T** B, int* info,
+                 cudaStream_t s) {
     constexpr int MPB = BlockShape<NW>::MPB;
     if (max_nrhs <= 1)
-        gesv_small_kernel<T, NC, NW, 1><<<ceildiv(batch, MPB), 32 * NW * MPB, 0, s>>>(sz, A, ipiv, B, info, batch);
+        gesv_small_kernel<T, NC, NW, 1><<<grid, 32 * NW * MPB, 0, s>>>(wl, sz, A, ipiv, B, info);
     else
-        gesv_small_kernel<T, NC, NW, 4><<<ceildiv(batch, MPB), 32 * NW * MPB, 0, s>>>(sz, A, ipiv, B, info, batch);
+        gesv_small_kernel<T, NC, NW, 4><<<grid, 32 * NW * MPB, 0, s>>>(wl, sz, A, ipiv, B, info);
 }
 
 template <typename T, int NC, int NW>
-void launch_getrs(const LuSizes& sz, bool trans, int max_nrhs, T** A, int** ipiv, T** B, int batch, cudaStream_t s) {
+void launch_getrs(const WorkList& wl, int grid, const LuSizes& sz, bool trans, int max_nrhs, T** A, int** ipiv, T** B,
+                  cudaStream_t s) {
     constexpr int MPB = BlockShape<NW>::MPB;
-    const dim3 grid(ceildiv(batch, MPB)), block(32 * NW * MPB);
+    const dim3 block(32 * NW * MPB);
     if (trans) {
-        if (max_nrhs <= 1) getrs_small_kernel<T, NC, NW, 1, true><<<grid, block, 0, s>>>(sz, A, ipiv, B, batch);
-        else getrs_small_kernel<T, NC, NW, 4, true><<<grid, block, 0, s>>>(sz, A, ipiv, B, batch);
+        if (max_nrhs <= 1) getrs_small_kernel<T, NC, NW, 1, true><<<grid, block, 0, s>>>(wl, sz, A, ipiv, B);
+        else getrs_small_kernel<T, NC, NW, 4, true><<<grid, block, 0, s>>>(wl, sz, A, ipiv, B);
     } else {
-        if (max_nrhs <= 1) getrs_small_kernel<T, NC, NW, 1, false><<<grid, block, 0, s>>>(sz, A, ipiv, B, batch);
-        else getrs_small_kernel<T, NC, NW, 4, false><<<grid, block, 0, s>>>(sz, A, ipiv, B, batch);
+        if (max_nrhs <= 1) getrs_small_kernel<T, NC, NW, 1, false><<<grid, block, 0, s>>>(wl, sz, A, ipiv, B);
+        else getrs_small_kernel<T, NC, NW, 4, false><<<grid, block, 0, s>>>(wl, sz, A, ipiv, B);
     }
 }
 
-
-#define MB200_INSTANTIATE_SMALL(T, NC, NW)                                                   \
-    template void launch_getrf<T, NC, NW>(const LuSizes&, T**, int**, int*, int, cudaStream_t); \
-    template void launch_gesv<T, NC, NW>(const LuSizes&, int, T**, int**, T**, int*, int, cudaStream_t); \
-    template void launch_getrs<T, NC, NW>(const LuSizes&, bool, int, T**, int**, T**, int, cudaStream_t);
+#define MB200_INSTANTIATE_SMALL(T, NC, NW)                                                                   \
+    template void launch_getrf<T, NC, NW>(const WorkList&, int, const LuSizes&, T**, int**, int*, cudaStream_t); \
+    template void launch_gesv<T, NC, NW>(const WorkList&, int, const LuSizes&, int, T**, int**, T**, int*,       \
+                                         cudaStream_t);                                                          \
+    template void launch_getrs<T, NC, NW>(const WorkList&, int, const LuSizes&, bool, int, T**, int**, T**,      \
+                                          cudaStream_t);
 
 }  // namespace mb200
 
 // Every (type, column bound, warps per matrix) the dispatcher may select.
 #define MB200_SMALL_VARIANTS(X) \
     X(double, 8, 1) X(double, 16, 1) X(double, 32, 1) X(double, 64, 1) \
-    X(double, 32, 2) X(double, 64, 2) X(double, 32, 4) X(double, 64, 4)
+    X(double, 32, 2) X(double, 64, 2) X(double, 32, 4) X(double, 64, 4) \
+    X(float, 8, 1) X(float, 16, 1) X(float, 32, 1) X(float, 64, 1) \
+    X(float, 32, 2) X(float, 64, 2) X(float, 32, 4) X(float, 64, 4)

@@ -1,0 +1,115 @@
+// vbatched.cu -- shared machinery of the variable-size ("vbatched") entry points:
+// argument checking, max-size reduction and size bucketing, all on the device.
+//
+// Reference counterparts: magmablas/vbatched_check.cu:17-100 (checker kernels +
+// host sync), magmablas/vbatched_aux.cu:504-590 (magma_imax_size_*). Instead of
+// sizing one grid by the largest instance (so that every block of a smaller
+// instance exits early, gemm_template_kernel_vbatched.cuh:53-54), instances
+// are counting-sorted into size buckets and each bucket's kernel walks only
+// its own list.
+#include "internal.h"
+#include "vbatched.h"
+
+namespace mb200 {
+
+__global__ void bucketize_kernel(const int* __restrict__ key, int batch, BucketEdges edges,
+                                 int* __restrict__ counts, int* __restrict__ lists) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= batch) return;
+    const int v = key[i];
+    if (v <= 0) return;                       // empty instances need no work
+    int b = 0;
+    while (b < edges.n - 1 && v > edges.e[b]) ++b;
+    const int slot = atomicAdd(&counts[b], 1);
+    lists[(size_t)b * batch + slot] = i;
+}
+
+__global__ void reduce_sizes_kernel(const int* __restrict__ a, const int* __restrict__ b, const int* __restrict__ c,
+                                    int batch, int* __restrict__ out) {
+    // out[0..2] = max of a, b, c; out[3..5] = min of a, b, c
+    int mx[3] = {0, 0, 0}, mn[3] = {INT_MAX, INT_MAX, INT_MAX};
+    const int* src[3] = {a, b, c};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < batch; i += gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int t = 0; t < 3; ++t)
+            if (src[t]) { mx[t] = max(mx[t], src[t][i]); mn[t] = min(mn[t], src[t][i]); }
+    }
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+        for (int off = 16; off > 0; off >>= 1) {
+            mx[t] = max(mx[t], __shfl_xor_sync(0xffffffffu, mx[t], off));
+            mn[t] = min(mn[t], __shfl_xor_sync(0xffffffffu, mn[t], off));
+        }
+        if ((threadIdx.x & 31) == 0) { atomicMax(&out[t], mx[t]); atomicMin(&out[3 + t], mn[t]); }
+    }
+}
+
+// min over i of (ld[i] - rows[i]): negative when some leading dimension is too
+// small (the reference's checkers test ld < rows, vbatched_check.cu:38-40, :852)
+__global__ void ld_slack_kernel(const int* __restrict__ rows, const int* __restrict__ ld, int batch,
+                                int* __restrict__ out) {
+    int mn = INT_MAX;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < batch; i += gridDim.x * blockDim.x)
+        mn = min(mn, ld[i] - rows[i]);
+    for (int off = 16; off > 0; off >>= 1) mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, off));
+    if ((threadIdx.x & 31) == 0) atomicMin(out, mn);
+}
+
+__global__ void init_ints_kernel(int* p, int n, int v0, int v1, int split) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = (i < split) ? v0 : v1;
+}
+
+magma_int_t bucketize(const int* key, int batch, const int* edges_host, int nb, cudaStream_t s, int* ws,
+                      int** counts_out, int** lists_out) {
+    // ws layout: [counts nb (padded to 2*nb)][lists nb*batch]; the edges travel as a kernel argument
+    if (nb > BucketEdges::kMax) return MAGMA_ERR_NOT_SUPPORTED;
+    BucketEdges edges;
+    edges.n = nb;
+    for (int b = 0; b < nb; ++b) edges.e[b] = edges_host[b];
+    int* d_counts = ws;
+    int* d_lists = ws + 2 * nb;
+    cudaMemsetAsync(d_counts, 0, sizeof(int) * nb, s);
+    bucketize_kernel<<<ceildiv(batch, 256), 256, 0, s>>>(key, batch, edges, d_counts, d_lists);
+    *counts_out = d_counts;
+    *lists_out = d_lists;
+    return launch_status();
+}
+
+size_t bucketize_ws_ints(int batch, int nb) { return (size_t)2 * nb + (size_t)nb * batch; }
+
+// Device reduction of up to three size arrays, copied back to the host
+// (the reference does the same with magma_imax_size_* + getvector + sync).
+magma_int_t reduce_sizes(const int* a, const int* b, const int* c, int batch, magma_queue_t queue, int out[6]) {
+    int* d = static_cast<int*>(queue_workspace(queue, 64));
+    if (!d) return MAGMA_ERR_DEVICE_ALLOC;
+    init_ints_kernel<<<1, 32, 0, queue->stream>>>(d, 6, 0, INT_MAX, 3);
+    reduce_sizes_kernel<<<min(ceildiv(batch, 256), 148), 256, 0, queue->stream>>>(a, b, c, batch, d);
+    cudaMemcpyAsync(out, d, sizeof(int) * 6, cudaMemcpyDeviceToHost, queue->stream);
+    cudaStreamSynchronize(queue->stream);
+    return launch_status();
+}
+
+magma_int_t ld_slack(const int* rows, const int* ld, int batch, magma_queue_t queue, int* out) {
+    int* d = static_cast<int*>(queue_workspace(queue, 64));
+    if (!d) return MAGMA_ERR_DEVICE_ALLOC;
+    init_ints_kernel<<<1, 32, 0, queue->stream>>>(d, 1, INT_MAX, INT_MAX, 1);
+    ld_slack_kernel<<<min(ceildiv(batch, 256), 148), 256, 0, queue->stream>>>(rows, ld, batch, d);
+    cudaMemcpyAsync(out, d, sizeof(int), cudaMemcpyDeviceToHost, queue->stream);
+    cudaStreamSynchronize(queue->stream);
+    return launch_status();
+}
+
+int resident_blocks(const void* kernel, int threads, size_t smem) {
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    }
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+    return max(1, per_sm) * sms;
+}
+
+}  // namespace mb200

@@ -1,0 +1,31 @@
+// vbatched.h -- device-side size checks, reductions and bucketing shared by
+// the variable-size entry points.
+#pragma once
+#include "internal.h"
+#include <climits>
+
+namespace mb200 {
+
+struct BucketEdges {
+    static constexpr int kMax = 16;
+    int n;
+    int e[kMax];
+};
+
+// Counting-sorts instances 0..batch-1 into nb buckets by key[i] (bucket b
+// holds keys <= edges[b]; keys <= 0 are dropped). ws must hold
+// bucketize_ws_ints(batch, nb) ints. Outputs device pointers to the counts
+// (nb ints) and the lists (bucket b at lists + b*batch).
+magma_int_t bucketize(const int* key, int batch, const int* edges_host, int nb, cudaStream_t s, int* ws,
+                      int** counts_out, int** lists_out);
+size_t bucketize_ws_ints(int batch, int nb);
+
+// out[0..2] = max of a, b, c (null arrays give 0), out[3..5] = their minima. Synchronises the queue.
+magma_int_t reduce_sizes(const int* a, const int* b, const int* c, int batch, magma_queue_t queue, int out[6]);
+// *out = min over i of ld[i] - rows[i]. Synchronises the queue.
+magma_int_t ld_slack(const int* rows, const int* ld, int batch, magma_queue_t queue, int* out);
+
+// Blocks of `kernel` that fit on the whole GPU at once.
+int resident_blocks(const void* kernel, int threads, size_t smem);
+
+}  // namespace mb200

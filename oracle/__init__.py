@@ -123,6 +123,17 @@ def dgesv_batched(A: np.ndarray, B: np.ndarray):
     return ipiv, info
 
 
+def dposv_vbatched(As, Bs, ns, nrhss, ldas, ldbs, solve=True, upper=False):
+    """Restated Cholesky (+ solve) on lists of column-major arrays, in place. Returns info."""
+    batch = len(As)
+    info = np.zeros(batch, np.int32)
+    n, nr, la, lb = (np.asarray(v, np.int32) for v in (ns, nrhss, ldas, ldbs))
+    Bl = Bs if Bs is not None else As
+    lib().oracle_dposv_vbatched(int(upper), _i(n), _i(nr), _ptrs(As, C.c_double), _i(la),
+                                _ptrs(Bl, C.c_double), _i(lb), _i(info), batch, int(solve))
+    return info
+
+
 # ---------------------------------------------------- reference CPU LAPACK loop
 def lapack_dgetrf_batched(A: np.ndarray, m: int, nthreads: int | None = None):
     batch, n, lda = A.shape

@@ -151,3 +151,60 @@ void oracle_dgesv_batched(int n, int nrhs, double* A, int lda, long strideA, int
         oracle_dgetrs(0, n, nrhs, Ai, lda, pi, B + (size_t)i * strideB, ldb);
     }
 }
+
+/* ---------------------------------------------------------------------------
+ * Cholesky. LAPACK dpotrf / dpotf2 (uplo = 'L'): A = L L^T. The reference's
+ * GPU path supports Lower only (src/zpotf2_vbatched.cpp:32-34). This
+ * restatement uses the outer-product (right-looking) form of the same
+ * factorisation: for k = 0..n-1
+ *     d = A(k,k); if !(d > 0) -> info = k+1, A(k,k) keeps d, stop  (dpotf2:
+ *         "IF( AJJ.LE.ZERO.OR.DISNAN( AJJ ) )", A(J,J) = AJJ, INFO = J)
+ *     A(k,k) = sqrt(d); A(k+1:n,k) *= 1/A(k,k)           (dpotf2: DSCAL by ONE/AJJ)
+ *     A(i,j) = fma(-A(i,k), A(j,k), A(i,j)) for k < j <= i (rank-1 update)
+ * It differs from dpotf2's dot-product form only in the summation order, and
+ * is pinned to OpenBLAS's dpotrf on the golden vectors within tolerance.
+ * Upper: the same on the transpose (A = U^T U with U = L^T).
+ */
+void oracle_dpotrf(int upper, int n, double* a, int lda, int* info) {
+    *info = 0;
+#define AL(i, j) (*(upper ? &A_(j, i) : &A_(i, j)))
+    for (int k = 0; k < n; ++k) {
+        double d = AL(k, k);
+        if (!(d > 0.0)) { *info = k + 1; return; }
+        d = sqrt(d);
+        AL(k, k) = d;
+        const double r = 1.0 / d;
+        for (int i = k + 1; i < n; ++i) AL(i, k) = AL(i, k) * r;
+        for (int j = k + 1; j < n; ++j)
+            for (int i = j; i < n; ++i) AL(i, j) = fma(-AL(i, k), AL(j, k), AL(i, j));
+    }
+#undef AL
+}
+
+/* LAPACK dpotrs: L y = b (column sweep, reference DTRSM Left Lower NoTrans
+ * NonUnit), then L^T x = y by the column sweep of the upper-triangular solve
+ * with U = L^T (reference DTRSM Left Upper NoTrans NonUnit loop order). */
+void oracle_dpotrs(int upper, int n, int nrhs, const double* a, int lda, double* b, int ldb) {
+#define LL(i, j) (*(upper ? &A_(j, i) : &A_(i, j)))
+    for (int c = 0; c < nrhs; ++c) {
+        for (int k = 0; k < n; ++k) {
+            B_(k, c) = B_(k, c) / LL(k, k);
+            for (int i = k + 1; i < n; ++i) B_(i, c) = fma(-B_(k, c), LL(i, k), B_(i, c));
+        }
+        for (int k = n - 1; k >= 0; --k) {
+            B_(k, c) = B_(k, c) / LL(k, k);
+            for (int i = 0; i < k; ++i) B_(i, c) = fma(-B_(k, c), LL(k, i), B_(i, c));
+        }
+    }
+#undef LL
+}
+
+/* Variable-size batched Cholesky over pointer lists (one instance per iteration). */
+void oracle_dposv_vbatched(int upper, const int* n, const int* nrhs, double* const* A, const int* lda,
+                           double* const* B, const int* ldb, int* info, int batch, int do_solve) {
+#pragma omp parallel for schedule(dynamic)
+    for (int i = 0; i < batch; ++i) {
+        oracle_dpotrf(upper, n[i], A[i], lda[i], &info[i]);
+        if (do_solve) oracle_dpotrs(upper, n[i], nrhs[i], A[i], lda[i], B[i], ldb[i]);
+    }
+}

@@ -1,0 +1,60 @@
+"""GPU tests of the mixed-precision batched solve (magma_dsgesv_batched).
+
+Criterion: every instance's solution has normwise backward error
+||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= 1e-14 against the FP64
+data; instances that refine keep A untouched; instances that fall back
+(iter < 0) hold the FP64 LU, bit-identical to the oracle's dgetf2."""
+import numpy as np
+import pytest
+
+import oracle
+from magma_b200 import testing as T
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(a, cuda):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).to(cuda)
+
+
+@pytest.mark.parametrize("n,batch", [(16, 64), (48, 64), (64, 48), (100, 32), (256, 24), (400, 6)])
+def test_dsgesv_svd_logrand(cuda, n, batch):
+    import magma_b200 as mb
+    A_np, B_np, kap = T.svd_logrand(batch, n, 1e2, 1e6, nrhs=4, seed=n)
+    A, B = dev(A_np, cuda), dev(B_np, cuda)
+    X, ipiv, it, info = mb.dsgesv_batched(A, B)
+    X, it, info = X.cpu().numpy(), it.cpu().numpy(), info.cpu().numpy()
+    be = T.backward_error(A_np, X, B_np, n)
+    assert be.max() <= 1e-14, (be.max(), it)
+    assert np.array_equal(B.cpu().numpy(), B_np)             # B untouched
+    ok = it >= 0
+    assert ok.mean() > 0.5, it                               # most instances refine in FP32
+    assert np.array_equal(A.cpu().numpy()[ok], A_np[ok])     # A untouched when refinement succeeded
+    assert np.all(info == 0)
+    if (~ok).any():                                          # fallback instances hold the FP64 LU
+        O = A_np[~ok].copy()
+        oip, oinf = oracle.dgetrf_batched(O, n)
+        assert np.array_equal(A.cpu().numpy()[~ok], O)
+        assert np.array_equal(ipiv.cpu().numpy()[~ok], oip)
+
+
+def test_dsgesv_forced_fallbacks(cuda):
+    import magma_b200 as mb
+    n = 40
+    A_np, B_np = T.lu_uniform(4, n, 2, seed=17)
+    A_np[1, 3, 5] = 1e39                        # overflows single precision -> iter -2
+    A_np[2, :, :] = 0.0                         # singular in both precisions -> iter -3, info > 0
+    A_np[2, 0, 0] = 1.0
+    A = dev(A_np, cuda)
+    X, ipiv, it, info = mb.dsgesv_batched(A, dev(B_np, cuda))
+    it, info = it.cpu().numpy(), info.cpu().numpy()
+    assert it[0] >= 0 and it[3] >= 0
+    assert it[1] == -2 and info[1] == 0
+    assert it[2] == -3 and info[2] == 2
+    O = A_np[[1, 2]].copy()
+    oip, oinf = oracle.dgetrf_batched(O, n)
+    assert np.array_equal(A.cpu().numpy()[[1, 2]], O)
+    assert list(oinf) == [0, 2]
+    be = T.backward_error(A_np[[0, 1, 3]], X.cpu().numpy()[[0, 1, 3]], B_np[[0, 1, 3]], n)
+    assert be.max() <= 1e-14

@@ -109,3 +109,33 @@ def test_svd_logrand_condition():
         assert s.max() <= 1 + 1e-12
         assert s.max() / s.min() <= kap[i] * (1 + 1e-8)
     assert kap.min() >= 1e2 and kap.max() <= 1e6
+
+
+def test_oracle_cholesky_matches_lapack_golden(chol_golden):
+    g = chol_golden
+    for tag in g["tags"]:
+        a = g[f"{tag}/A"]
+        n = a.shape[0]
+        A = [np.ascontiguousarray(a.T).copy()]
+        has_b = f"{tag}/B" in g
+        B = [np.ascontiguousarray(g[f"{tag}/B"].T).copy()] if has_b else [np.zeros((1, n))]
+        info = oracle.dposv_vbatched(A, B, [n], [B[0].shape[0]], [n], [n], solve=has_b)
+        assert info[0] == g[f"{tag}/info"], tag
+        if info[0] == 0:
+            L = np.tril(A[0].T)
+            anorm = np.abs(a).max()
+            assert np.abs(L - g[f"{tag}/L"]).max() <= 8 * n * EPS * np.sqrt(anorm), tag
+            X = B[0].T
+            assert np.abs(X - g[f"{tag}/X"]).max() <= 1e3 * n * EPS * max(np.abs(X).max(), 1), tag
+
+
+def test_oracle_cholesky_upper_is_transpose():
+    n = 23
+    a = T.spd_gram(n, 5, 0)
+    lo = [np.ascontiguousarray(a.T).copy()]
+    up = [np.ascontiguousarray(a.T).copy()]
+    b = np.ones((1, n))
+    i1 = oracle.dposv_vbatched(lo, [b.copy()], [n], [1], [n], [n], solve=False)
+    i2 = oracle.dposv_vbatched(up, [b.copy()], [n], [1], [n], [n], solve=False, upper=True)
+    assert i1[0] == 0 and i2[0] == 0
+    assert np.array_equal(np.tril(lo[0].T), np.triu(up[0].T).T)
