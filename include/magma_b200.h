@@ -190,6 +190,21 @@ magma_int_t magma_dpotrf_vbatched_max_nocheck(magma_uplo_t uplo, magma_int_t* n,
                                               magma_int_t* ldda, magma_int_t* info_array, magma_int_t batchCount,
                                               magma_int_t max_n, magma_queue_t queue);
 
+/* No counterpart in the reference. Same contract and results as
+ * magma_dpotrf_vbatched_max_nocheck, for callers that cannot allocate device
+ * memory (a stream being captured into a CUDA graph, a fixed device-memory
+ * budget, allocator callbacks): its scratch is a static device array built
+ * into the library (about 2 MiB per GPU that loads it, held until exit)
+ * instead of queue workspace. At most 65536 instances per call; larger
+ * batches return -6 with a message. The first call on a device looks up the
+ * array's address (cudaGetSymbolAddress), so make it before any stream
+ * capture. All calls share the array: calls whose work can overlap on the
+ * GPU (unordered streams) race and must be serialised by the caller. */
+magma_int_t magma_dpotrf_vbatched_max_nocheck_noalloc(magma_uplo_t uplo, magma_int_t* n, double** dA_array,
+                                                      magma_int_t* ldda, magma_int_t* info_array,
+                                                      magma_int_t batchCount, magma_int_t max_n,
+                                                      magma_queue_t queue);
+
 /* No counterpart in MAGMA 2.2 (potrs is fixed-size only, src/zpotrs_batched.cpp:71);
  * defined by analogy with magma_dpotrf_vbatched. Checks: uplo -1, n -2, nrhs -3,
  * ldda -5, lddb -7, batchCount -9. */

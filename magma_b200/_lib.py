@@ -66,6 +66,7 @@ SIGNATURES: dict[str, tuple] = {
     "magma_dposv_batched": (_i, [_i, _i, _i, _p, _i, _p, _i, _p, _i, _p]),
     "magma_dpotrf_vbatched": (_i, [_i, _p, _p, _p, _p, _i, _p]),
     "magma_dpotrf_vbatched_max_nocheck": (_i, [_i, _p, _p, _p, _p, _i, _i, _p]),
+    "magma_dpotrf_vbatched_max_nocheck_noalloc": (_i, [_i, _p, _p, _p, _p, _i, _i, _p]),
     "magma_dpotrs_vbatched": (_i, [_i, _p, _p, _p, _p, _p, _p, _i, _p]),
     "magma_dpotrs_vbatched_max_nocheck": (_i, [_i, _p, _p, _p, _p, _p, _p, _i, _i, _i, _p]),
     "magma_dposv_vbatched": (_i, [_i, _p, _p, _p, _p, _p, _p, _p, _i, _p]),
