@@ -3,22 +3,28 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
 
-A step is one pass of the hot path over one batch of synthetic input:
-  c1   plain FP64 LU + solve: magma_dgesv_batched on 10,000 x (32x32), 1 RHS,
-       entries U[-1,1] (seeded).
+A step is one pass of the hot path over one batch of synthetic input.
+Workloads (the default is the one the metric is quoted on):
+  c3  mixed-precision dgesv: 2,048 x (256x256), A = U diag(sigma) V^T with Haar U, V and
+      log-uniform sigma (kappa log-uniform in [1e2, 1e6]), 4 RHS ~ N(0,1);
+      magma_dsgesv_batched (FP32 LU + FP64 refinement + FP64 fallback) against the
+      plain FP64 form magma_dgesv_batched on the same inputs.       [default]
+  c1  plain FP64 LU + solve: magma_dgesv_batched on 10,000 x (32x32), 1 RHS, U[-1,1].
+  c2  gemm_vbatched: 20,000 instances, M, N, K ~ U{8..128}, FP64 (GFLOP/s).
+  c4  potrf_vbatched: 50,000 SPD instances, n power-law on [4, 512] (factorisations/s).
 
-Timing: W untimed steps, then exactly K steps between a barrier +
-cudaDeviceSynchronize on both sides, measured with CUDA events on the
-library's stream, max over ranks. Each step factors a different input buffer
-from a ring whose total size exceeds the 126 MB L2, so a step never finds its
-inputs in L2. N > 1 runs one replica per GPU on its own batch (independent
-instances, no collective on the data path; scaling "weak").
+Timing: W untimed steps, then exactly K steps between a barrier + device
+synchronisation on both sides, measured with CUDA events on the library's
+stream, max over ranks. The c3 inputs (1 GiB of A) exceed the 126 MB L2; c1
+cycles through a ring of input buffers larger than L2. N > 1 runs one replica
+per GPU on its own batch (instances are independent; no collective on the
+data path; scaling "weak").
 
 `value` has the inputs resident in HBM; `e2e` is the same metric through the
 public C ABI with the inputs copied from pinned host memory and the results
-(x, ipiv, info) copied back inside every timed step. `cpu_baseline` times the
-reference's own CPU path (an OpenMP loop of LAPACK dgesv, one instance per
-iteration, testing_zgetrf_batched.cpp:188-206) on this host's cores.
+copied back inside every timed step. `cpu_baseline` (and `--impl reference`)
+time the reference's own CPU path -- host LAPACK called per instance in an
+OpenMP loop (testing/testing_zgetrf_batched.cpp:188-206) -- on this host.
 """
 from __future__ import annotations
 
@@ -39,6 +45,7 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "solves/s at bwd err ≤1e-14: mixed-prec vs FP64 on 1 B200; p50/p99 latency"
 L2_BYTES = 126 * 2**20
+FP64_NOMINAL_TFLOPS = 37.0   # B200 dense FP64 (CUDA cores / DMMA), nominal
 
 
 def measured_peaks() -> dict:
@@ -65,14 +72,14 @@ class ClockSampler:
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_id: str):
-        self.index = gpu_id
+        self.gpu_id = gpu_id
         self.proc = None
         self.out = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
 
     def start(self):
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                ["nvidia-smi", f"--id={self.gpu_id}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                  "-lms", "50"], stdout=self.out, stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
@@ -87,8 +94,14 @@ class ClockSampler:
         self.out.flush()
         rows = [r.split(",") for r in Path(self.out.name).read_text().strip().splitlines() if r.strip()]
         os.unlink(self.out.name)
-        sm = [float(r[0]) for r in rows if r[0].strip().replace(".", "").isdigit()]
-        smax = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [v for v in (num(r[0]) for r in rows) if v is not None]
+        smax = [v for v in (num(r[1]) for r in rows if len(r) > 1) if v is not None]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = set()
         for r in rows:
@@ -99,35 +112,175 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
+def timed(stream, fn, steps):
+    """ms for `steps` calls of fn(i), CUDA events on `stream`."""
+    import torch
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(steps):
+        fn(i)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def vp(t):
+    return C.c_void_p(t.data_ptr())
+
+
 # ------------------------------------------------------------------ workloads
+class C3Mixed:
+    """Mixed-precision dgesv vs plain FP64 on 2,048 x (256x256), kappa in [1e2, 1e6], 4 RHS."""
+    name = "c3_dsgesv_batched_2048x256_kappa1e2-1e6_nrhs4"
+    unit = "solves/s"
+    dtype = "f32-factor+f64-refine"
+    data = "synthetic: A = U diag(sigma) V^T, Haar U,V (QR of seeded Gaussians), log-uniform sigma, B ~ N(0,1)"
+
+    def __init__(self, dev, batch=2048, n=256, nrhs=4, seed=3):
+        import torch
+
+        from magma_b200.api import ptr_array
+        from magma_b200.testing import svd_logrand_torch
+
+        self.torch, self.dev, self.batch, self.n, self.nrhs = torch, dev, batch, n, nrhs
+        self.A0, self.B0, self.kappa = svd_logrand_torch(batch, n, 1e2, 1e6, nrhs, seed, dev)
+        self.A = self.A0.clone()
+        self.B = self.B0.clone()
+        self.X = torch.empty_like(self.B)
+        self.ipiv = torch.zeros((batch, n), dtype=torch.int32, device=dev)
+        self.iter = torch.zeros(batch, dtype=torch.int32, device=dev)
+        self.info = torch.zeros(batch, dtype=torch.int32, device=dev)
+        self.A64 = self.A0.clone()
+        self.B64 = self.B0.clone()
+        self.pA, self.pB, self.pX = ptr_array(self.A), ptr_array(self.B), ptr_array(self.X)
+        self.pP = ptr_array(self.ipiv)
+        self.pA64, self.pB64 = ptr_array(self.A64), ptr_array(self.B64)
+        self.l2 = f"inputs {batch * n * n * 8 / 2**30:.2f} GiB > L2 (126 MB)"
+
+    def units(self):
+        return self.batch
+
+    # algorithmic bytes per solve for the mixed path: read A and B, write X and ipiv
+    def bytes_per_unit(self):
+        n, r = self.n, self.nrhs
+        return 8 * n * n + 2 * 8 * n * r + 4 * n
+
+    def launches_per_step(self):
+        return 6   # dlag2s+norm, sgetrf, refine, fallback getrf, copy, fallback getrs
+
+    def step(self, q, i):
+        n = self.n
+        return q.lib.magma_dsgesv_batched(n, self.nrhs, vp(self.pA), n, vp(self.pP), vp(self.pB), n, vp(self.pX), n,
+                                          vp(self.iter), vp(self.info), self.batch, q.handle)
+
+    def step_fp64(self, q, i):
+        n = self.n
+        return q.lib.magma_dgesv_batched(n, self.nrhs, vp(self.pA64), n, vp(self.pP), vp(self.pB64), n,
+                                         vp(self.info), self.batch, q.handle)
+
+    def validate(self, q):
+        from magma_b200.testing import backward_error_torch
+
+        t = self.torch
+        self.A.copy_(self.A0)
+        rc = self.step(q, 0)
+        q.sync()
+        assert rc == 0, rc
+        be_mixed = backward_error_torch(self.A0, self.X, self.B0).max().item()
+        it = self.iter.cpu()
+        hist = {int(k): int(v) for k, v in zip(*t.unique(it, return_counts=True))}
+        A, B = self.A0.clone(), self.B0.clone()
+        from magma_b200.api import dgesv_batched
+
+        dgesv_batched(A, B, queue=q)
+        q.sync()
+        be_64 = backward_error_torch(self.A0, B, self.B0).max().item()
+        self.A.copy_(self.A0)
+        return {"bwd_err_max_mixed": be_mixed, "bwd_err_max_fp64": be_64, "iter_hist": hist}
+
+    def dominant_kernel(self, q, stream, reps=5):
+        """The FP32 LU (getrf_blocked_kernel<float>) alone: magma_sgetrf_batched on a float copy."""
+        from magma_b200.api import ptr_array
+
+        t = self.torch
+        SA0 = self.A0.float()
+        SA = SA0.clone()
+        pS = ptr_array(SA)
+        n = self.n
+
+        def one(i):
+            q.lib.magma_sgetrf_batched(n, n, vp(pS), n, vp(self.pP), vp(self.info), self.batch, q.handle)
+        one(0)
+        t.cuda.synchronize()
+        ms = timed(stream, one, reps) / reps
+        alg_bytes = self.batch * (2 * 4 * n * n + 4 * n)
+        flops = self.batch * (2.0 / 3.0) * n ** 3
+        return {"kernel": "getrf_blocked_kernel<float,32,256> (magma_sgetrf_batched)", "ms": ms,
+                "alg_bytes": alg_bytes, "tflops": flops / ms / 1e9}
+
+    def e2e_setup(self):
+        t = self.torch
+        self.hA = self.A0.cpu().pin_memory()
+        self.hB = self.B0.cpu().pin_memory()
+        self.hX = t.empty(self.B0.shape, dtype=t.float64).pin_memory()
+        self.hI = t.empty(self.batch, dtype=t.int32).pin_memory()
+        self.hF = t.empty(self.batch, dtype=t.int32).pin_memory()
+        self.h2d = self.hA.numel() * 8 + self.hB.numel() * 8
+        self.d2h = self.hX.numel() * 8 + 8 * self.batch
+
+    def e2e_step(self, q, i):
+        self.A.copy_(self.hA, non_blocking=True)
+        self.B.copy_(self.hB, non_blocking=True)
+        self.step(q, i)
+        self.hX.copy_(self.X, non_blocking=True)
+        self.hI.copy_(self.iter, non_blocking=True)
+        self.hF.copy_(self.info, non_blocking=True)
+
+    def cpu_reference(self, seconds=10.0, nthreads=None, sample=512):
+        """LAPACK dsgesv (the CPU mixed-precision solver) per instance, bounded sample."""
+        import oracle
+
+        A0 = self.A0[:sample].cpu().numpy().copy()
+        B0 = self.B0[:sample].cpu().numpy().copy()
+        done, t_total = 0, 0.0
+        while t_total < seconds:
+            A = A0.copy()
+            t0 = time.perf_counter()
+            X, ip, it, inf = oracle.lapack_dsgesv_batched(A, B0, nthreads=nthreads)
+            t_total += time.perf_counter() - t0
+            done += sample
+        return done / t_total, done, (nthreads or oracle.max_threads()), \
+            f"{done} solves ({sample}-instance slices of the same inputs, re-run); LAPACK dsgesv " \
+            f"(OpenBLAS 0.3.30, scipy) in an OpenMP loop, 1 BLAS thread each"
+
+
 class C1DgesvSmall:
     """Plain FP64 LU + solve, 10,000 x (32x32), 1 RHS (magma_dgesv_batched)."""
-    name = "c1_dgesv_batched_32x32"
-    kernel = "gesv_small_kernel"
+    name = "c1_dgesv_batched_10000x32_nrhs1"
+    unit = "solves/s"
     dtype = "f64"
+    data = "synthetic: seeded U[-1,1] (splitmix64)"
 
     def __init__(self, dev, batch=10000, n=32, nrhs=1, seed=1):
-        import numpy as np
         import torch
 
         from magma_b200 import testing as T
+        from magma_b200.api import ptr_array
 
-        self.np, self.torch = np, torch
-        self.dev, self.batch, self.n, self.nrhs = dev, batch, n, nrhs
+        self.torch, self.dev, self.batch, self.n, self.nrhs = torch, dev, batch, n, nrhs
         self.A_np, self.B_np = T.lu_uniform(batch, n, nrhs, seed=seed)
         step_bytes = 8 * batch * (n * n + n * nrhs)
-        self.ring = max(2, -(-3 * L2_BYTES // step_bytes))     # ring larger than L2 (x3)
+        self.ring = max(2, -(-3 * L2_BYTES // step_bytes))
         self.A = [torch.from_numpy(self.A_np).to(dev) for _ in range(self.ring)]
         self.B = [torch.from_numpy(self.B_np).to(dev) for _ in range(self.ring)]
         self.ipiv = torch.zeros((batch, n), dtype=torch.int32, device=dev)
         self.info = torch.zeros(batch, dtype=torch.int32, device=dev)
-        from magma_b200.api import ptr_array
-
         self.pA = [ptr_array(a) for a in self.A]
         self.pB = [ptr_array(b) for b in self.B]
         self.pP = ptr_array(self.ipiv)
+        self.l2 = f"ring of {self.ring} distinct input buffers ({step_bytes / 2**20:.0f} MiB each) > L2"
 
-    # algorithmic counts (MAGMA testing/flops.h FLOPS_DGETRF + FLOPS_DGETRS; bytes read/written once)
     def units(self):
         return self.batch
 
@@ -140,23 +293,24 @@ class C1DgesvSmall:
 
     def step(self, q, i):
         k = i % self.ring
-        return q.lib.magma_dgesv_batched(self.n, self.nrhs, C.c_void_p(self.pA[k].data_ptr()), self.n,
-                                         C.c_void_p(self.pP.data_ptr()), C.c_void_p(self.pB[k].data_ptr()),
-                                         self.n, C.c_void_p(self.info.data_ptr()), self.batch, q.handle)
+        return q.lib.magma_dgesv_batched(self.n, self.nrhs, vp(self.pA[k]), self.n, vp(self.pP), vp(self.pB[k]),
+                                         self.n, vp(self.info), self.batch, q.handle)
 
     def validate(self, q):
-        """Fresh solve of the pristine batch; returns the max normwise backward error (checked on host)."""
         from magma_b200 import testing as T
+        from magma_b200.api import dgesv_batched
 
         A = self.torch.from_numpy(self.A_np).to(self.dev)
         B = self.torch.from_numpy(self.B_np).to(self.dev)
-        from magma_b200.api import dgesv_batched
-
         dgesv_batched(A, B, queue=q)
         q.sync()
-        return float(T.backward_error(self.A_np, B.cpu().numpy(), self.B_np, self.n).max())
+        return {"bwd_err_max_fp64": float(T.backward_error(self.A_np, B.cpu().numpy(), self.B_np, self.n).max())}
 
-    # end-to-end through the C ABI with host buffers
+    def dominant_kernel(self, q, stream, reps=200):
+        ms = timed(stream, lambda i: self.step(q, i), reps) / reps
+        return {"kernel": "gesv_small_kernel<double,32,1,1>", "ms": ms, "alg_bytes": self.bytes_per_unit() * self.batch,
+                "tflops": None}
+
     def e2e_setup(self):
         t = self.torch
         self.hA = t.from_numpy(self.A_np).pin_memory()
@@ -176,23 +330,23 @@ class C1DgesvSmall:
         self.hP.copy_(self.ipiv, non_blocking=True)
         self.hI.copy_(self.info, non_blocking=True)
 
-    # reference CPU path on a bounded sample
     def cpu_reference(self, seconds=10.0, nthreads=None):
         import oracle
 
-        sample = min(self.batch, 10000)
-        A0, B0 = self.A_np[:sample], self.B_np[:sample]
         done, t_total = 0, 0.0
         while t_total < seconds:
-            A, B = A0.copy(), B0.copy()
+            A, B = self.A_np.copy(), self.B_np.copy()
             t0 = time.perf_counter()
             oracle.lapack_dgesv_batched(A, B, nthreads=nthreads)
             t_total += time.perf_counter() - t0
-            done += sample
-        return done / t_total, done, (nthreads or oracle.max_threads())
+            done += self.batch
+        return done / t_total, done, (nthreads or oracle.max_threads()), \
+            f"{done} solves (10,000-instance batches, same inputs); LAPACK dgesv (OpenBLAS 0.3.30, scipy) " \
+            f"in an OpenMP loop, 1 BLAS thread each"
 
 
-WORKLOADS = {"c1": C1DgesvSmall}
+WORKLOADS = {"c3": C3Mixed, "c1": C1DgesvSmall}
+DEFAULT_STEPS = {"c3": (60, 5), "c1": (20000, 50)}
 
 
 # ---------------------------------------------------------------------- main
@@ -202,13 +356,11 @@ def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
+    if world > 1 and args.impl != "reference":
         import datetime
 
         import torch.distributed as dist
 
-        if args.impl == "reference":
-            return rank, world, local, None
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
@@ -216,40 +368,51 @@ def dist_setup(args):
     return rank, world, local, None
 
 
-def run_reference(args, rank, world):
-    """The reference's CPU implementation (LAPACK loop) on this host; rank 0 only."""
+def run_reference(args, rank):
+    """The reference's CPU implementation (host LAPACK loop) on this host; rank 0 only."""
     if rank != 0:
         return
-    import numpy as np  # noqa: F401
+    import numpy as np
 
     import oracle
-
-    W = WORKLOADS[args.workload]
     from magma_b200 import testing as T
 
     nthreads = oracle.max_threads()
-    if args.workload == "c1":
+    # each step gets fresh copies of the inputs, made outside the timed call
+    if args.workload == "c3":
+        sample = 256
+        A0, B0, _ = T.svd_logrand(sample, 256, 1e2, 1e6, nrhs=4, seed=3)
+        prep = lambda: (A0.copy(), B0)   # noqa: E731
+        fn = lambda a, b: oracle.lapack_dsgesv_batched(a, b, nthreads=nthreads)   # noqa: E731
+        desc = f"{sample} instances per step (256x256, kappa in [1e2,1e6], 4 RHS); LAPACK dsgesv"
+        cfg = {"workload": C3Mixed.name, "batch": sample, "n": 256, "nrhs": 4}
+        dtype = C3Mixed.dtype
+    else:
         sample = 10000
         A0, B0 = T.lu_uniform(sample, 32, 1, seed=1)
-        for _ in range(args.warmup):
-            oracle.lapack_dgesv_batched(A0.copy(), B0.copy(), nthreads=nthreads)
-        times = []
-        for _ in range(args.steps):
-            A, B = A0.copy(), B0.copy()
-            t0 = time.perf_counter()
-            oracle.lapack_dgesv_batched(A, B, nthreads=nthreads)
-            times.append(time.perf_counter() - t0)
-        total = sum(times)
-        value = sample * args.steps / total
-        ms = 1e3 * total / args.steps
+        prep = lambda: (A0.copy(), B0.copy())   # noqa: E731
+        fn = lambda a, b: oracle.lapack_dgesv_batched(a, b, nthreads=nthreads)   # noqa: E731
+        desc = f"{sample} instances per step (32x32, 1 RHS); LAPACK dgesv"
+        cfg = {"workload": C1DgesvSmall.name, "batch": sample, "n": 32, "nrhs": 1}
+        dtype = C1DgesvSmall.dtype
+    for _ in range(args.warmup):
+        fn(*prep())
+    times = []
+    for _ in range(args.steps):
+        a, b = prep()
+        t0 = time.perf_counter()
+        fn(a, b)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = sample * args.steps / total
+    del np
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": W.dtype, "data": "synthetic (seeded U[-1,1])",
-        "config": {"workload": W.name, "batch": sample, "n": 32, "nrhs": 1},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype, "data": "synthetic",
+        "config": cfg,
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": nthreads, "kind": "reference",
-                         "sample": f"{sample} instances per step; LAPACK dgesv (OpenBLAS 0.3.30, scipy) in an "
-                                   f"OpenMP loop, 1 BLAS thread per instance"},
+                         "sample": desc + " (OpenBLAS 0.3.30, scipy) in an OpenMP loop, 1 BLAS thread each"},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -261,19 +424,18 @@ def main():
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=None)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c1")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c3")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
-    defaults = {"c1": (20000, 50)}
     if args.steps is None:
-        args.steps = defaults[args.workload][0] if args.impl == "ours" else 20
+        args.steps = DEFAULT_STEPS[args.workload][0] if args.impl == "ours" else 5
     if args.warmup is None:
-        args.warmup = defaults[args.workload][1] if args.impl == "ours" else 3
+        args.warmup = DEFAULT_STEPS[args.workload][1] if args.impl == "ours" else 3
     args.warmup = max(args.warmup, 3)
 
     rank, world, local, dist = dist_setup(args)
     if args.impl == "reference":
-        run_reference(args, rank, world)
+        run_reference(args, rank)
         return
 
     import torch
@@ -285,10 +447,10 @@ def main():
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     stream = torch.cuda.Stream(dev)
-    W = WORKLOADS[args.workload](dev)
     with torch.cuda.stream(stream):
+        W = WORKLOADS[args.workload](dev)
         q = Queue(stream, local)
-        bwd = W.validate(q)
+        checks = W.validate(q)
         for i in range(args.warmup):
             W.step(q, i)
         torch.cuda.synchronize(dev)
@@ -300,69 +462,68 @@ def main():
         torch.cuda.synchronize(dev)
         if dist:
             dist.barrier()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for i in range(args.steps):
-            rc = W.step(q, i)
-        e1.record(stream)
-        torch.cuda.synchronize(dev)
+        rcs = []
+        ms_total = timed(stream, lambda i: rcs.append(W.step(q, i)), args.steps)
         if dist:
             dist.barrier()
         clk = clocks.stop()
-        assert rc == 0, f"library returned {rc}"
-        ms_total = e0.elapsed_time(e1)
+        assert all(rc == 0 for rc in rcs), f"library returned {set(rcs)}"
+        extra = {}
+        if hasattr(W, "step_fp64"):
+            for i in range(3):
+                W.step_fp64(q, i)
+            torch.cuda.synchronize(dev)
+            ms_fp64 = timed(stream, lambda i: W.step_fp64(q, i), args.steps)
+            extra["fp64_ms_per_step"] = ms_fp64 / args.steps
+        dom = W.dominant_kernel(q, stream)
         # end to end (host buffers, copies inside each step)
         W.e2e_setup()
-        ke = max(3, min(args.steps, 200))
-        for i in range(3):
+        ke = max(3, min(args.steps, 10 if args.workload == "c3" else 200))
+        for i in range(2):
             W.e2e_step(q, i)
         torch.cuda.synchronize(dev)
         if dist:
             dist.barrier()
-        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        f0.record(stream)
-        for i in range(ke):
-            W.e2e_step(q, i)
-        f1.record(stream)
-        torch.cuda.synchronize(dev)
-        ms_e2e = f0.elapsed_time(f1)
+        ms_e2e = timed(stream, lambda i: W.e2e_step(q, i), ke)
+    vals = [ms_total, ms_e2e, extra.get("fp64_ms_per_step", 0.0) * args.steps]
     if dist:
-        t = torch.tensor([ms_total, ms_e2e, bwd], device=dev, dtype=torch.float64)
+        t = torch.tensor(vals, device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total, ms_e2e, bwd = (float(v) for v in t.tolist())
+        vals = [float(v) for v in t.tolist()]
+    ms_total, ms_e2e, ms_fp64_total = vals
     units = W.units() * world
     value = units * args.steps / (ms_total * 1e-3)
-    e2e_value = units * ke / (ms_e2e * 1e-3)
     if rank == 0:
         peaks = measured_peaks()
-        per_launch_ms = ms_total / (args.steps * W.launches_per_step())
-        alg_bytes = W.bytes_per_unit() * W.units()
-        achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9
-        traffic = profile_traffic(W.kernel, W.name)
+        achieved = dom["alg_bytes"] / (dom["ms"] * 1e-3) / 1e9
         line = {
-            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "metric": METRIC, "value": value, "unit": W.unit, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": W.dtype,
-            "data": "synthetic (seeded U[-1,1], splitmix64)",
+            "scaling": "weak", "vs_baseline": None, "dtype": W.dtype, "data": W.data,
             "config": {"workload": W.name, "batch_per_gpu": W.batch, "n": W.n, "nrhs": W.nrhs,
-                       "parallelism": f"replicas x{world}",
-                       "l2": f"ring of {W.ring} distinct input buffers ({W.ring} x "
-                             f"{8 * W.batch * (W.n * W.n + W.n * W.nrhs) / 2**20:.0f} MiB) > L2"},
-            "bwd_err_max": bwd,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                         "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
-                         "kernel": W.kernel, "peak_src": peaks["src"],
-                         "alg_bytes_per_launch": alg_bytes},
-            "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": W.h2d,
-                    "d2h_bytes_per_step": W.d2h, "steps": ke},
-            "gpu_launches": args.steps * W.launches_per_step(),
-            "clocks": clk,
+                       "parallelism": f"replicas x{world}", "l2": W.l2},
         }
+        line.update(checks)
+        if ms_fp64_total:
+            fp64_value = units * args.steps / (ms_fp64_total * 1e-3)
+            line["fp64_value"] = fp64_value
+            line["mixed_over_fp64"] = value / fp64_value
+        line["roofline"] = {
+            "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / peaks["hbm_gbs"], "traffic": profile_traffic(dom["kernel"].split("<")[0], W.name),
+            "kernel": dom["kernel"], "kernel_ms": dom["ms"], "alg_bytes_per_launch": dom["alg_bytes"],
+            "peak_src": peaks["src"],
+        }
+        if dom.get("tflops"):
+            line["roofline"]["kernel_tflops"] = dom["tflops"]
+        line["e2e"] = {"value": units * ke / (ms_e2e * 1e-3), "unit": W.unit, "h2d_bytes_per_step": W.h2d,
+                       "d2h_bytes_per_step": W.d2h, "steps": ke}
+        line["gpu_launches"] = args.steps * W.launches_per_step()
+        line["clocks"] = clk
         if not args.no_cpu_baseline and world == 1:
-            v, done, cores = W.cpu_reference()
-            line["cpu_baseline"] = {"value": v, "unit": "solves/s", "cores": cores, "kind": "reference",
-                                    "sample": f"{done} solves (10,000-instance batches, same inputs); LAPACK dgesv "
-                                              f"(OpenBLAS 0.3.30, scipy) in an OpenMP loop, 1 BLAS thread each"}
+            v, done, cores, sample = W.cpu_reference()
+            line["cpu_baseline"] = {"value": v, "unit": W.unit, "cores": cores, "kind": "reference",
+                                    "sample": sample}
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()

@@ -138,6 +138,18 @@ magma_int_t magma_dgesv_batched(magma_int_t n, magma_int_t nrhs, double** dA_arr
                                 magma_int_t* dinfo_array, magma_int_t batchCount, magma_queue_t queue);
 
 
+/* Single-precision forms (generated from the same templates in MAGMA:
+ * src/zgetrf_batched.cpp:83, src/zgetrs_batched.cpp:87, src/zgesv_batched.cpp:93). */
+magma_int_t magma_sgetrf_batched(magma_int_t m, magma_int_t n, float** dA_array, magma_int_t ldda,
+                                 magma_int_t** ipiv_array, magma_int_t* info_array, magma_int_t batchCount,
+                                 magma_queue_t queue);
+magma_int_t magma_sgetrs_batched(magma_trans_t trans, magma_int_t n, magma_int_t nrhs, float** dA_array,
+                                 magma_int_t ldda, magma_int_t** dipiv_array, float** dB_array, magma_int_t lddb,
+                                 magma_int_t batchCount, magma_queue_t queue);
+magma_int_t magma_sgesv_batched(magma_int_t n, magma_int_t nrhs, float** dA_array, magma_int_t ldda,
+                                magma_int_t** dipiv_array, float** dB_array, magma_int_t lddb,
+                                magma_int_t* dinfo_array, magma_int_t batchCount, magma_queue_t queue);
+
 /* Mixed precision: FP32 LU + FP64 iterative refinement with FP64 fallback.
  * No batched counterpart in MAGMA 2.2; per instance it is magma_dsgesv_gpu
  * (src/zcgesv_gpu.cpp:144-365): stopping test max|R_j| <= max|X_j| ||A||_inf
@@ -225,6 +237,75 @@ magma_int_t magma_dposv_vbatched_max_nocheck(magma_uplo_t uplo, magma_int_t* n, 
                                              double** dA_array, magma_int_t* ldda, double** dB_array,
                                              magma_int_t* lddb, magma_int_t* dinfo_array, magma_int_t batchCount,
                                              magma_int_t max_n, magma_int_t max_nrhs, magma_queue_t queue);
+
+/* ------------------------------------------------------------------------
+ * Batched GEMM: C_i = alpha op(A_i) op(B_i) + beta C_i (C not read when beta == 0,
+ * magmablas/gemm_template_device.cuh:197). Checks as
+ * magmablas/dgemm_batched_core.cu:180-213 (transA -1, transB -2, m -3, n -4, k -5,
+ * ldda -8, lddb -10, lddc -13; quick return when m, n or k <= 0).
+ * ---------------------------------------------------------------------- */
+/* magmablas/zgemm_batched.cpp:148-160 */
+void magmablas_dgemm_batched(magma_trans_t transA, magma_trans_t transB, magma_int_t m, magma_int_t n, magma_int_t k,
+                             double alpha, double const* const* dA_array, magma_int_t ldda,
+                             double const* const* dB_array, magma_int_t lddb, double beta, double** dC_array,
+                             magma_int_t lddc, magma_int_t batchCount, magma_queue_t queue);
+/* magmablas/zgemm_batched.cpp:169-196 (the reference picks cuBLAS or its own kernel; here always the library's) */
+void magma_dgemm_batched(magma_trans_t transA, magma_trans_t transB, magma_int_t m, magma_int_t n, magma_int_t k,
+                         double alpha, double const* const* dA_array, magma_int_t ldda, double const* const* dB_array,
+                         magma_int_t lddb, double beta, double** dC_array, magma_int_t lddc, magma_int_t batchCount,
+                         magma_queue_t queue);
+void magmablas_sgemm_batched(magma_trans_t transA, magma_trans_t transB, magma_int_t m, magma_int_t n, magma_int_t k,
+                             float alpha, float const* const* dA_array, magma_int_t ldda, float const* const* dB_array,
+                             magma_int_t lddb, float beta, float** dC_array, magma_int_t lddc, magma_int_t batchCount,
+                             magma_queue_t queue);
+void magma_sgemm_batched(magma_trans_t transA, magma_trans_t transB, magma_int_t m, magma_int_t n, magma_int_t k,
+                         float alpha, float const* const* dA_array, magma_int_t ldda, float const* const* dB_array,
+                         magma_int_t lddb, float beta, float** dC_array, magma_int_t lddc, magma_int_t batchCount,
+                         magma_queue_t queue);
+
+/* Variable-size GEMM, m/n/k/ldda/lddb/lddc device arrays of batchCount+1 entries.
+ * magmablas/zgemm_vbatched.cpp:235-271 (checked; one host synchronisation for the
+ * checker and the maxima), :19-29 (_max_nocheck), :33 (_max), :81 (_nocheck);
+ * checks as magmablas/vbatched_check.cu:78-99 (batchCount -14). */
+void magmablas_dgemm_vbatched(magma_trans_t transA, magma_trans_t transB, magma_int_t* m, magma_int_t* n,
+                              magma_int_t* k, double alpha, double const* const* dA_array, magma_int_t* ldda,
+                              double const* const* dB_array, magma_int_t* lddb, double beta, double** dC_array,
+                              magma_int_t* lddc, magma_int_t batchCount, magma_queue_t queue);
+void magmablas_dgemm_vbatched_max_nocheck(magma_trans_t transA, magma_trans_t transB, magma_int_t* m, magma_int_t* n,
+                                          magma_int_t* k, double alpha, double const* const* dA_array,
+                                          magma_int_t* ldda, double const* const* dB_array, magma_int_t* lddb,
+                                          double beta, double** dC_array, magma_int_t* lddc, magma_int_t batchCount,
+                                          magma_int_t max_m, magma_int_t max_n, magma_int_t max_k,
+                                          magma_queue_t queue);
+void magmablas_dgemm_vbatched_max(magma_trans_t transA, magma_trans_t transB, magma_int_t* m, magma_int_t* n,
+                                  magma_int_t* k, double alpha, double const* const* dA_array, magma_int_t* ldda,
+                                  double const* const* dB_array, magma_int_t* lddb, double beta, double** dC_array,
+                                  magma_int_t* lddc, magma_int_t batchCount, magma_int_t max_m, magma_int_t max_n,
+                                  magma_int_t max_k, magma_queue_t queue);
+void magmablas_dgemm_vbatched_nocheck(magma_trans_t transA, magma_trans_t transB, magma_int_t* m, magma_int_t* n,
+                                      magma_int_t* k, double alpha, double const* const* dA_array, magma_int_t* ldda,
+                                      double const* const* dB_array, magma_int_t* lddb, double beta,
+                                      double** dC_array, magma_int_t* lddc, magma_int_t batchCount,
+                                      magma_queue_t queue);
+void magmablas_sgemm_vbatched(magma_trans_t transA, magma_trans_t transB, magma_int_t* m, magma_int_t* n,
+                              magma_int_t* k, float alpha, float const* const* dA_array, magma_int_t* ldda,
+                              float const* const* dB_array, magma_int_t* lddb, float beta, float** dC_array,
+                              magma_int_t* lddc, magma_int_t batchCount, magma_queue_t queue);
+void magmablas_sgemm_vbatched_max_nocheck(magma_trans_t transA, magma_trans_t transB, magma_int_t* m, magma_int_t* n,
+                                          magma_int_t* k, float alpha, float const* const* dA_array,
+                                          magma_int_t* ldda, float const* const* dB_array, magma_int_t* lddb,
+                                          float beta, float** dC_array, magma_int_t* lddc, magma_int_t batchCount,
+                                          magma_int_t max_m, magma_int_t max_n, magma_int_t max_k,
+                                          magma_queue_t queue);
+void magmablas_sgemm_vbatched_max(magma_trans_t transA, magma_trans_t transB, magma_int_t* m, magma_int_t* n,
+                                  magma_int_t* k, float alpha, float const* const* dA_array, magma_int_t* ldda,
+                                  float const* const* dB_array, magma_int_t* lddb, float beta, float** dC_array,
+                                  magma_int_t* lddc, magma_int_t batchCount, magma_int_t max_m, magma_int_t max_n,
+                                  magma_int_t max_k, magma_queue_t queue);
+void magmablas_sgemm_vbatched_nocheck(magma_trans_t transA, magma_trans_t transB, magma_int_t* m, magma_int_t* n,
+                                      magma_int_t* k, float alpha, float const* const* dA_array, magma_int_t* ldda,
+                                      float const* const* dB_array, magma_int_t* lddb, float beta, float** dC_array,
+                                      magma_int_t* lddc, magma_int_t batchCount, magma_queue_t queue);
 
 #ifdef __cplusplus
 }

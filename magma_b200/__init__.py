@@ -11,10 +11,12 @@ from __future__ import annotations
 
 from . import _lib
 from .api import (Queue, VarBatch, ptr_array, dgetrf_batched, dgetrs_batched, dgesv_batched, dpotrf_batched,
-                  dpotrs_batched, dposv_batched, dposv_vbatched, dsgesv_batched)
+                  dpotrs_batched, dposv_batched, dposv_vbatched, dsgesv_batched,
+                  gemm_batched, gemm_vbatched)
 
 __all__ = ["Queue", "VarBatch", "ptr_array", "dgetrf_batched", "dgetrs_batched", "dgesv_batched", "dpotrf_batched",
-           "dpotrs_batched", "dposv_batched", "dposv_vbatched", "dsgesv_batched", "load"]
+           "dpotrs_batched", "dposv_batched", "dposv_vbatched", "dsgesv_batched", "gemm_batched",
+           "gemm_vbatched", "load"]
 
 
 def load():

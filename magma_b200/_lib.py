@@ -59,6 +59,9 @@ SIGNATURES: dict[str, tuple] = {
     "magma_dgetrf_batched": (_i, [_i, _i, _p, _i, _p, _p, _i, _p]),
     "magma_dgetrs_batched": (_i, [_i, _i, _i, _p, _i, _p, _p, _i, _i, _p]),
     "magma_dgesv_batched": (_i, [_i, _i, _p, _i, _p, _p, _i, _p, _i, _p]),
+    "magma_sgetrf_batched": (_i, [_i, _i, _p, _i, _p, _p, _i, _p]),
+    "magma_sgetrs_batched": (_i, [_i, _i, _i, _p, _i, _p, _p, _i, _i, _p]),
+    "magma_sgesv_batched": (_i, [_i, _i, _p, _i, _p, _p, _i, _p, _i, _p]),
     "magma_dsgesv_batched": (_i, [_i, _i, _p, _i, _p, _p, _i, _p, _i, _p, _p, _i, _p]),
     # batched Cholesky
     "magma_dpotrf_batched": (_i, [_i, _i, _p, _i, _p, _i, _p]),
@@ -71,6 +74,21 @@ SIGNATURES: dict[str, tuple] = {
     "magma_dpotrs_vbatched_max_nocheck": (_i, [_i, _p, _p, _p, _p, _p, _p, _i, _i, _i, _p]),
     "magma_dposv_vbatched": (_i, [_i, _p, _p, _p, _p, _p, _p, _p, _i, _p]),
     "magma_dposv_vbatched_max_nocheck": (_i, [_i, _p, _p, _p, _p, _p, _p, _p, _i, _i, _i, _p]),
+    # batched gemm
+    "magmablas_dgemm_batched": (None, [_i, _i, _i, _i, _i, _d, _p, _i, _p, _i, _d, _p, _i, _i, _p]),
+    "magma_dgemm_batched": (None, [_i, _i, _i, _i, _i, _d, _p, _i, _p, _i, _d, _p, _i, _i, _p]),
+    "magmablas_sgemm_batched": (None, [_i, _i, _i, _i, _i, _f, _p, _i, _p, _i, _f, _p, _i, _i, _p]),
+    "magma_sgemm_batched": (None, [_i, _i, _i, _i, _i, _f, _p, _i, _p, _i, _f, _p, _i, _i, _p]),
+    "magmablas_dgemm_vbatched": (None, [_i, _i, _p, _p, _p, _d, _p, _p, _p, _p, _d, _p, _p, _i, _p]),
+    "magmablas_dgemm_vbatched_max_nocheck": (None, [_i, _i, _p, _p, _p, _d, _p, _p, _p, _p, _d, _p, _p, _i, _i, _i,
+                                                    _i, _p]),
+    "magmablas_dgemm_vbatched_max": (None, [_i, _i, _p, _p, _p, _d, _p, _p, _p, _p, _d, _p, _p, _i, _i, _i, _i, _p]),
+    "magmablas_dgemm_vbatched_nocheck": (None, [_i, _i, _p, _p, _p, _d, _p, _p, _p, _p, _d, _p, _p, _i, _p]),
+    "magmablas_sgemm_vbatched": (None, [_i, _i, _p, _p, _p, _f, _p, _p, _p, _p, _f, _p, _p, _i, _p]),
+    "magmablas_sgemm_vbatched_max_nocheck": (None, [_i, _i, _p, _p, _p, _f, _p, _p, _p, _p, _f, _p, _p, _i, _i, _i,
+                                                    _i, _p]),
+    "magmablas_sgemm_vbatched_max": (None, [_i, _i, _p, _p, _p, _f, _p, _p, _p, _p, _f, _p, _p, _i, _i, _i, _i, _p]),
+    "magmablas_sgemm_vbatched_nocheck": (None, [_i, _i, _p, _p, _p, _f, _p, _p, _p, _p, _f, _p, _p, _i, _p]),
 }
 
 _lib: C.CDLL | None = None

@@ -181,6 +181,7 @@ class VarBatch:
         self.offsets = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64) if mats else np.zeros(0, np.int64)
         total = int(sum(sizes)) if mats else 1
         flat = np.zeros(max(total, 1), dtype=np.float64 if dtype == torch.float64 else np.float32)
+        self.dtype = dtype
         for m, o in zip(mats, self.offsets):
             flat[o:o + m.size] = m.reshape(-1)
         self.buf = torch.from_numpy(flat).to(device)
@@ -258,3 +259,35 @@ def dsgesv_batched(A: torch.Tensor, B: torch.Tensor, queue: Queue | None = None)
     _check(q.lib.magma_dsgesv_batched(n, nrhs, _vp(pA), lda, _vp(pP), _vp(pB), ldb, _vp(pX), n, _vp(it), _vp(info),
                                       batch, q.handle), "magma_dsgesv_batched")
     return X, ipiv, it, info
+
+
+# ------------------------------------------------------------------------------- GEMM
+def _trans(t: bool) -> int:
+    return MagmaTrans if t else MagmaNoTrans
+
+
+def gemm_batched(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor, m: int, n: int, k: int, alpha=1.0, beta=0.0,
+                 transA=False, transB=False, queue: Queue | None = None) -> None:
+    """C_i = alpha op(A_i) op(B_i) + beta C_i for column-major batches (batch, cols, ld), in place."""
+    q = queue or default_queue()
+    batch = C.shape[0]
+    pre = "d" if C.dtype == torch.float64 else "s"
+    fn = getattr(q.lib, f"magmablas_{pre}gemm_batched")
+    pA, pB, pC = ptr_array(A), ptr_array(B), ptr_array(C)
+    fn(_trans(transA), _trans(transB), m, n, k, alpha, _vp(pA), A.shape[2], _vp(pB), B.shape[2], beta, _vp(pC),
+       C.shape[2], batch, q.handle)
+
+
+def gemm_vbatched(A: "VarBatch", B: "VarBatch", C: "VarBatch", m, n, k, lda, ldb, ldc, alpha=1.0, beta=0.0,
+                  transA=False, transB=False, max_sizes=None, queue: Queue | None = None) -> None:
+    """Variable-size GEMM through magmablas_{d,s}gemm_vbatched (or _max_nocheck when max_sizes is given)."""
+    q = queue or default_queue()
+    pre = "d" if C.buf.dtype == torch.float64 else "s"
+    dm, dn, dk = C.ints(m), C.ints(n), C.ints(k)
+    dla, dlb, dlc = C.ints(lda), C.ints(ldb), C.ints(ldc)
+    args = [_trans(transA), _trans(transB), _vp(dm), _vp(dn), _vp(dk), alpha, _vp(A.ptrs), _vp(dla), _vp(B.ptrs),
+            _vp(dlb), beta, _vp(C.ptrs), _vp(dlc), C.batch]
+    if max_sizes:
+        getattr(q.lib, f"magmablas_{pre}gemm_vbatched_max_nocheck")(*args, *max_sizes, q.handle)
+    else:
+        getattr(q.lib, f"magmablas_{pre}gemm_vbatched")(*args, q.handle)

@@ -1,0 +1,272 @@
+// gemm.cu -- batched and variable-size batched GEMM: C = alpha op(A) op(B) + beta C.
+//
+// Replaces magmablas_{d,s}gemm_batched_core (magmablas/dgemm_batched_core.cu:161-436) and
+// magmablas_{d,s}gemm_vbatched_core (magmablas/dgemm_vbatched_core.cu:28-266). One
+// thread block computes one 64x64 tile of one instance's C with 256 threads (4x4
+// outputs each); op(A) and op(B) are staged through shared memory in K chunks of
+// 16, transposed at load time so the inner loop always reads contiguous vectors,
+// with the next chunk prefetched into registers while the current one is used.
+// Instances are laid out along grid.x as (instance, tile) pairs sized by the
+// largest instance; tiles past an instance's own size exit at once.
+// Epilogue as the reference (magmablas/gemm_template_device.cuh:197-227): C is not
+// read when beta == 0.
+#include "internal.h"
+#include "vbatched.h"
+#include <algorithm>
+
+namespace mb200 {
+
+struct GemmSizes {
+    int m, n, k, lda, ldb, ldc;
+    const int *m_arr, *n_arr, *k_arr, *lda_arr, *ldb_arr, *ldc_arr;
+    __device__ __forceinline__ int M(int i) const { return m_arr ? m_arr[i] : m; }
+    __device__ __forceinline__ int N(int i) const { return n_arr ? n_arr[i] : n; }
+    __device__ __forceinline__ int K(int i) const { return k_arr ? k_arr[i] : k; }
+    __device__ __forceinline__ int LDA(int i) const { return lda_arr ? lda_arr[i] : lda; }
+    __device__ __forceinline__ int LDB(int i) const { return ldb_arr ? ldb_arr[i] : ldb; }
+    __device__ __forceinline__ int LDC(int i) const { return ldc_arr ? ldc_arr[i] : ldc; }
+};
+
+template <typename T, bool TA, bool TB>
+__global__ void __launch_bounds__(256)
+gemm_tile_kernel(GemmSizes g, T alpha, const T* const* __restrict__ A_arr, const T* const* __restrict__ B_arr, T beta,
+                 T** __restrict__ C_arr, int tiles_m, int tiles_n) {
+    constexpr int BM = 64, BN = 64, BK = 16, TM = 4, TN = 4, NT = 256;
+    // rows padded by one element: the K-fastest staging stores would otherwise
+    // hit one bank 16 times
+    __shared__ T sA[BK][BM + 1];
+    __shared__ T sB[BK][BN + 1];
+    const int tiles = tiles_m * tiles_n;
+    const int id = blockIdx.x / tiles;
+    const int t = blockIdx.x - id * tiles;
+    const int i0 = (t / tiles_n) * BM, j0 = (t % tiles_n) * BN;
+    const int m = g.M(id), n = g.N(id), k = g.K(id);
+    if (i0 >= m || j0 >= n) return;
+    const int lda = g.LDA(id), ldb = g.LDB(id), ldc = g.LDC(id);
+    const T* A = A_arr[id];
+    const T* B = B_arr[id];
+    T* C = C_arr[id];
+    const int tid = threadIdx.x;
+    // thread (tx, ty) owns rows tx + 16*i and columns ty*4 + j of the tile: consecutive
+    // threads read consecutive A values (no bank conflicts) and write consecutive
+    // rows of column-major C (coalesced); the B values are warp-wide broadcasts
+    const int tx = tid % (BM / TM), ty = tid / (BM / TM);
+    T acc[TM][TN];
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+        for (int j = 0; j < TN; ++j) acc[i][j] = T(0);
+
+    // each thread stages 4 elements of the A chunk and 4 of the B chunk
+    T ra[4], rb[4];
+    auto load_chunk = [&](int k0) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int idx = tid + e * NT;
+            int r, c;
+            if (!TA) { r = idx % BM; c = idx / BM; } else { c = idx % BK; r = idx / BK; }
+            const int gi = i0 + r, gk = k0 + c;
+            ra[e] = (gi < m && gk < k) ? (TA ? A[gk + (size_t)gi * lda] : A[gi + (size_t)gk * lda]) : T(0);
+        }
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int idx = tid + e * NT;
+            int c, j;
+            if (!TB) { c = idx % BK; j = idx / BK; } else { j = idx % BN; c = idx / BN; }
+            const int gk = k0 + c, gj = j0 + j;
+            rb[e] = (gk < k && gj < n) ? (TB ? B[gj + (size_t)gk * ldb] : B[gk + (size_t)gj * ldb]) : T(0);
+        }
+    };
+    auto store_chunk = [&]() {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int idx = tid + e * NT;
+            int r, c;
+            if (!TA) { r = idx % BM; c = idx / BM; } else { c = idx % BK; r = idx / BK; }
+            sA[c][r] = ra[e];
+        }
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int idx = tid + e * NT;
+            int c, j;
+            if (!TB) { c = idx % BK; j = idx / BK; } else { j = idx % BN; c = idx / BN; }
+            sB[c][j] = rb[e];
+        }
+    };
+    if (k > 0) load_chunk(0);
+    for (int k0 = 0; k0 < k; k0 += BK) {
+        __syncthreads();
+        store_chunk();
+        __syncthreads();
+        if (k0 + BK < k) load_chunk(k0 + BK);   // prefetch the next chunk while computing
+#pragma unroll
+        for (int kk = 0; kk < BK; ++kk) {
+            T a[TM], b[TN];
+#pragma unroll
+            for (int i = 0; i < TM; ++i) a[i] = sA[kk][tx + (BM / TM) * i];
+#pragma unroll
+            for (int j = 0; j < TN; ++j) b[j] = sB[kk][ty * TN + j];
+#pragma unroll
+            for (int i = 0; i < TM; ++i)
+#pragma unroll
+                for (int j = 0; j < TN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+        const int gj = j0 + ty * TN + j;
+        if (gj >= n) continue;
+#pragma unroll
+        for (int i = 0; i < TM; ++i) {
+            const int gi = i0 + tx + (BM / TM) * i;
+            if (gi >= m) continue;
+            T* c = C + gi + (size_t)gj * ldc;
+            *c = (beta == T(0)) ? alpha * acc[i][j] : alpha * acc[i][j] + beta * (*c);
+        }
+    }
+}
+
+template <typename T>
+static magma_int_t gemm_launch(magma_trans_t ta, magma_trans_t tb, const GemmSizes& g, T alpha, const T* const* A,
+                               const T* const* B, T beta, T** C, int batch, int max_m, int max_n, cudaStream_t s) {
+    const int tiles_m = ceildiv(max_m, 64), tiles_n = ceildiv(max_n, 64);
+    const long blocks = (long)batch * tiles_m * tiles_n;
+    if (blocks > 0x7fffffffL) return MAGMA_ERR_NOT_SUPPORTED;
+    const bool TA = (ta != MagmaNoTrans), TB = (tb != MagmaNoTrans);   // real types: ConjTrans == Trans
+    const dim3 grid((unsigned)blocks);
+    if (!TA && !TB) gemm_tile_kernel<T, false, false><<<grid, 256, 0, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n);
+    else if (!TA && TB) gemm_tile_kernel<T, false, true><<<grid, 256, 0, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n);
+    else if (TA && !TB) gemm_tile_kernel<T, true, false><<<grid, 256, 0, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n);
+    else gemm_tile_kernel<T, true, true><<<grid, 256, 0, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n);
+    return launch_status();
+}
+
+static bool bad_trans(magma_trans_t t) { return t != MagmaNoTrans && t != MagmaTrans && t != MagmaConjTrans; }
+
+// magmablas/dgemm_batched_core.cu:180-213: transA -1, transB -2, m -3, n -4, k -5,
+// ldda -8, lddb -10, lddc -13; quick return when m, n or k <= 0.
+template <typename T>
+static void gemm_batched(const char* name, magma_trans_t ta, magma_trans_t tb, int m, int n, int k, T alpha,
+                         const T* const* A, int lda, const T* const* B, int ldb, T beta, T** C, int ldc, int batch,
+                         magma_queue_t queue) {
+    int info = 0;
+    if (bad_trans(ta)) info = -1;
+    else if (bad_trans(tb)) info = -2;
+    else if (m < 0) info = -3;
+    else if (n < 0) info = -4;
+    else if (k < 0) info = -5;
+    else if (ta == MagmaNoTrans ? lda < m : lda < k) info = -8;
+    else if (tb == MagmaNoTrans ? ldb < k : ldb < n) info = -10;
+    else if (ldc < m) info = -13;
+    if (info != 0) {
+        magma_xerbla(name, -info);
+        return;
+    }
+    if (m <= 0 || n <= 0 || k <= 0 || batch <= 0) return;
+    GemmSizes g{m, n, k, lda, ldb, ldc, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    gemm_launch<T>(ta, tb, g, alpha, A, B, beta, C, batch, m, n, queue->stream);
+}
+
+// magmablas/zgemm_vbatched.cpp:19-29 (_max_nocheck): quick return when a max is <= 0.
+template <typename T>
+static void gemm_vbatched_max_nocheck(magma_trans_t ta, magma_trans_t tb, int* m, int* n, int* k, T alpha,
+                                      const T* const* A, int* lda, const T* const* B, int* ldb, T beta, T** C,
+                                      int* ldc, int batch, int max_m, int max_n, int max_k, magma_queue_t queue) {
+    if (max_m <= 0 || max_n <= 0 || max_k <= 0 || batch <= 0) return;
+    GemmSizes g{0, 0, 0, 0, 0, 0, m, n, k, lda, ldb, ldc};
+    gemm_launch<T>(ta, tb, g, alpha, A, B, beta, C, batch, max_m, max_n, queue->stream);
+}
+
+// magmablas/vbatched_check.cu:48-100 (gemm checker): transA -1, transB -2, m -3, n -4, k -5,
+// ldda -8, lddb -10, lddc -13, batchCount -14. Returns the code; fills the maxima.
+static int gemm_vbatched_check(magma_trans_t ta, magma_trans_t tb, int* m, int* n, int* k, int* lda, int* ldb,
+                               int* ldc, int batch, magma_queue_t queue, int mx[3]) {
+    if (bad_trans(ta)) return -1;
+    if (bad_trans(tb)) return -2;
+    if (batch < 0) return -14;
+    mx[0] = mx[1] = mx[2] = 0;
+    if (batch == 0) return 0;
+    int r[6];
+    if (reduce_sizes(m, n, k, batch, queue, r)) return MAGMA_ERR_UNKNOWN;
+    if (r[3] < 0) return -3;
+    if (r[4] < 0) return -4;
+    if (r[5] < 0) return -5;
+    int s = 0;
+    if (ld_slack(ta == MagmaNoTrans ? m : k, lda, batch, queue, &s)) return MAGMA_ERR_UNKNOWN;
+    if (s < 0) return -8;
+    if (ld_slack(tb == MagmaNoTrans ? k : n, ldb, batch, queue, &s)) return MAGMA_ERR_UNKNOWN;
+    if (s < 0) return -10;
+    if (ld_slack(m, ldc, batch, queue, &s)) return MAGMA_ERR_UNKNOWN;
+    if (s < 0) return -13;
+    mx[0] = r[0]; mx[1] = r[1]; mx[2] = r[2];
+    return 0;
+}
+
+}  // namespace mb200
+
+using namespace mb200;
+
+#define MB200_GEMM_API(P, T)                                                                                          \
+    void magmablas_##P##gemm_batched(magma_trans_t ta, magma_trans_t tb, magma_int_t m, magma_int_t n, magma_int_t k, \
+                                     T alpha, T const* const* dA_array, magma_int_t ldda, T const* const* dB_array,   \
+                                     magma_int_t lddb, T beta, T** dC_array, magma_int_t lddc, magma_int_t batchCount, \
+                                     magma_queue_t queue) {                                                           \
+        gemm_batched<T>(__func__, ta, tb, m, n, k, alpha, dA_array, ldda, dB_array, lddb, beta, dC_array, lddc,       \
+                        batchCount, queue);                                                                           \
+    }                                                                                                                 \
+    void magma_##P##gemm_batched(magma_trans_t ta, magma_trans_t tb, magma_int_t m, magma_int_t n, magma_int_t k,     \
+                                 T alpha, T const* const* dA_array, magma_int_t ldda, T const* const* dB_array,       \
+                                 magma_int_t lddb, T beta, T** dC_array, magma_int_t lddc, magma_int_t batchCount,     \
+                                 magma_queue_t queue) {                                                               \
+        gemm_batched<T>(__func__, ta, tb, m, n, k, alpha, dA_array, ldda, dB_array, lddb, beta, dC_array, lddc,       \
+                        batchCount, queue);                                                                           \
+    }                                                                                                                 \
+    void magmablas_##P##gemm_vbatched_max_nocheck(                                                                    \
+        magma_trans_t ta, magma_trans_t tb, magma_int_t* m, magma_int_t* n, magma_int_t* k, T alpha,                  \
+        T const* const* dA_array, magma_int_t* ldda, T const* const* dB_array, magma_int_t* lddb, T beta,             \
+        T** dC_array, magma_int_t* lddc, magma_int_t batchCount, magma_int_t max_m, magma_int_t max_n,                \
+        magma_int_t max_k, magma_queue_t queue) {                                                                     \
+        gemm_vbatched_max_nocheck<T>(ta, tb, m, n, k, alpha, dA_array, ldda, dB_array, lddb, beta, dC_array, lddc,    \
+                                     batchCount, max_m, max_n, max_k, queue);                                        \
+    }                                                                                                                 \
+    void magmablas_##P##gemm_vbatched_max(magma_trans_t ta, magma_trans_t tb, magma_int_t* m, magma_int_t* n,         \
+                                          magma_int_t* k, T alpha, T const* const* dA_array, magma_int_t* ldda,       \
+                                          T const* const* dB_array, magma_int_t* lddb, T beta, T** dC_array,          \
+                                          magma_int_t* lddc, magma_int_t batchCount, magma_int_t max_m,               \
+                                          magma_int_t max_n, magma_int_t max_k, magma_queue_t queue) {                \
+        int mx[3];                                                                                                    \
+        const int info = gemm_vbatched_check(ta, tb, m, n, k, ldda, lddb, lddc, batchCount, queue, mx);              \
+        if (info != 0) {                                                                                              \
+            magma_xerbla(__func__, -info);                                                                            \
+            return;                                                                                                   \
+        }                                                                                                             \
+        gemm_vbatched_max_nocheck<T>(ta, tb, m, n, k, alpha, dA_array, ldda, dB_array, lddb, beta, dC_array, lddc,    \
+                                     batchCount, max_m, max_n, max_k, queue);                                        \
+    }                                                                                                                 \
+    void magmablas_##P##gemm_vbatched_nocheck(magma_trans_t ta, magma_trans_t tb, magma_int_t* m, magma_int_t* n,     \
+                                              magma_int_t* k, T alpha, T const* const* dA_array, magma_int_t* ldda,   \
+                                              T const* const* dB_array, magma_int_t* lddb, T beta, T** dC_array,      \
+                                              magma_int_t* lddc, magma_int_t batchCount, magma_queue_t queue) {       \
+        int r[6];                                                                                                     \
+        if (batchCount <= 0 || reduce_sizes(m, n, k, batchCount, queue, r)) return;                                   \
+        gemm_vbatched_max_nocheck<T>(ta, tb, m, n, k, alpha, dA_array, ldda, dB_array, lddb, beta, dC_array, lddc,    \
+                                     batchCount, r[0], r[1], r[2], queue);                                            \
+    }                                                                                                                 \
+    void magmablas_##P##gemm_vbatched(magma_trans_t ta, magma_trans_t tb, magma_int_t* m, magma_int_t* n,             \
+                                      magma_int_t* k, T alpha, T const* const* dA_array, magma_int_t* ldda,           \
+                                      T const* const* dB_array, magma_int_t* lddb, T beta, T** dC_array,              \
+                                      magma_int_t* lddc, magma_int_t batchCount, magma_queue_t queue) {               \
+        int mx[3];                                                                                                    \
+        const int info = gemm_vbatched_check(ta, tb, m, n, k, ldda, lddb, lddc, batchCount, queue, mx);              \
+        if (info != 0) {                                                                                              \
+            magma_xerbla(__func__, -info);                                                                            \
+            return;                                                                                                   \
+        }                                                                                                             \
+        gemm_vbatched_max_nocheck<T>(ta, tb, m, n, k, alpha, dA_array, ldda, dB_array, lddb, beta, dC_array, lddc,    \
+                                     batchCount, mx[0], mx[1], mx[2], queue);                                        \
+    }
+
+extern "C" {
+MB200_GEMM_API(d, double)
+MB200_GEMM_API(s, float)
+}

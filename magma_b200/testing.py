@@ -143,3 +143,40 @@ def lu_residual(A0_cm: np.ndarray, LU_cm: np.ndarray, ipiv: np.ndarray, m: int, 
                 A[[j, p], :] = A[[p, j], :]
         out[b] = np.linalg.norm(A - L @ U) / (np.linalg.norm(A) * n)
     return out
+
+
+def svd_logrand_torch(batch: int, n: int, kappa_lo: float = 1e2, kappa_hi: float = 1e6, nrhs: int = 4,
+                      seed: int = 3, device="cuda"):
+    """GPU version of svd_logrand for benchmark-sized batches (torch's seeded generator;
+    U, V from the QR of Gaussians with R's diagonal made positive). Returns
+    (A (batch, n, n) column-major, B (batch, nrhs, n), kappa (batch,)) as CUDA tensors."""
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+
+    def haar_t():
+        G = torch.randn(batch, n, n, dtype=torch.float64, device=device, generator=g)
+        Q, R = torch.linalg.qr(G)
+        d = torch.sign(torch.diagonal(R, dim1=1, dim2=2))
+        d[d == 0] = 1.0
+        return Q * d[:, None, :]
+
+    kap = torch.exp(math.log(kappa_lo) + torch.rand(batch, dtype=torch.float64, device=device, generator=g)
+                    * (math.log(kappa_hi) - math.log(kappa_lo)))
+    sig = torch.exp(torch.rand(batch, n, dtype=torch.float64, device=device, generator=g)
+                    * torch.log(1.0 / kap)[:, None])
+    A_row = (haar_t() * sig[:, None, :]) @ haar_t().transpose(1, 2)
+    A = A_row.transpose(1, 2).contiguous()
+    B = torch.randn(batch, nrhs, n, dtype=torch.float64, device=device, generator=g)
+    return A, B, kap
+
+
+def backward_error_torch(A_cm, X_cm, B_cm):
+    """Normwise backward error per instance and RHS on the GPU (FP64; checker only)."""
+    A = A_cm.transpose(1, 2)
+    X = X_cm.transpose(1, 2)
+    Bm = B_cm.transpose(1, 2)
+    R = Bm - A @ X
+    anorm = A.abs().sum(dim=2).amax(dim=1)
+    return R.abs().amax(dim=1) / (anorm[:, None] * X.abs().amax(dim=1) + Bm.abs().amax(dim=1))
