@@ -138,6 +138,37 @@ magma_int_t magma_dgesv_batched(magma_int_t n, magma_int_t nrhs, double** dA_arr
                                 magma_int_t* dinfo_array, magma_int_t batchCount, magma_queue_t queue);
 
 
+/* Variable-size batched LU. No counterpart in MAGMA 2.2 (its only vbatched
+ * LAPACK routine is potrf, include/magma_zvbatched.h:29-70); defined by analogy
+ * with magma_dpotrf_vbatched: m, n, nrhs, ldda, lddb are device arrays of
+ * batchCount+1 entries; checked forms reduce the sizes on the device (one host
+ * synchronisation), _max_nocheck forms take the maxima and never synchronise.
+ * max(m, n) <= 1024. Pivots, info and factors as magma_dgetrf_batched.
+ * Checks: getrf m -1, n -2, ldda -4, batchCount -7; getrs trans -1, n -2,
+ * nrhs -3, ldda -5, lddb -8, batchCount -10; gesv n -1, nrhs -2, ldda -4,
+ * lddb -7, batchCount -9. */
+magma_int_t magma_dgetrf_vbatched(magma_int_t* m, magma_int_t* n, double** dA_array, magma_int_t* ldda,
+                                  magma_int_t** ipiv_array, magma_int_t* info_array, magma_int_t batchCount,
+                                  magma_queue_t queue);
+magma_int_t magma_dgetrf_vbatched_max_nocheck(magma_int_t* m, magma_int_t* n, double** dA_array, magma_int_t* ldda,
+                                              magma_int_t** ipiv_array, magma_int_t* info_array,
+                                              magma_int_t batchCount, magma_int_t max_m, magma_int_t max_n,
+                                              magma_queue_t queue);
+magma_int_t magma_dgetrs_vbatched(magma_trans_t trans, magma_int_t* n, magma_int_t* nrhs, double** dA_array,
+                                  magma_int_t* ldda, magma_int_t** dipiv_array, double** dB_array, magma_int_t* lddb,
+                                  magma_int_t batchCount, magma_queue_t queue);
+magma_int_t magma_dgetrs_vbatched_max_nocheck(magma_trans_t trans, magma_int_t* n, magma_int_t* nrhs,
+                                              double** dA_array, magma_int_t* ldda, magma_int_t** dipiv_array,
+                                              double** dB_array, magma_int_t* lddb, magma_int_t batchCount,
+                                              magma_int_t max_n, magma_int_t max_nrhs, magma_queue_t queue);
+magma_int_t magma_dgesv_vbatched(magma_int_t* n, magma_int_t* nrhs, double** dA_array, magma_int_t* ldda,
+                                 magma_int_t** dipiv_array, double** dB_array, magma_int_t* lddb,
+                                 magma_int_t* dinfo_array, magma_int_t batchCount, magma_queue_t queue);
+magma_int_t magma_dgesv_vbatched_max_nocheck(magma_int_t* n, magma_int_t* nrhs, double** dA_array, magma_int_t* ldda,
+                                             magma_int_t** dipiv_array, double** dB_array, magma_int_t* lddb,
+                                             magma_int_t* dinfo_array, magma_int_t batchCount, magma_int_t max_n,
+                                             magma_int_t max_nrhs, magma_queue_t queue);
+
 /* Single-precision forms (generated from the same templates in MAGMA:
  * src/zgetrf_batched.cpp:83, src/zgetrs_batched.cpp:87, src/zgesv_batched.cpp:93). */
 magma_int_t magma_sgetrf_batched(magma_int_t m, magma_int_t n, float** dA_array, magma_int_t ldda,

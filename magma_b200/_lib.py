@@ -59,6 +59,12 @@ SIGNATURES: dict[str, tuple] = {
     "magma_dgetrf_batched": (_i, [_i, _i, _p, _i, _p, _p, _i, _p]),
     "magma_dgetrs_batched": (_i, [_i, _i, _i, _p, _i, _p, _p, _i, _i, _p]),
     "magma_dgesv_batched": (_i, [_i, _i, _p, _i, _p, _p, _i, _p, _i, _p]),
+    "magma_dgetrf_vbatched": (_i, [_p, _p, _p, _p, _p, _p, _i, _p]),
+    "magma_dgetrf_vbatched_max_nocheck": (_i, [_p, _p, _p, _p, _p, _p, _i, _i, _i, _p]),
+    "magma_dgetrs_vbatched": (_i, [_i, _p, _p, _p, _p, _p, _p, _p, _i, _p]),
+    "magma_dgetrs_vbatched_max_nocheck": (_i, [_i, _p, _p, _p, _p, _p, _p, _p, _i, _i, _i, _p]),
+    "magma_dgesv_vbatched": (_i, [_p, _p, _p, _p, _p, _p, _p, _p, _i, _p]),
+    "magma_dgesv_vbatched_max_nocheck": (_i, [_p, _p, _p, _p, _p, _p, _p, _p, _i, _i, _i, _p]),
     "magma_sgetrf_batched": (_i, [_i, _i, _p, _i, _p, _p, _i, _p]),
     "magma_sgetrs_batched": (_i, [_i, _i, _i, _p, _i, _p, _p, _i, _i, _p]),
     "magma_sgesv_batched": (_i, [_i, _i, _p, _i, _p, _p, _i, _p, _i, _p]),
@@ -89,6 +95,14 @@ SIGNATURES: dict[str, tuple] = {
                                                     _i, _p]),
     "magmablas_sgemm_vbatched_max": (None, [_i, _i, _p, _p, _p, _f, _p, _p, _p, _p, _f, _p, _p, _i, _i, _i, _i, _p]),
     "magmablas_sgemm_vbatched_nocheck": (None, [_i, _i, _p, _p, _p, _f, _p, _p, _p, _p, _f, _p, _p, _i, _p]),
+    # request loop (include/magma_b200_serve.h)
+    "magma_b200_server_create": (_i, [_i, _sz, _i, _i, C.POINTER(_p)]),
+    "magma_b200_server_submit": (_i, [_p, _i, _i, _i, _p, _i, _p, _i, _p, _i, C.c_longlong]),
+    "magma_b200_server_poll": (_i, [_p, _p, _p, _p, _p, _i]),
+    "magma_b200_server_drain": (_i, [_p]),
+    "magma_b200_server_stats": (None, [_p, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
+                                       C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
+    "magma_b200_server_destroy": (_i, [_p]),
 }
 
 _lib: C.CDLL | None = None

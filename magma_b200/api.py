@@ -291,3 +291,56 @@ def gemm_vbatched(A: "VarBatch", B: "VarBatch", C: "VarBatch", m, n, k, lda, ldb
         getattr(q.lib, f"magmablas_{pre}gemm_vbatched_max_nocheck")(*args, *max_sizes, q.handle)
     else:
         getattr(q.lib, f"magmablas_{pre}gemm_vbatched")(*args, q.handle)
+
+
+# --------------------------------------------------------------- variable-size LU
+def dgesv_vbatched(A: "VarBatch", B: "VarBatch | None", n, nrhs=None, lda=None, ldb=None, m=None, factor=True,
+                   solve=True, trans=False, ipiv: torch.Tensor | None = None, max_sizes=None,
+                   queue: Queue | None = None):
+    """Variable-size getrf / getrs / gesv through the C ABI.
+
+    Returns (ipiv (batch, max) int32 device tensor, info device tensor or None). For getrs
+    pass the ipiv returned by the factorisation. max_sizes selects the _max_nocheck forms
+    ((max_m, max_n) for getrf, (max_n, max_nrhs) otherwise)."""
+    import numpy as np
+
+    q = queue or default_queue()
+    L = q.lib
+    batch = A.batch
+    n = np.asarray(n, np.int32)
+    m = n if m is None else np.asarray(m, np.int32)
+    lda = [s[1] for s in A.shapes] if lda is None else lda
+    dm, dn, dla = A.ints(m), A.ints(n), A.ints(lda)
+    width = int(max(1, np.minimum(m, n).max() if batch else 1))
+    if ipiv is None:
+        ipiv = torch.zeros((batch, width), dtype=torch.int32, device=A.device)
+    pP = ptr_array(ipiv)
+    info = torch.empty(batch + 1, dtype=torch.int32, device=A.device)
+    if factor and not solve:
+        if max_sizes:
+            rc = L.magma_dgetrf_vbatched_max_nocheck(_vp(dm), _vp(dn), _vp(A.ptrs), _vp(dla), _vp(pP), _vp(info),
+                                                     batch, max_sizes[0], max_sizes[1], q.handle)
+        else:
+            rc = L.magma_dgetrf_vbatched(_vp(dm), _vp(dn), _vp(A.ptrs), _vp(dla), _vp(pP), _vp(info), batch, q.handle)
+        _check(rc, "magma_dgetrf_vbatched")
+        return ipiv, info[:batch]
+    dnr = A.ints(nrhs)
+    dlb = A.ints([s[1] for s in B.shapes] if ldb is None else ldb)
+    if solve and not factor:
+        if max_sizes:
+            rc = L.magma_dgetrs_vbatched_max_nocheck(_trans(trans), _vp(dn), _vp(dnr), _vp(A.ptrs), _vp(dla), _vp(pP),
+                                                     _vp(B.ptrs), _vp(dlb), batch, max_sizes[0], max_sizes[1],
+                                                     q.handle)
+        else:
+            rc = L.magma_dgetrs_vbatched(_trans(trans), _vp(dn), _vp(dnr), _vp(A.ptrs), _vp(dla), _vp(pP),
+                                         _vp(B.ptrs), _vp(dlb), batch, q.handle)
+        _check(rc, "magma_dgetrs_vbatched")
+        return ipiv, None
+    if max_sizes:
+        rc = L.magma_dgesv_vbatched_max_nocheck(_vp(dn), _vp(dnr), _vp(A.ptrs), _vp(dla), _vp(pP), _vp(B.ptrs),
+                                                _vp(dlb), _vp(info), batch, max_sizes[0], max_sizes[1], q.handle)
+    else:
+        rc = L.magma_dgesv_vbatched(_vp(dn), _vp(dnr), _vp(A.ptrs), _vp(dla), _vp(pP), _vp(B.ptrs), _vp(dlb),
+                                    _vp(info), batch, q.handle)
+    _check(rc, "magma_dgesv_vbatched")
+    return ipiv, info[:batch]

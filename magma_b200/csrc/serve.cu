@@ -1,0 +1,381 @@
+// serve.cu -- continuous-batching request loop for batched LU / Cholesky solves
+// (include/magma_b200_serve.h). No counterpart in the reference.
+//
+// Three parties share the server state under one mutex:
+//   callers     submit requests into a FIFO (`pending`);
+//   dispatcher  admits requests from the head of the FIFO while their device memory
+//               (A, B, ipiv) fits in the arena (first-fit free list), takes everything
+//               admitted as one micro-batch, and launches it on a free stream slot:
+//               host->device copies, one metadata upload, one variable-size LU call
+//               (magma_dgesv_vbatched_max_nocheck) and one variable-size Cholesky call
+//               (magma_dposv_vbatched_max_nocheck), result copies back, an event;
+//   completer   waits for the oldest in-flight batch's event, publishes its results,
+//               frees their arena memory and the slot, and wakes the dispatcher.
+// With several slots, a batch's copies and kernels overlap the previous batch's.
+#include "internal.h"
+#include "vbatched.h"
+#include "../../include/magma_b200_serve.h"
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+namespace {
+
+long long now_ns() {
+    return std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// First-fit allocator over [0, size) with coalescing of freed neighbours.
+class Arena {
+   public:
+    explicit Arena(size_t size) { free_[0] = size; }
+    bool alloc(size_t bytes, size_t* off) {
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second >= bytes) {
+                *off = it->first;
+                const size_t rest = it->second - bytes, start = it->first + bytes;
+                free_.erase(it);
+                if (rest) free_[start] = rest;
+                used_ += bytes;
+                peak_ = std::max(peak_, used_);
+                return true;
+            }
+        }
+        return false;
+    }
+    void release(size_t off, size_t bytes) {
+        used_ -= bytes;
+        auto it = free_.emplace(off, bytes).first;
+        auto nx = std::next(it);
+        if (nx != free_.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            free_.erase(nx);
+        }
+        if (it != free_.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
+    size_t peak() const { return peak_; }
+
+   private:
+    std::map<size_t, size_t> free_;
+    size_t used_ = 0, peak_ = 0;
+};
+
+struct Request {
+    int kind, n, nrhs, lda, ldb, ldx;
+    const double* A;
+    const double* B;
+    double* X;
+    long long tag, t_submit = 0, t_done = 0;
+    size_t off = 0, bytes = 0;
+    int info = 0;
+    size_t offA() const { return off; }
+    size_t offB() const { return off + align256(sizeof(double) * n * n); }
+    size_t offP() const { return offB() + align256(sizeof(double) * n * nrhs); }
+    static size_t need(int n, int nrhs) {
+        return align256(sizeof(double) * n * n) + align256(sizeof(double) * n * nrhs) + align256(sizeof(int) * n);
+    }
+};
+
+// Per-batch metadata for one solver family (LU or Cholesky): size arrays with
+// count+1 entries and pointer arrays, laid out back to back.
+struct MetaLayout {
+    size_t n, nrhs, lda, ldb, pa, pb, pp, info, bytes;
+    explicit MetaLayout(int cap) {
+        const size_t ints = align256(sizeof(int) * (cap + 1)), ptrs = align256(sizeof(void*) * cap);
+        n = 0; nrhs = n + ints; lda = nrhs + ints; ldb = lda + ints;
+        pa = ldb + ints; pb = pa + ptrs; pp = pb + ptrs; info = pp + ptrs; bytes = info + ints;
+    }
+};
+
+struct Slot {
+    cudaStream_t stream = nullptr;
+    magma_queue_t queue = nullptr;
+    cudaEvent_t done = nullptr;
+    char* h_meta = nullptr;   // pinned: [LU meta][Cholesky meta]
+    char* d_meta = nullptr;
+    std::vector<Request*> reqs;
+    bool busy = false;
+};
+
+}  // namespace
+
+struct magma_b200_server {
+    int device = 0, max_batch = 0;
+    size_t budget = 0;
+    char* arena_base = nullptr;
+    Arena arena{0};
+    std::vector<Slot> slots;
+    MetaLayout meta{1};
+    std::mutex mu;
+    std::condition_variable cv_dispatch, cv_complete, cv_drain;
+    std::deque<Request*> pending;
+    std::deque<Slot*> inflight;
+    std::vector<Request*> finished;
+    long long submitted = 0, completed = 0, batches = 0;
+    bool stop = false;
+    std::thread dispatcher, completer;
+
+    void dispatch_loop();
+    void complete_loop();
+    void launch(Slot& s);
+};
+
+void magma_b200_server::launch(Slot& s) {
+    cudaSetDevice(device);
+    // host -> device copies of every request's A and B (packed with ld = n)
+    for (Request* r : s.reqs) {
+        cudaMemcpy2DAsync(arena_base + r->offA(), sizeof(double) * r->n, r->A, sizeof(double) * r->lda,
+                          sizeof(double) * r->n, r->n, cudaMemcpyHostToDevice, s.stream);
+        cudaMemcpy2DAsync(arena_base + r->offB(), sizeof(double) * r->n, r->B, sizeof(double) * r->ldb,
+                          sizeof(double) * r->n, r->nrhs, cudaMemcpyHostToDevice, s.stream);
+    }
+    // metadata for the two families
+    int cnt[2] = {0, 0}, maxn[2] = {0, 0}, maxr[2] = {0, 0};
+    for (int f = 0; f < 2; ++f) {
+        char* h = s.h_meta + f * meta.bytes;
+        int* n = reinterpret_cast<int*>(h + meta.n);
+        int* nr = reinterpret_cast<int*>(h + meta.nrhs);
+        int* la = reinterpret_cast<int*>(h + meta.lda);
+        int* lb = reinterpret_cast<int*>(h + meta.ldb);
+        void** pa = reinterpret_cast<void**>(h + meta.pa);
+        void** pb = reinterpret_cast<void**>(h + meta.pb);
+        void** pp = reinterpret_cast<void**>(h + meta.pp);
+        for (Request* r : s.reqs) {
+            if (r->kind != f) continue;
+            const int i = cnt[f]++;
+            n[i] = r->n; nr[i] = r->nrhs; la[i] = r->n; lb[i] = r->n;
+            pa[i] = arena_base + r->offA();
+            pb[i] = arena_base + r->offB();
+            pp[i] = arena_base + r->offP();
+            maxn[f] = std::max(maxn[f], r->n);
+            maxr[f] = std::max(maxr[f], r->nrhs);
+        }
+    }
+    cudaMemcpyAsync(s.d_meta, s.h_meta, 2 * meta.bytes, cudaMemcpyHostToDevice, s.stream);
+    for (int f = 0; f < 2; ++f) {
+        if (!cnt[f]) continue;
+        char* d = s.d_meta + f * meta.bytes;
+        auto I = [&](size_t o) { return reinterpret_cast<int*>(d + o); };
+        auto P = [&](size_t o) { return reinterpret_cast<double**>(d + o); };
+        if (f == MAGMA_B200_SOLVE_LU)
+            magma_dgesv_vbatched_max_nocheck(I(meta.n), I(meta.nrhs), P(meta.pa), I(meta.lda),
+                                             reinterpret_cast<int**>(d + meta.pp), P(meta.pb), I(meta.ldb),
+                                             I(meta.info), cnt[f], maxn[f], maxr[f], s.queue);
+        else
+            magma_dposv_vbatched_max_nocheck(MagmaLower, I(meta.n), I(meta.nrhs), P(meta.pa), I(meta.lda),
+                                             P(meta.pb), I(meta.ldb), I(meta.info), cnt[f], maxn[f], maxr[f],
+                                             s.queue);
+    }
+    // results back: X and info
+    for (Request* r : s.reqs)
+        cudaMemcpy2DAsync(r->X, sizeof(double) * r->ldx, arena_base + r->offB(), sizeof(double) * r->n,
+                          sizeof(double) * r->n, r->nrhs, cudaMemcpyDeviceToHost, s.stream);
+    for (int f = 0; f < 2; ++f)
+        if (cnt[f])
+            cudaMemcpyAsync(s.h_meta + f * meta.bytes + meta.info, s.d_meta + f * meta.bytes + meta.info,
+                            sizeof(int) * cnt[f], cudaMemcpyDeviceToHost, s.stream);
+    cudaEventRecord(s.done, s.stream);
+}
+
+void magma_b200_server::dispatch_loop() {
+    cudaSetDevice(device);
+    std::unique_lock<std::mutex> lk(mu);
+    for (;;) {
+        Slot* free_slot = nullptr;
+        cv_dispatch.wait(lk, [&] {
+            if (stop) return true;
+            free_slot = nullptr;
+            for (Slot& s : slots)
+                if (!s.busy) { free_slot = &s; break; }
+            if (!free_slot || pending.empty()) return false;
+            size_t off;   // can the head be admitted now?
+            if (!arena.alloc(pending.front()->bytes, &off)) return false;
+            arena.release(off, pending.front()->bytes);
+            return true;
+        });
+        if (stop) return;
+        Slot& s = *free_slot;
+        s.reqs.clear();
+        while (!pending.empty() && (int)s.reqs.size() < max_batch) {
+            Request* r = pending.front();
+            if (!arena.alloc(r->bytes, &r->off)) break;   // FIFO admission by memory budget
+            pending.pop_front();
+            s.reqs.push_back(r);
+        }
+        s.busy = true;
+        ++batches;
+        lk.unlock();
+        launch(s);
+        lk.lock();
+        inflight.push_back(&s);
+        cv_complete.notify_one();
+    }
+}
+
+void magma_b200_server::complete_loop() {
+    cudaSetDevice(device);
+    std::unique_lock<std::mutex> lk(mu);
+    for (;;) {
+        cv_complete.wait(lk, [&] { return stop || !inflight.empty(); });
+        if (inflight.empty() && stop) return;
+        Slot* s = inflight.front();
+        lk.unlock();
+        cudaEventSynchronize(s->done);
+        const long long t = now_ns();
+        lk.lock();
+        inflight.pop_front();
+        int idx[2] = {0, 0};
+        for (Request* r : s->reqs) {
+            const int* info = reinterpret_cast<const int*>(s->h_meta + r->kind * meta.bytes + meta.info);
+            r->info = info[idx[r->kind]++];
+            r->t_done = t;
+            arena.release(r->off, r->bytes);
+            finished.push_back(r);
+            ++completed;
+        }
+        s->reqs.clear();
+        s->busy = false;
+        cv_dispatch.notify_one();
+        cv_drain.notify_all();
+    }
+}
+
+extern "C" {
+
+magma_int_t magma_b200_server_create(magma_int_t device, size_t budget_bytes, magma_int_t streams,
+                                     magma_int_t max_batch, magma_b200_server_t* out) {
+    if (streams < 1 || max_batch < 1 || budget_bytes < 4096) return MAGMA_ERR_ILLEGAL_VALUE;
+    cudaSetDevice(device);
+    auto* sv = new magma_b200_server();
+    sv->device = device;
+    sv->max_batch = max_batch;
+    sv->meta = MetaLayout(max_batch);
+    if (cudaMalloc(&sv->arena_base, budget_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        delete sv;
+        return MAGMA_ERR_DEVICE_ALLOC;
+    }
+    sv->arena = Arena(budget_bytes);
+    sv->budget = budget_bytes;
+    sv->slots.resize(streams);
+    for (Slot& s : sv->slots) {
+        cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
+        magma_queue_create_from_cuda_internal(device, s.stream, nullptr, nullptr, &s.queue, "server", __FILE__,
+                                              __LINE__);
+        // bucket lists of the vbatched calls: reserve once so batches never grow the workspace
+        magma_queue_reserve_workspace(s.queue, sizeof(int) * mb200::bucketize_ws_ints(max_batch, 16));
+        cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming);
+        if (cudaHostAlloc(reinterpret_cast<void**>(&s.h_meta), 2 * sv->meta.bytes, cudaHostAllocDefault) !=
+                cudaSuccess ||
+            cudaMalloc(&s.d_meta, 2 * sv->meta.bytes) != cudaSuccess) {
+            cudaGetLastError();
+            magma_b200_server_destroy(sv);
+            return MAGMA_ERR_DEVICE_ALLOC;
+        }
+    }
+    sv->dispatcher = std::thread([sv] { sv->dispatch_loop(); });
+    sv->completer = std::thread([sv] { sv->complete_loop(); });
+    *out = sv;
+    return MAGMA_SUCCESS;
+}
+
+magma_int_t magma_b200_server_submit(magma_b200_server_t sv, magma_int_t kind, magma_int_t n, magma_int_t nrhs,
+                                     const double* A, magma_int_t lda, const double* B, magma_int_t ldb, double* X,
+                                     magma_int_t ldx, long long tag) {
+    if (kind != MAGMA_B200_SOLVE_LU && kind != MAGMA_B200_SOLVE_CHOLESKY) return -1;
+    if (n < 1) return -2;
+    if (nrhs < 1) return -3;
+    if (!A) return -4;
+    if (lda < n) return -5;
+    if (!B) return -6;
+    if (ldb < n) return -7;
+    if (!X) return -8;
+    if (ldx < n) return -9;
+    if (n > 1024) return MAGMA_ERR_NOT_SUPPORTED;
+    auto* r = new Request{(int)kind, (int)n, (int)nrhs, (int)lda, (int)ldb, (int)ldx, A, B, X, tag};
+    r->bytes = Request::need(n, nrhs);
+    if (r->bytes > sv->budget) {   // could never be admitted
+        delete r;
+        return MAGMA_ERR_NOT_SUPPORTED;
+    }
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        r->t_submit = now_ns();
+        sv->pending.push_back(r);
+        ++sv->submitted;
+    }
+    sv->cv_dispatch.notify_one();
+    return MAGMA_SUCCESS;
+}
+
+magma_int_t magma_b200_server_poll(magma_b200_server_t sv, long long* tags, magma_int_t* infos, long long* t_submit,
+                                   long long* t_done, magma_int_t max) {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    const int k = std::min<int>(max, (int)sv->finished.size());
+    for (int i = 0; i < k; ++i) {
+        Request* r = sv->finished[i];
+        tags[i] = r->tag;
+        infos[i] = r->info;
+        t_submit[i] = r->t_submit;
+        t_done[i] = r->t_done;
+        delete r;
+    }
+    sv->finished.erase(sv->finished.begin(), sv->finished.begin() + k);
+    return k;
+}
+
+magma_int_t magma_b200_server_drain(magma_b200_server_t sv) {
+    std::unique_lock<std::mutex> lk(sv->mu);
+    sv->cv_drain.wait(lk, [&] { return sv->completed == sv->submitted; });
+    return MAGMA_SUCCESS;
+}
+
+void magma_b200_server_stats(magma_b200_server_t sv, long long* submitted, long long* completed, long long* batches,
+                             long long* peak_bytes) {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    *submitted = sv->submitted;
+    *completed = sv->completed;
+    *batches = sv->batches;
+    *peak_bytes = (long long)sv->arena.peak();
+}
+
+magma_int_t magma_b200_server_destroy(magma_b200_server_t sv) {
+    if (!sv) return MAGMA_SUCCESS;
+    if (sv->dispatcher.joinable()) magma_b200_server_drain(sv);
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        sv->stop = true;
+    }
+    sv->cv_dispatch.notify_all();
+    sv->cv_complete.notify_all();
+    if (sv->dispatcher.joinable()) sv->dispatcher.join();
+    if (sv->completer.joinable()) sv->completer.join();
+    for (Slot& s : sv->slots) {
+        if (s.queue) magma_queue_destroy_internal(s.queue, "server", __FILE__, __LINE__);
+        if (s.stream) cudaStreamDestroy(s.stream);
+        if (s.done) cudaEventDestroy(s.done);
+        if (s.h_meta) cudaFreeHost(s.h_meta);
+        if (s.d_meta) cudaFree(s.d_meta);
+    }
+    for (Request* r : sv->finished) delete r;
+    if (sv->arena_base) cudaFree(sv->arena_base);
+    delete sv;
+    return MAGMA_SUCCESS;
+}
+
+}  // extern "C"

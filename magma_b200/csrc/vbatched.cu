@@ -12,11 +12,11 @@
 
 namespace mb200 {
 
-__global__ void bucketize_kernel(const int* __restrict__ key, int batch, BucketEdges edges,
-                                 int* __restrict__ counts, int* __restrict__ lists) {
+__global__ void bucketize_kernel(const int* __restrict__ key, const int* __restrict__ key2, int batch,
+                                 BucketEdges edges, int* __restrict__ counts, int* __restrict__ lists) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= batch) return;
-    const int v = key[i];
+    const int v = key2 ? ((key[i] <= 0 || key2[i] <= 0) ? 0 : max(key[i], key2[i])) : key[i];
     if (v <= 0) return;                       // empty instances need no work
     int b = 0;
     while (b < edges.n - 1 && v > edges.e[b]) ++b;
@@ -62,6 +62,11 @@ __global__ void init_ints_kernel(int* p, int n, int v0, int v1, int split) {
 
 magma_int_t bucketize(const int* key, int batch, const int* edges_host, int nb, cudaStream_t s, int* ws,
                       int** counts_out, int** lists_out) {
+    return bucketize2(key, nullptr, batch, edges_host, nb, s, ws, counts_out, lists_out);
+}
+
+magma_int_t bucketize2(const int* key, const int* key2, int batch, const int* edges_host, int nb, cudaStream_t s,
+                       int* ws, int** counts_out, int** lists_out) {
     // ws layout: [counts nb (padded to 2*nb)][lists nb*batch]; the edges travel as a kernel argument
     if (nb > BucketEdges::kMax) return MAGMA_ERR_NOT_SUPPORTED;
     BucketEdges edges;
@@ -70,7 +75,7 @@ magma_int_t bucketize(const int* key, int batch, const int* edges_host, int nb, 
     int* d_counts = ws;
     int* d_lists = ws + 2 * nb;
     cudaMemsetAsync(d_counts, 0, sizeof(int) * nb, s);
-    bucketize_kernel<<<ceildiv(batch, 256), 256, 0, s>>>(key, batch, edges, d_counts, d_lists);
+    bucketize_kernel<<<ceildiv(batch, 256), 256, 0, s>>>(key, key2, batch, edges, d_counts, d_lists);
     *counts_out = d_counts;
     *lists_out = d_lists;
     return launch_status();

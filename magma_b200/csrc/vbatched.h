@@ -19,6 +19,9 @@ struct BucketEdges {
 magma_int_t bucketize(const int* key, int batch, const int* edges_host, int nb, cudaStream_t s, int* ws,
                       int** counts_out, int** lists_out);
 size_t bucketize_ws_ints(int batch, int nb);
+// As bucketize, keyed by max(key[i], key2[i]) (instances with a key <= 0 in either are dropped).
+magma_int_t bucketize2(const int* key, const int* key2, int batch, const int* edges_host, int nb, cudaStream_t s,
+                       int* ws, int** counts_out, int** lists_out);
 
 // out[0..2] = max of a, b, c (null arrays give 0), out[3..5] = their minima. Synchronises the queue.
 magma_int_t reduce_sizes(const int* a, const int* b, const int* c, int batch, magma_queue_t queue, int out[6]);

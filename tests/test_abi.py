@@ -79,3 +79,17 @@ def test_strerror_and_xerbla(capfd):
     lib.magma_xerbla(b"magma_dgetrf_batched", 4)
     err = capfd.readouterr().err
     assert "On entry to magma_dgetrf_batched, parameter 4 had an illegal value (info = -4)" in err
+
+
+def test_server_submit_argument_errors():
+    """magma_b200_server_submit checks its arguments before it touches the server."""
+    lib = _lib.load()
+    buf = (C.c_double * 16)()
+    p = C.cast(buf, C.c_void_p)
+    assert lib.magma_b200_server_submit(None, 2, 4, 1, p, 4, p, 4, p, 4, 0) == -1
+    assert lib.magma_b200_server_submit(None, 0, 0, 1, p, 4, p, 4, p, 4, 0) == -2
+    assert lib.magma_b200_server_submit(None, 0, 4, 0, p, 4, p, 4, p, 4, 0) == -3
+    assert lib.magma_b200_server_submit(None, 1, 4, 1, None, 4, p, 4, p, 4, 0) == -4
+    assert lib.magma_b200_server_submit(None, 0, 4, 1, p, 3, p, 4, p, 4, 0) == -5
+    assert lib.magma_b200_server_submit(None, 0, 4, 1, p, 4, p, 4, p, 2, 0) == -9
+    assert lib.magma_b200_server_submit(None, 0, 2000, 1, p, 2000, p, 2000, p, 2000, 0) == _lib.MAGMA_ERR_NOT_SUPPORTED
