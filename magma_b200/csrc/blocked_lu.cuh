@@ -15,7 +15,7 @@
 //        (LAPACK applies DLASWP to A(:,1:k0));
 //     3. for the trailing columns, in chunks of CW: the NB pivot rows are
 //        gathered into shared memory and solved with L11 (U12 = L11^-1 A12,
-//        one thread per column), then every other live row applies
+//        one thread per column, in registers), then every other live row applies
 //        A22 -= L21 U12 from its registers while moving to its new position,
 //        and the U12 rows are stored.
 //   After each panel the matrix is again in LAPACK's row order, so the next
@@ -37,6 +37,37 @@ struct BlockedLuShared {
     T   U[NB][CW];
     int src[NB];
 };
+
+// U12 = L11^-1 A12 for column c of the staged pivot rows (sh.U[0..NB-1][c]),
+// in groups of H rows held in registers: a group first takes the updates of
+// the finished rows above it (read back from shared memory), then is solved
+// in registers. Every entry receives fma(L11(r, rr), -U(rr, c), x) for rr
+// ascending -- the unblocked order. Rows past the panel's last step hold
+// unused values and are never stored.
+template <typename T, int NB, int NT, int CW>
+__device__ __forceinline__ void blocked_trsm_column(BlockedLuShared<T, NB, NT, CW>& sh, int c) {
+    constexpr int H = 8;
+    static_assert(NB % H == 0, "panel width must be a multiple of the TRSM group");
+#pragma unroll 1
+    for (int q0 = 0; q0 < NB; q0 += H) {
+        T x[H];
+#pragma unroll
+        for (int r = 0; r < H; ++r) x[r] = sh.U[q0 + r][c];
+#pragma unroll 2
+        for (int rr = 0; rr < q0; ++rr) {
+            const T u = sh.U[rr][c];
+#pragma unroll
+            for (int r = 0; r < H; ++r) x[r] = fma_rn(sh.L11[q0 + r][rr], -u, x[r]);
+        }
+        static_for<0, H>([&](auto rrc) {
+            constexpr int rr = decltype(rrc)::value;
+#pragma unroll
+            for (int r = rr + 1; r < H; ++r) x[r] = fma_rn(sh.L11[q0 + r][q0 + rr], -x[rr], x[r]);
+        });
+#pragma unroll
+        for (int r = 0; r < H; ++r) sh.U[q0 + r][c] = x[r];
+    }
+}
 
 template <typename T, int NB, int NT, int CW, int CB>
 __device__ void blocked_getrf(T* __restrict__ A, int m, int n, int lda, int* __restrict__ ipiv, int& info,
@@ -88,6 +119,16 @@ __device__ void blocked_getrf(T* __restrict__ A, int m, int n, int lda, int* __r
             }
         }
         // ---- 3. trailing columns ----
+        // A non-pivot row's own trailing entries are written only by itself, so the
+        // next CB of them are loaded one group ahead (across the barriers) to hide
+        // the load latency behind the current group's arithmetic.
+        const bool upd = live && !pivot_row;
+        T nxt[CB];
+        auto prefetch = [&](int j) {
+#pragma unroll
+            for (int c = 0; c < CB; ++c) nxt[c] = (upd && j + c < n) ? A[tid + (size_t)(j + c) * lda] : T(0);
+        };
+        prefetch(k0 + nbp);
         for (int j0 = k0 + nbp; j0 < n; j0 += CW) {
             const int cw = min(CW, n - j0);
             __syncthreads();   // sU / L11 / src ready; previous chunk's readers done
@@ -96,23 +137,19 @@ __device__ void blocked_getrf(T* __restrict__ A, int m, int n, int lda, int* __r
                 sh.U[r][c] = A[sh.src[r] + (size_t)(j0 + c) * lda];
             }
             __syncthreads();
-            // U12 = L11^-1 A12, one thread per column, fma order of the unblocked steps
-            for (int c = tid; c < cw; c += NT) {
-                for (int r = 1; r < nbp; ++r) {
-                    T x = sh.U[r][c];
-                    for (int rr = 0; rr < r; ++rr) x = fma_rn(sh.L11[r][rr], -sh.U[rr][c], x);
-                    sh.U[r][c] = x;
-                }
-            }
+            // U12 = L11^-1 A12, one thread per column, in two halves of H rows held in
+            // registers; each entry gets its fma's in ascending step order.
+            for (int c = tid; c < cw; c += NT) blocked_trsm_column<T, NB, NT, CW>(sh, c);
             __syncthreads();
             // A22 -= L21 U12 for the non-pivot live rows, stored at their new positions.
             // A row only ever overwrites the old row of a pivot (already gathered above),
             // so no barrier is needed between these loads and stores.
-            if (live && !pivot_row) {
+            if (upd) {
                 for (int c0 = 0; c0 < cw; c0 += CB) {
                     T acc[CB];
 #pragma unroll
-                    for (int c = 0; c < CB; ++c) acc[c] = (c0 + c < cw) ? A[tid + (size_t)(j0 + c0 + c) * lda] : T(0);
+                    for (int c = 0; c < CB; ++c) acc[c] = nxt[c];
+                    prefetch(j0 + c0 + CB);
                     static_for<0, NB>([&](auto rc) {
                         constexpr int r = decltype(rc)::value;
                         if (r < nbp) {

@@ -9,8 +9,14 @@
 
 namespace mb200 {
 
+// Resident blocks per SM the register allocation is sized for.
+template <typename T, int NT>
+constexpr int blocked_min_blocks() {
+    return NT <= 128 ? 4 : NT == 256 ? (sizeof(T) == 8 ? 2 : 3) : 1;
+}
+
 template <typename T, int NB, int NT, int CW, int CB>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, (blocked_min_blocks<T, NT>()))
 getrf_blocked_kernel(WorkList wl, LuSizes sz, T** dA_array, int** ipiv_array, int* info_array) {
     __shared__ BlockedLuShared<T, NB, NT, CW> sh;
     for (int w = blockIdx.x; w < wl.size(); w += gridDim.x) {
@@ -54,10 +60,10 @@ static void launch_getrf_blocked(const WorkList& wl, int bound, bool persistent,
 template <typename T>
 magma_int_t getrf_blocked(const WorkList& wl, int bound, bool persistent, const LuSizes& sz, int max_m, T** A,
                           int** ipiv, int* info, cudaStream_t s) {
-    if (max_m <= 128) launch_getrf_blocked<T, 32, 128, 128, 16>(wl, bound, persistent, sz, A, ipiv, info, s);
-    else if (max_m <= 256) launch_getrf_blocked<T, 32, 256, 128, 8>(wl, bound, persistent, sz, A, ipiv, info, s);
+    if (max_m <= 128) launch_getrf_blocked<T, 32, 128, 128, (sizeof(T) == 8 ? 8 : 16)>(wl, bound, persistent, sz, A, ipiv, info, s);
+    else if (max_m <= 256) launch_getrf_blocked<T, 32, 256, 128, (sizeof(T) == 8 ? 4 : 8)>(wl, bound, persistent, sz, A, ipiv, info, s);
     else if (max_m <= 512) launch_getrf_blocked<T, 32, 512, 128, 8>(wl, bound, persistent, sz, A, ipiv, info, s);
-    else launch_getrf_blocked<T, 16, 1024, 128, 4>(wl, bound, persistent, sz, A, ipiv, info, s);
+    else launch_getrf_blocked<T, 16, 1024, 128, (sizeof(T) == 8 ? 2 : 4)>(wl, bound, persistent, sz, A, ipiv, info, s);
     return launch_status();
 }
 

@@ -141,13 +141,11 @@ __device__ __forceinline__ void lu_panel_steps(T (&a)[NC], int m, int nsteps, in
         if (NW > 1) {
             if (lane == 0) { sh.red_hi[buf][warp] = key.hi; sh.red_lo[buf][warp] = key.lo; sh.red_p[buf][warp] = p; sh.red_s[buf][warp] = s; }
             __syncthreads();
-            key.hi = sh.red_hi[buf][0]; key.lo = sh.red_lo[buf][0]; p = sh.red_p[buf][0]; s = sh.red_s[buf][0];
-#pragma unroll
-            for (int w = 1; w < NW; ++w) {
-                const PivotKey k2{sh.red_hi[buf][w], sh.red_lo[buf][w]};
-                const int p2 = sh.red_p[buf][w];
-                if (key_beats(k2, p2, key, p)) { key = k2; p = p2; s = sh.red_s[buf][w]; }
-            }
+            // every warp reduces the NW warp winners lane-parallel (lane w = warp w's winner)
+            const bool v = lane < NW;
+            key = PivotKey{v ? sh.red_hi[buf][lane] : 0u, v ? sh.red_lo[buf][lane] : 0u};
+            p = v ? sh.red_p[buf][lane] : INT_MAX;
+            s = sh.red_s[buf][warp_argmax(key, p, lane)];
         }
         // ---- the pivot row publishes columns k..NC-1 (aligned pairs) ----
         constexpr int jw = k & ~1;
