@@ -22,6 +22,7 @@
 #include "internal.h"
 #include "batched_kernels.h"
 #include "getrs_blocked.cuh"
+#include "mixed_refine.cuh"
 #include "lu_sizes.h"
 #include "vbatched.h"
 #include <cfloat>
@@ -106,46 +107,15 @@ dlag2s_norm_kernel(int n, double** dA_array, int lda, MixedWs ws, int* iter_arra
     }
 }
 
-// ---- 2. refinement, one block per instance, thread = row ----
+// ---- 2. refinement, one block per instance, thread = row (mixed_refine.cuh) ----
 template <int NT, int R>
-struct RefineShared {
-    BlockedRsShared<float, NT, R> rs;
-    double x[NT][R];
-    double red[2][NT / 32][R];
-    int flag;
-};
-
-template <int NT, int R>
-__device__ __forceinline__ void block_max2(double (&v)[R], double (&w)[R], RefineShared<NT, R>& sh) {
-    // in-place block-wide max of v and w (all threads get the result)
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        for (int off = 16; off > 0; off >>= 1) {
-            v[r] = fmax(v[r], __shfl_xor_sync(kFullMask, v[r], off));
-            w[r] = fmax(w[r], __shfl_xor_sync(kFullMask, w[r], off));
-        }
-    }
-    __syncthreads();
-    if ((threadIdx.x & 31) == 0) {
-#pragma unroll
-        for (int r = 0; r < R; ++r) { sh.red[0][threadIdx.x >> 5][r] = v[r]; sh.red[1][threadIdx.x >> 5][r] = w[r]; }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        v[r] = 0.0;
-        w[r] = 0.0;
-        for (int k = 0; k < NT / 32; ++k) { v[r] = fmax(v[r], sh.red[0][k][r]); w[r] = fmax(w[r], sh.red[1][k][r]); }
-    }
-}
-
-template <int NT, int R>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 512 / NT))
 dsgesv_refine_kernel(int n, int nrhs, double** dA_array, int lda, int** ipiv_array, double** dB_array, int ldb,
                      double** dX_array, int ldx, MixedWs ws, int* iter_array) {
-    __shared__ RefineShared<NT, R> sh;
+    extern __shared__ __align__(16) unsigned char refine_smem[];
+    RefineSmem<NT, R>& sh = *reinterpret_cast<RefineSmem<NT, R>*>(refine_smem);
     const int id = blockIdx.x;
-    const int t = threadIdx.x;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
     if (iter_array[id] < 0) return;          // conversion already failed
     if (ws.sinfo[id] != 0) {                 // singular in single precision
         if (t == 0) {
@@ -159,8 +129,12 @@ dsgesv_refine_kernel(int n, int nrhs, double** dA_array, int lda, int** ipiv_arr
     double* X = dX_array[id];
     const float* SA = ws.SA + (size_t)id * n * n;
     const int* ipiv = ipiv_array[id];
-    float* Rf = ws.R + (size_t)id * n * R;
     const double cte = ws.anrm[id] * (DBL_EPSILON * 0.5) * sqrt((double)n);
+    for (int k = t; k < n; k += NT) sh.ipiv[k] = ipiv[k];
+    const int nblk = (n + 31) / 32;
+    for (int J = w; J < nblk; J += NT / 32) invert_diag_block<NT, R>(SA, n, J, lane, sh);
+    __syncthreads();
+    const int fwd = (t < n) ? laswp_target(sh.ipiv, n, t, false) : t;
     int iter_out = 0;
     for (int c0 = 0; c0 < nrhs && iter_out >= 0; c0 += R) {
         double b[R], x[R], res[R];
@@ -175,21 +149,26 @@ dsgesv_refine_kernel(int n, int nrhs, double** dA_array, int lda, int** ipiv_arr
         for (;;) {
             // C = SA^-1 res in single precision (res = B on the first pass)
             bool ovf = false;
-            if (t < n) {
+            float f[R];
 #pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    ovf |= !(fabs(res[r]) <= (double)FLT_MAX);
-                    Rf[t + (size_t)r * n] = (float)res[r];
-                }
+            for (int r = 0; r < R; ++r) {
+                ovf |= !(fabs(res[r]) <= (double)FLT_MAX);
+                f[r] = (float)res[r];
             }
             if (__syncthreads_or(ovf)) { iter_out = -2; break; }
-            blocked_getrs<float, NT, R>(false, SA, n, n, ipiv, Rf, R, n, sh.rs);
+            if (t < n) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) sh.xch[fwd][r] = f[r];
+            }
             __syncthreads();
+#pragma unroll
+            for (int r = 0; r < R; ++r) f[r] = (t < n) ? sh.xch[t][r] : 0.0f;
+            refine_solve<NT, R>(SA, n, f, sh);
             if (t < n) {
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
-                    x[r] += (double)Rf[t + (size_t)r * n];
-                    sh.x[t][r] = x[r];
+                    x[r] += (double)f[r];
+                    sh.xs[t][r] = x[r];
                 }
             }
             __syncthreads();
@@ -197,10 +176,11 @@ dsgesv_refine_kernel(int n, int nrhs, double** dA_array, int lda, int** ipiv_arr
 #pragma unroll
             for (int r = 0; r < R; ++r) res[r] = b[r];
             if (t < n) {
+#pragma unroll 16
                 for (int j = 0; j < n; ++j) {
                     const double a = A[t + (size_t)j * lda];
 #pragma unroll
-                    for (int r = 0; r < R; ++r) res[r] = fma(-a, sh.x[j][r], res[r]);
+                    for (int r = 0; r < R; ++r) res[r] = fma(-a, sh.xs[j][r], res[r]);
                 }
             }
             // max |X_j| and max |R_j| per right-hand side
@@ -210,7 +190,7 @@ dsgesv_refine_kernel(int n, int nrhs, double** dA_array, int lda, int** ipiv_arr
                 xn[r] = (t < n && c0 + r < nrhs) ? fabs(x[r]) : 0.0;
                 rn[r] = (t < n && c0 + r < nrhs) ? fabs(res[r]) : 0.0;
             }
-            block_max2<NT, R>(xn, rn, sh);
+            refine_max2<NT, R>(xn, rn, sh);
             bool ok = true;
             double ratio = 0.0;
 #pragma unroll
@@ -257,7 +237,10 @@ __global__ void copy_rhs_kernel(WorkList wl, int n, int nrhs, double** dB_array,
 template <int NT, int R>
 static void launch_refine(int n, int nrhs, double** A, int lda, int** ipiv, double** B, int ldb, double** X, int ldx,
                           const MixedWs& w, int* iter, int batch, cudaStream_t s) {
-    dsgesv_refine_kernel<NT, R><<<batch, NT, 0, s>>>(n, nrhs, A, lda, ipiv, B, ldb, X, ldx, w, iter);
+    auto k = dsgesv_refine_kernel<NT, R>;
+    const int smem = (int)sizeof(RefineSmem<NT, R>);
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    k<<<batch, NT, smem, s>>>(n, nrhs, A, lda, ipiv, B, ldb, X, ldx, w, iter);
 }
 
 bool dsgesv_supported(int n) { return n <= 512; }

@@ -58,3 +58,14 @@ def test_dsgesv_forced_fallbacks(cuda):
     assert list(oinf) == [0, 2]
     be = T.backward_error(A_np[[0, 1, 3]], X.cpu().numpy()[[0, 1, 3]], B_np[[0, 1, 3]], n)
     assert be.max() <= 1e-14
+
+
+@pytest.mark.parametrize("n,nrhs", [(37, 1), (130, 7), (255, 5)])
+def test_dsgesv_rhs_counts(cuda, n, nrhs):
+    """RHS counts that are not a multiple of the kernel's 4-column pass."""
+    import magma_b200 as mb
+    A_np, B_np, kap = T.svd_logrand(16, n, 1e2, 1e5, nrhs=nrhs, seed=7 * n + nrhs)
+    X, ipiv, it, info = mb.dsgesv_batched(dev(A_np, cuda), dev(B_np, cuda))
+    be = T.backward_error(A_np, X.cpu().numpy(), B_np, n)
+    assert be.max() <= 1e-14, (be.max(), it)
+    assert (it.cpu().numpy() >= 0).mean() > 0.5
