@@ -195,6 +195,27 @@ magma_int_t magma_dsgesv_batched(magma_int_t n, magma_int_t nrhs, double** dA_ar
                                  magma_int_t lddx, magma_int_t* iter_array, magma_int_t* dinfo_array,
                                  magma_int_t batchCount, magma_queue_t queue);
 
+/* Mixed-precision Cholesky solve on variable sizes: FP32 potrf + FP64 refinement
+ * with FP64 fallback. No batched counterpart in MAGMA 2.2; per instance it is
+ * magma_dsposv_gpu (src/zcposv_gpu.cpp:134-330) with the vbatched conventions of
+ * magma_dpotrf_vbatched (include/magma_zvbatched.h:59-70): device size arrays of
+ * batchCount+1 entries and, like the reference's variable-size Cholesky, uplo =
+ * MagmaLower only (MagmaUpper returns MAGMA_ERR_NOT_SUPPORTED). dworks_array[i]
+ * is caller-owned single-precision workspace of at least n_i*(n_i+nrhs_i)
+ * floats (the reference's dworks). iter_array / info_array as
+ * magma_dsgesv_batched (info: dpotrf info of the FP64 fallback). Checks: uplo
+ * -1, n -2, nrhs -3, ldda -5, lddb -7, lddx -9, batchCount -13. max_n <= 512. */
+magma_int_t magma_dsposv_vbatched(magma_uplo_t uplo, magma_int_t* n, magma_int_t* nrhs, double** dA_array,
+                                  magma_int_t* ldda, double** dB_array, magma_int_t* lddb, double** dX_array,
+                                  magma_int_t* lddx, float** dworks_array, magma_int_t* iter_array,
+                                  magma_int_t* info_array, magma_int_t batchCount, magma_queue_t queue);
+magma_int_t magma_dsposv_vbatched_max_nocheck(magma_uplo_t uplo, magma_int_t* n, magma_int_t* nrhs,
+                                              double** dA_array, magma_int_t* ldda, double** dB_array,
+                                              magma_int_t* lddb, double** dX_array, magma_int_t* lddx,
+                                              float** dworks_array, magma_int_t* iter_array,
+                                              magma_int_t* info_array, magma_int_t batchCount, magma_int_t max_n,
+                                              magma_int_t max_nrhs, magma_queue_t queue);
+
 /* ------------------------------------------------------------------------
  * Batched Cholesky (fixed size). Lower and Upper are both supported (the
  * reference's batched potrf handles Lower only, src/zpotf2_vbatched.cpp:32-34).

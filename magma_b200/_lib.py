@@ -95,6 +95,8 @@ SIGNATURES: dict[str, tuple] = {
                                                     _i, _p]),
     "magmablas_sgemm_vbatched_max": (None, [_i, _i, _p, _p, _p, _f, _p, _p, _p, _p, _f, _p, _p, _i, _i, _i, _i, _p]),
     "magmablas_sgemm_vbatched_nocheck": (None, [_i, _i, _p, _p, _p, _f, _p, _p, _p, _p, _f, _p, _p, _i, _p]),
+    "magma_dsposv_vbatched": (_i, [_i, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _i, _p]),
+    "magma_dsposv_vbatched_max_nocheck": (_i, [_i, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _i, _i, _i, _p]),
     # request loop (include/magma_b200_serve.h)
     "magma_b200_server_create": (_i, [_i, _sz, _i, _i, C.POINTER(_p)]),
     "magma_b200_server_submit": (_i, [_p, _i, _i, _i, _p, _i, _p, _i, _p, _i, C.c_longlong]),

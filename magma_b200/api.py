@@ -344,3 +344,38 @@ def dgesv_vbatched(A: "VarBatch", B: "VarBatch | None", n, nrhs=None, lda=None, 
                                     _vp(info), batch, q.handle)
     _check(rc, "magma_dgesv_vbatched")
     return ipiv, info[:batch]
+
+
+def dsposv_vbatched(A: "VarBatch", B: "VarBatch", n, nrhs, lda=None, ldb=None, max_sizes=None,
+                    queue: Queue | None = None):
+    """Variable-size mixed-precision Cholesky solve (magma_dsposv_vbatched, Lower).
+
+    Returns (X as a VarBatch shaped like B, iter, info); the single-precision
+    workspaces (n_i*(n_i+nrhs_i) floats each) are allocated here."""
+    import numpy as np
+
+    q = queue or default_queue()
+    batch = A.batch
+    X = VarBatch([np.zeros(s) for s in B.shapes], A.device)
+    nn = np.asarray(n, np.int64)
+    rr = np.asarray(nrhs, np.int64)
+    words = ((nn * (nn + rr) + 7) // 8) * 8
+    offs = np.concatenate([[0], np.cumsum(words)[:-1]]) if batch else np.zeros(0, np.int64)
+    S = torch.empty(max(int(words.sum()), 1), dtype=torch.float32, device=A.device)
+    Sp = S.data_ptr() + torch.from_numpy(offs * 4).to(A.device)
+    dn, dr = A.ints(n), A.ints(nrhs)
+    dla = A.ints(lda if lda is not None else [s[1] for s in A.shapes])
+    dlb = A.ints(ldb if ldb is not None else [s[1] for s in B.shapes])
+    dlx = A.ints([s[1] for s in X.shapes])
+    it = torch.empty(batch + 1, dtype=torch.int32, device=A.device)
+    info = torch.empty(batch + 1, dtype=torch.int32, device=A.device)
+    args = [MagmaLower, _vp(dn), _vp(dr), _vp(A.ptrs), _vp(dla), _vp(B.ptrs), _vp(dlb), _vp(X.ptrs), _vp(dlx),
+            _vp(Sp), _vp(it), _vp(info), batch]
+    if max_sizes:
+        rc = q.lib.magma_dsposv_vbatched_max_nocheck(*args, max_sizes[0], max_sizes[1], q.handle)
+    else:
+        rc = q.lib.magma_dsposv_vbatched(*args, q.handle)
+    _check(rc, "magma_dsposv_vbatched")
+    q.sync()
+    del S
+    return X, it[:batch], info[:batch]
