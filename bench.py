@@ -10,8 +10,14 @@ Workloads (the default is the one the metric is quoted on):
       magma_dsgesv_batched (FP32 LU + FP64 refinement + FP64 fallback) against the
       plain FP64 form magma_dgesv_batched on the same inputs.       [default]
   c1  plain FP64 LU + solve: magma_dgesv_batched on 10,000 x (32x32), 1 RHS, U[-1,1].
-  c2  gemm_vbatched: 20,000 instances, M, N, K ~ U{8..128}, FP64 (GFLOP/s).
-  c4  potrf_vbatched: 50,000 SPD instances, n power-law on [4, 512] (factorisations/s).
+  c2  gemm_vbatched: 20,000 instances, M, N, K ~ U{8..128}, alpha 1, beta 0.5, FP64 with
+      the FP32 arm beside (GFLOP/s).
+  c4  posv_vbatched: 50,000 SPD instances, n power-law on [4, 512], 1-8 RHS, FP64 and
+      FP32-factor + FP64-refinement (dsposv_vbatched), each replayed as one CUDA graph
+      (solves/s).
+  c5  the request loop: Poisson arrivals swept 1e3..1e5 req/s, 70% LU / 30% Cholesky,
+      n log-uniform on [8, 1024], 1-16 RHS, 40 GB admission budget; throughput and
+      p50/p99 latency at 1e4 req/s, the sweep beside.
 
 Timing: W untimed steps, then exactly K steps between a barrier + device
 synchronisation on both sides, measured with CUDA events on the library's
@@ -150,7 +156,6 @@ def vp(t):
 # ------------------------------------------------------------------ workloads
 class C3Mixed:
     """Mixed-precision dgesv vs plain FP64 on 2,048 x (256x256), kappa in [1e2, 1e6], 4 RHS."""
-    name = "c3_dsgesv_batched_2048x256_kappa1e2-1e6_nrhs4"
     unit = "solves/s"
     dtype = "f32-factor+f64-refine"
     data = "synthetic: A = U diag(sigma) V^T, Haar U,V (QR of seeded Gaussians), log-uniform sigma, B ~ N(0,1)"
@@ -162,6 +167,7 @@ class C3Mixed:
         from magma_b200.testing import svd_logrand_torch
 
         self.torch, self.dev, self.batch, self.n, self.nrhs = torch, dev, batch, n, nrhs
+        self.name = f"c3_dsgesv_batched_{batch}x{n}_kappa1e2-1e6_nrhs{nrhs}"
         self.A0, self.B0, self.kappa = svd_logrand_torch(batch, n, 1e2, 1e6, nrhs, seed, dev)
         self.A = self.A0.clone()
         self.B = self.B0.clone()
@@ -195,11 +201,19 @@ class C3Mixed:
     def restore(self, i):
         self.A.copy_(self.A0)
 
-    def restore_fp64(self, i):
+    alt_name = "fp64"
+
+    def config_extra(self):
+        return {"n": self.n, "nrhs": self.nrhs}
+
+    def ratios(self, value, alt_value):
+        return {"mixed_over_fp64": value / alt_value}
+
+    def restore_alt(self, i):
         self.A64.copy_(self.A0)
         self.B64.copy_(self.B0)
 
-    def step_fp64(self, q, i):
+    def step_alt(self, q, i):
         n = self.n
         return q.lib.magma_dgesv_batched(n, self.nrhs, vp(self.pA64), n, vp(self.pP), vp(self.pB64), n,
                                          vp(self.info), self.batch, q.handle)
@@ -309,6 +323,9 @@ class C1DgesvSmall:
     def units(self):
         return self.batch
 
+    def config_extra(self):
+        return {"n": self.n, "nrhs": self.nrhs}
+
     def bytes_per_unit(self):
         n, r = self.n, self.nrhs
         return 2 * 8 * n * n + 2 * 8 * n * r + 4 * n + 4
@@ -370,8 +387,339 @@ class C1DgesvSmall:
             f"in an OpenMP loop, 1 BLAS thread each"
 
 
-WORKLOADS = {"c3": C3Mixed, "c1": C1DgesvSmall}
-DEFAULT_STEPS = {"c3": (60, 5), "c1": (20000, 50)}
+
+class C2GemmVbatched:
+    """magmablas_dgemm_vbatched (and the sgemm arm) on 20,000 instances, M, N, K ~ U{8..128}."""
+    unit = "GFLOP/s"
+    dtype = "f64"
+    metric = "gemm_vbatched GFLOP/s (FP64; FP32 arm beside)"
+    data = "synthetic: M, N, K ~ U{8..128} (splitmix64), A, B, C ~ N(0,1) (torch seeded)"
+    alt_name = "fp32"
+
+    def __init__(self, dev, batch=20000, seed=2):
+        import numpy as np
+        import torch
+
+        from magma_b200 import testing as T
+
+        self.torch, self.dev, self.batch = torch, dev, batch
+        self.name = f"c2_gemm_vbatched_{batch}_MNK8-128_alpha1_beta0.5"
+        M, N, K = T.gemm_sizes(batch, 8, 128, seed=seed)
+        r8 = lambda v: ((v + 7) // 8) * 8
+        self.M, self.N, self.K = M, N, K
+        self.lda, self.ldb, self.ldc = r8(M), r8(K), r8(M)
+        self.flops = float((2.0 * M.astype(np.float64) * N * K).sum())
+        self.bytes64 = float(8 * (M.astype(np.float64) * K + K * N + 2 * M * N).sum())
+        g = torch.Generator(device=dev)
+        g.manual_seed(seed)
+        self.bufs = {}
+        for dt, tag in ((torch.float64, "d"), (torch.float32, "s")):
+            parts = {}
+            for name, rows, cols in (("A", self.lda, K), ("B", self.ldb, N), ("C", self.ldc, N)):
+                sizes = rows.astype(np.int64) * cols
+                offs = np.concatenate([[0], np.cumsum(sizes)[:-1]])
+                flat = torch.randn(int(sizes.sum()), dtype=torch.float64, device=dev, generator=g).to(dt)
+                esz = flat.element_size()
+                ptrs = flat.data_ptr() + torch.from_numpy(offs * esz).to(dev)
+                parts[name] = (flat, ptrs, offs, sizes)
+            self.bufs[tag] = parts
+        self.C0 = {t: self.bufs[t]["C"][0].clone() for t in "ds"}
+        ints = lambda v: torch.from_numpy(np.concatenate([v, [0]]).astype(np.int32)).to(dev)
+        self.dM, self.dN, self.dK = ints(M), ints(N), ints(K)
+        self.dla, self.dlb, self.dlc = ints(self.lda), ints(self.ldb), ints(self.ldc)
+        self.l2 = f"A+B+C {self.bytes64 / 2**30:.2f} GiB (FP64) > L2 (126 MB)"
+
+    def units(self):
+        return self.flops / 1e9
+
+    def config_extra(self):
+        return {"M": "U{8..128}", "N": "U{8..128}", "K": "U{8..128}", "ld": "roundup(rows, 8)",
+                "alpha": 1.0, "beta": 0.5, "gflop_per_step": self.flops / 1e9}
+
+    def launches_per_step(self):
+        return 1
+
+    def _call(self, q, tag):
+        b = self.bufs[tag]
+        fn = q.lib.magmablas_dgemm_vbatched_max_nocheck if tag == "d" else q.lib.magmablas_sgemm_vbatched_max_nocheck
+        fn(111, 111, vp(self.dM), vp(self.dN), vp(self.dK), 1.0, vp(b["A"][1]), vp(self.dla), vp(b["B"][1]),
+           vp(self.dlb), 0.5, vp(b["C"][1]), vp(self.dlc), self.batch, 128, 128, 128, q.handle)
+        return 0
+
+    def restore(self, i):
+        self.bufs["d"]["C"][0].copy_(self.C0["d"])
+
+    def step(self, q, i):
+        return self._call(q, "d")
+
+    def restore_alt(self, i):
+        self.bufs["s"]["C"][0].copy_(self.C0["s"])
+
+    def step_alt(self, q, i):
+        return self._call(q, "s")
+
+    def ratios(self, value, alt_value):
+        return {"fp32_over_fp64": alt_value / value}
+
+    def _check(self, q, tag, sample):
+        t = self.torch
+        b = self.bufs[tag]
+        b["C"][0].copy_(self.C0[tag])
+        self._call(q, tag)
+        q.sync()
+        worst = 0.0
+        for i in sample:
+            m, n, k = int(self.M[i]), int(self.N[i]), int(self.K[i])
+            sl = lambda nm, rows, cols: b[nm][0][int(b[nm][2][i]):int(b[nm][2][i]) + rows * cols].view(cols, rows)
+            A = sl("A", int(self.lda[i]), k)[:, :m].T.double()
+            Bm = sl("B", int(self.ldb[i]), n)[:, :k].T.double()
+            C0 = self.C0[tag][int(b["C"][2][i]):int(b["C"][2][i]) + int(self.ldc[i]) * n].view(n, -1)[:, :m].T.double()
+            C = sl("C", int(self.ldc[i]), n)[:, :m].T.double()
+            ref = A @ Bm + 0.5 * C0
+            # normalised max error |C - C_ref| / (k |A|max |B|max + beta |C0|max)
+            err = (C - ref).abs().max() / ((A.abs().max() * Bm.abs().max() * k + 0.5 * C0.abs().max()) + 1e-300)
+            worst = max(worst, float(err))
+        b["C"][0].copy_(self.C0[tag])
+        return worst
+
+    def validate(self, q):
+        sample = list(range(0, self.batch, max(1, self.batch // 200)))
+        return {"gemm_err_max_fp64": self._check(q, "d", sample), "gemm_err_max_fp32": self._check(q, "s", sample)}
+
+    def dominant_kernel(self, q, stream, reps=20):
+        ms = timed_restore(stream, lambda i: self.step(q, i), self.restore, reps) / reps
+        return {"kernel": "gemm_vbatched_kernel<double> (magmablas_dgemm_vbatched_max_nocheck)", "ms": ms,
+                "alg_bytes": self.bytes64, "tflops": self.flops / ms / 1e9}
+
+    def e2e_setup(self):
+        t = self.torch
+        b = self.bufs["d"]
+        self.h = {k: b[k][0].cpu().pin_memory() for k in "ABC"}
+        self.hC0 = self.C0["d"].cpu().pin_memory()
+        self.h2d = sum(self.h[k].numel() * 8 for k in "ABC")
+        self.d2h = self.h["C"].numel() * 8
+
+    def e2e_step(self, q, i):
+        b = self.bufs["d"]
+        b["A"][0].copy_(self.h["A"], non_blocking=True)
+        b["B"][0].copy_(self.h["B"], non_blocking=True)
+        b["C"][0].copy_(self.hC0, non_blocking=True)
+        self.step(q, i)
+        self.h["C"].copy_(b["C"][0], non_blocking=True)
+
+    def cpu_reference(self, seconds=10.0, nthreads=None, sample=2000):
+        import numpy as np
+
+        import oracle
+
+        b = self.bufs["d"]
+        flat = {k: b[k][0][: int(b[k][2][sample - 1] + b[k][3][sample - 1])].cpu().numpy() for k in "ABC"}
+        cols = {"A": self.K, "B": self.N, "C": self.N}
+        rows = {"A": self.lda, "B": self.ldb, "C": self.ldc}
+        mats = {k: [flat[k][int(b[k][2][i]):int(b[k][2][i] + b[k][3][i])].reshape(int(cols[k][i]), int(rows[k][i]))
+                    for i in range(sample)] for k in "ABC"}
+        fl = float((2.0 * self.M[:sample].astype(np.float64) * self.N[:sample] * self.K[:sample]).sum())
+        done, t_total = 0.0, 0.0
+        while t_total < seconds:
+            t0 = time.perf_counter()
+            oracle.lapack_gemm_vbatched(0, 0, self.M[:sample], self.N[:sample], self.K[:sample], 1.0, mats["A"],
+                                        self.lda[:sample], mats["B"], self.ldb[:sample], 0.5, mats["C"],
+                                        self.ldc[:sample], nthreads=nthreads)
+            t_total += time.perf_counter() - t0
+            done += fl
+        return done / 1e9 / t_total, done, (nthreads or oracle.max_threads()), \
+            f"{sample}-instance slices of the same inputs, re-run; dgemm (OpenBLAS 0.3.30, scipy) in an OpenMP " \
+            f"loop, 1 BLAS thread each"
+
+
+class C4CholVbatched:
+    """Variable-size Cholesky solve on 50,000 SPD instances, n power-law on [4, 512] (exponent -1.5),
+    1-8 RHS: magma_dposv_vbatched_max_nocheck (FP64) replayed as one captured CUDA graph, beside
+    magma_dsposv_vbatched_max_nocheck (FP32 factor + FP64 refinement), also graph-replayed."""
+    unit = "solves/s"
+    dtype = "f64"
+    metric = "vbatched Cholesky solves/s at bwd err <=1e-14 (FP64; FP32-factor + FP64-refinement beside)"
+    data = "synthetic: n ~ power law on [4,512] (inverse CDF, seeded), A = G G^T + n I with G ~ N(0,1), B ~ N(0,1)"
+    alt_name = "mixed"
+
+    def __init__(self, dev, batch=50000, seed=4):
+        import numpy as np
+        import torch
+
+        self.torch, self.dev, self.batch = torch, dev, batch
+        self.name = f"c4_posv_vbatched_{batch}_n4-512_powerlaw1.5_nrhs1-8"
+        rng = np.random.default_rng(seed)
+        a, b = 4.0 ** -0.5, 512.0 ** -0.5
+        u = rng.random(batch)
+        n = np.rint((a - u * (a - b)) ** -2.0).astype(np.int64).clip(4, 512)
+        nrhs = rng.integers(1, 9, batch)
+        self.n, self.nrhs = n, nrhs
+        pad = lambda v: ((v + 3) // 4) * 4
+        order = np.argsort(n, kind="stable")            # lay instances out grouped by size
+        szA, szB = pad(n * n), pad(n * nrhs)
+        offA = np.zeros(batch, np.int64)
+        offB = np.zeros(batch, np.int64)
+        offA[order] = np.concatenate([[0], np.cumsum(szA[order])[:-1]])
+        offB[order] = np.concatenate([[0], np.cumsum(szB[order])[:-1]])
+        self.offA, self.offB = offA, offB
+        self.A0 = torch.zeros(int(szA.sum()), dtype=torch.float64, device=dev)
+        g = torch.Generator(device=dev)
+        g.manual_seed(seed)
+        for nv in np.unique(n):
+            ids = np.nonzero(n == nv)[0]
+            nv = int(nv)
+            G = torch.randn(len(ids), nv, nv, dtype=torch.float64, device=dev, generator=g)
+            S = G @ G.transpose(1, 2) + nv * torch.eye(nv, dtype=torch.float64, device=dev)
+            idx = torch.from_numpy(offA[ids]).to(dev)[:, None] + torch.arange(nv * nv, device=dev)[None, :]
+            self.A0[idx.reshape(-1)] = S.reshape(-1)
+            del G, S, idx
+        self.B0 = torch.randn(int(szB.sum()), dtype=torch.float64, device=dev, generator=g)
+        self.A = self.A0.clone()
+        self.B = self.B0.clone()
+        self.X = torch.zeros_like(self.B0)
+        self.Am = self.A0.clone()
+        self.W = torch.empty(int(pad(n * (n + nrhs)).sum()), dtype=torch.float32, device=dev)
+        offW = np.concatenate([[0], np.cumsum(pad(n * (n + nrhs)))[:-1]])
+        P = lambda buf, off, esz: buf.data_ptr() + torch.from_numpy(off * esz).to(dev)
+        self.pA, self.pB, self.pX = P(self.A, offA, 8), P(self.B, offB, 8), P(self.X, offB, 8)
+        self.pAm, self.pW = P(self.Am, offA, 8), P(self.W, offW, 4)
+        self.pB0 = P(self.B0, offB, 8)   # the mixed arm reads B0 (dsposv leaves B untouched)
+        ints = lambda v: torch.from_numpy(np.concatenate([v, [0]]).astype(np.int32)).to(dev)
+        self.dn, self.dr = ints(n), ints(nrhs)
+        self.info = torch.zeros(batch + 1, dtype=torch.int32, device=dev)
+        self.it = torch.zeros(batch + 1, dtype=torch.int32, device=dev)
+        self.flops = float((n ** 3 / 3.0 + n ** 2 / 2.0 + n / 6.0 + 2.0 * n * n * nrhs).sum())
+        self.l2 = f"A {self.A0.numel() * 8 / 2**30:.2f} GiB > L2 (126 MB)"
+        self.graphs = {}
+
+    def units(self):
+        return self.batch
+
+    def config_extra(self):
+        return {"n": "power law on [4,512], exponent -1.5", "nrhs": "U{1..8}", "uplo": "lower",
+                "graph": "one captured CUDA graph per step", "gflop_per_step": self.flops / 1e9}
+
+    def launches_per_step(self):
+        return 1 + 8 * 2   # bucketize + per-bucket factor/solve kernels (graph-replayed)
+
+    def _raw_fp64(self, q):
+        return q.lib.magma_dposv_vbatched_max_nocheck(122, vp(self.dn), vp(self.dr), vp(self.pA), vp(self.dn),
+                                                      vp(self.pB), vp(self.dn), vp(self.info), self.batch, 512, 8,
+                                                      q.handle)
+
+    def _raw_mixed(self, q):
+        return q.lib.magma_dsposv_vbatched_max_nocheck(122, vp(self.dn), vp(self.dr), vp(self.pAm), vp(self.dn),
+                                                       vp(self.pB0), vp(self.dn), vp(self.pX), vp(self.dn),
+                                                       vp(self.pW), vp(self.it), vp(self.info), self.batch, 512, 8,
+                                                       q.handle)
+
+    def _graph(self, q, key, fn):
+        """Capture fn once into a CUDA graph on the queue's stream (after an eager call has
+        grown the queue workspace to its final size), then replay it."""
+        t = self.torch
+        if key not in self.graphs:
+            assert fn(q) == 0
+            t.cuda.synchronize()
+            g = t.cuda.CUDAGraph()
+            with t.cuda.graph(g, stream=t.cuda.current_stream()):
+                rc = fn(q)
+            assert rc == 0, rc
+            self.graphs[key] = g
+        self.graphs[key].replay()
+        return 0
+
+    def restore(self, i):
+        self.A.copy_(self.A0)
+        self.B.copy_(self.B0)
+
+    def step(self, q, i):
+        return self._graph(q, "fp64", self._raw_fp64)
+
+    def restore_alt(self, i):
+        self.Am.copy_(self.A0)
+
+    def step_alt(self, q, i):
+        return self._graph(q, "mixed", self._raw_mixed)
+
+    def ratios(self, value, alt_value):
+        return {"mixed_over_fp64": alt_value / value}
+
+    def _bwd(self, X, sample):
+        import numpy as np
+
+        A0, B0 = self.A0.cpu().numpy(), self.B0.cpu().numpy()
+        Xh = X.cpu().numpy()
+        worst = 0.0
+        for i in sample:
+            n, r = int(self.n[i]), int(self.nrhs[i])
+            A = A0[self.offA[i]:self.offA[i] + n * n].reshape(n, n)
+            B = B0[self.offB[i]:self.offB[i] + n * r].reshape(r, n).T
+            x = Xh[self.offB[i]:self.offB[i] + n * r].reshape(r, n).T
+            R = B - A @ x
+            den = np.abs(A).sum(axis=1).max() * np.abs(x).max(axis=0) + np.abs(B).max(axis=0)
+            worst = max(worst, float((np.abs(R).max(axis=0) / den).max()))
+        return worst
+
+    def validate(self, q):
+        import numpy as np
+
+        t = self.torch
+        sample = sorted(set(np.argsort(self.n)[-50:].tolist() + list(range(0, self.batch, self.batch // 250))))
+        self.restore(0)
+        assert self._raw_fp64(q) == 0
+        q.sync()
+        be64 = self._bwd(self.B, sample)
+        nz64 = int((self.info[:self.batch] != 0).sum())
+        self.restore_alt(0)
+        assert self._raw_mixed(q) == 0
+        q.sync()
+        bem = self._bwd(self.X, sample)
+        it = self.it[:self.batch].cpu()
+        hist = {int(k): int(v) for k, v in zip(*t.unique(it, return_counts=True))}
+        self.restore(0)
+        return {"bwd_err_max_fp64": be64, "bwd_err_max_mixed": bem, "iter_hist_mixed": hist, "info_nonzero": nz64,
+                "bwd_err_sample": len(sample)}
+
+    def dominant_kernel(self, q, stream, reps=5):
+        ms = timed_restore(stream, lambda i: self.step(q, i), self.restore, reps) / reps
+        alg = float((16.0 * self.n ** 2 + 16.0 * self.n * self.nrhs + 4).sum())
+        return {"kernel": "posv_vbatched (graph: potrf/potrs bucket kernels)", "ms": ms, "alg_bytes": alg,
+                "tflops": self.flops / ms / 1e9}
+
+    def e2e_setup(self):
+        self.hA = self.A0.cpu().pin_memory()
+        self.hB = self.B0.cpu().pin_memory()
+        self.hX = self.torch.empty_like(self.hB).pin_memory()
+        self.hI = self.torch.empty(self.batch + 1, dtype=self.torch.int32).pin_memory()
+        self.h2d = (self.hA.numel() + self.hB.numel()) * 8
+        self.d2h = self.hX.numel() * 8 + self.hI.numel() * 4
+
+    def e2e_step(self, q, i):
+        self.A.copy_(self.hA, non_blocking=True)
+        self.B.copy_(self.hB, non_blocking=True)
+        self.step(q, i)
+        self.hX.copy_(self.B, non_blocking=True)
+        self.hI.copy_(self.info, non_blocking=True)
+
+    def cpu_reference(self, seconds=10.0, nthreads=None, sample=5000):
+        import oracle
+
+        A0, B0 = self.A0.cpu().numpy(), self.B0.cpu().numpy()
+        n, r = self.n[:sample], self.nrhs[:sample]
+        done, t_total = 0, 0.0
+        while t_total < seconds:
+            As = [A0[self.offA[i]:self.offA[i] + n[i] * n[i]].reshape(n[i], n[i]).copy() for i in range(sample)]
+            Bs = [B0[self.offB[i]:self.offB[i] + n[i] * r[i]].reshape(r[i], n[i]).copy() for i in range(sample)]
+            t0 = time.perf_counter()
+            oracle.lapack_dposv_vbatched(As, Bs, n, r, n, n, nthreads=nthreads)
+            t_total += time.perf_counter() - t0
+            done += sample
+        return done / t_total, done, (nthreads or oracle.max_threads()), \
+            f"{done} solves (first {sample} instances, re-run); LAPACK dpotrf + dpotrs (OpenBLAS 0.3.30, scipy) " \
+            f"in an OpenMP loop, 1 BLAS thread each"
+
+WORKLOADS = {"c3": C3Mixed, "c1": C1DgesvSmall, "c2": C2GemmVbatched, "c4": C4CholVbatched}
+DEFAULT_STEPS = {"c3": (60, 5), "c1": (20000, 50), "c2": (50, 5), "c4": (20, 3), "c5": (3000, 200)}
 
 
 # ---------------------------------------------------------------------- main
@@ -403,6 +751,10 @@ def run_reference(args, rank):
     from magma_b200 import testing as T
 
     nthreads = oracle.max_threads()
+    if args.workload not in ("c1", "c3"):
+        print(json.dumps({"impl": "reference", "unavailable": "the reference arm covers the c1 and c3 workloads; "
+                          "c2/c4 report their CPU LAPACK loop as cpu_baseline"}), flush=True)
+        return
     # each step gets fresh copies of the inputs, made outside the timed call
     if args.workload == "c3":
         sample = 256
@@ -410,7 +762,7 @@ def run_reference(args, rank):
         prep = lambda: (A0.copy(), B0)   # noqa: E731
         fn = lambda a, b: oracle.lapack_dsgesv_batched(a, b, nthreads=nthreads)   # noqa: E731
         desc = f"{sample} instances per step (256x256, kappa in [1e2,1e6], 4 RHS); LAPACK dsgesv"
-        cfg = {"workload": C3Mixed.name, "batch": sample, "n": 256, "nrhs": 4}
+        cfg = {"workload": "c3_dsgesv_batched_2048x256_kappa1e2-1e6_nrhs4", "batch": sample, "n": 256, "nrhs": 4}
         dtype = C3Mixed.dtype
     else:
         sample = 10000
@@ -443,13 +795,67 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+
+def run_serving(args, rank, world):
+    """C5: the request loop under Poisson arrivals (70% LU / 30% Cholesky, n log-uniform on
+    [8, 1024], 1-16 RHS, 40 GB admission budget). A step is one request; each offered rate
+    replays the same `steps` requests. Latency runs from a request's scheduled arrival to its
+    result in host memory, on the host's monotonic clock."""
+    import torch
+
+    from magma_b200 import serve
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    reqs = serve.make_requests(args.steps, seed=5 + rank)
+    warm = serve.make_requests(max(args.warmup, 3), seed=99 + rank)
+    rates = [1e3, 3e3, 1e4, 3e4, 1e5]
+    stated = 1e4
+    sweep = []
+    clocks = ClockSampler("GPU-" + str(torch.cuda.get_device_properties(dev).uuid))
+    with serve.Server(40 << 30, streams=4, max_batch=256) as sv:
+        serve.run_load(sv, warm, rate=1e4, seed=1)
+        clocks.start()
+        for r in rates:
+            res = serve.run_load(sv, reqs, rate=r, seed=int(r))
+            sweep.append({k: res[k] for k in ("offered_rate", "throughput", "p50_ms", "p99_ms", "max_ms",
+                                              "infos_nonzero", "max_submit_lag_ms")})
+        clk = clocks.stop()
+        stats = sv.stats()
+    be = max(serve.backward_error(r) for r in reqs)
+    at = next(x for x in sweep if x["offered_rate"] == stated)
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([at["throughput"]], dtype=torch.float64, device=dev)
+        dist.all_reduce(t)
+        total = float(t.item())
+    else:
+        total = at["throughput"]
+    if rank == 0:
+        line = {
+            "metric": "serving: requests/s with p50/p99 latency (arrival -> result on host)",
+            "value": total, "unit": "requests/s", "n_gpus": world, "steps": args.steps, "warmup": len(warm),
+            "ms_per_step": 1e3 / at["throughput"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": serve.__doc__.split("\n")[3].strip() + " (seeded)",
+            "config": {"workload": f"c5_serving_{args.steps}req_lu70_chol30_n8-1024_nrhs1-16",
+                       "offered_rate": stated, "hbm_budget_bytes": 40 << 30, "streams": 4, "max_batch": 256,
+                       "parallelism": f"replicas x{world}", "l2": "per-request copies from pinned host memory"},
+            "p50_ms": at["p50_ms"], "p99_ms": at["p99_ms"], "sweep": sweep, "bwd_err_max": be,
+            "peak_device_bytes": stats["peak_bytes"], "micro_batches": stats["batches"],
+            "e2e": {"value": total, "unit": "requests/s", "note": "every request is host-to-host",
+                    "h2d_bytes_per_step": sum(8 * (r.A.size + r.B.size) for r in reqs) / len(reqs),
+                    "d2h_bytes_per_step": sum(8 * r.X.size for r in reqs) / len(reqs)},
+            "gpu_launches": None, "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=None)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c3")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["c5"], default="c3")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch", type=int, default=None,
                     help="instances per GPU (default: the workload's own size; smaller only for profiling)")
@@ -463,6 +869,11 @@ def main():
     rank, world, local, dist = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.workload == "c5":
+        run_serving(args, rank, world)
+        if dist:
+            dist.destroy_process_group()
         return
 
     import torch
@@ -479,6 +890,8 @@ def main():
         q = Queue(stream, local)
         checks = W.validate(q)
         for i in range(args.warmup):
+            if hasattr(W, "restore"):
+                W.restore(i)
             W.step(q, i)
         torch.cuda.synchronize(dev)
         if dist:
@@ -499,12 +912,13 @@ def main():
         clk = clocks.stop()
         assert all(rc == 0 for rc in rcs), f"library returned {set(rcs)}"
         extra = {}
-        if hasattr(W, "step_fp64"):
+        if hasattr(W, "step_alt"):
             for i in range(3):
-                W.step_fp64(q, i)
+                W.restore_alt(i)
+                W.step_alt(q, i)
             torch.cuda.synchronize(dev)
-            ms_fp64 = timed_restore(stream, lambda i: W.step_fp64(q, i), W.restore_fp64, args.steps)
-            extra["fp64_ms_per_step"] = ms_fp64 / args.steps
+            ms_alt = timed_restore(stream, lambda i: W.step_alt(q, i), W.restore_alt, args.steps)
+            extra["alt_ms_per_step"] = ms_alt / args.steps
         dom = W.dominant_kernel(q, stream)
         # end to end (host buffers, copies inside each step)
         W.e2e_setup()
@@ -515,29 +929,30 @@ def main():
         if dist:
             dist.barrier()
         ms_e2e = timed(stream, lambda i: W.e2e_step(q, i), ke)
-    vals = [ms_total, ms_e2e, extra.get("fp64_ms_per_step", 0.0) * args.steps]
+    vals = [ms_total, ms_e2e, extra.get("alt_ms_per_step", 0.0) * args.steps]
     if dist:
         t = torch.tensor(vals, device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         vals = [float(v) for v in t.tolist()]
-    ms_total, ms_e2e, ms_fp64_total = vals
+    ms_total, ms_e2e, ms_alt_total = vals
     units = W.units() * world
     value = units * args.steps / (ms_total * 1e-3)
     if rank == 0:
         peaks = measured_peaks()
         achieved = dom["alg_bytes"] / (dom["ms"] * 1e-3) / 1e9
         line = {
-            "metric": METRIC, "value": value, "unit": W.unit, "n_gpus": world, "steps": args.steps,
+            "metric": getattr(W, "metric", METRIC), "value": value, "unit": W.unit, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": W.dtype, "data": W.data,
-            "config": {"workload": W.name, "batch_per_gpu": W.batch, "n": W.n, "nrhs": W.nrhs,
+            "config": {"workload": W.name, "batch_per_gpu": W.batch, **W.config_extra(),
                        "parallelism": f"replicas x{world}", "l2": W.l2},
         }
         line.update(checks)
-        if ms_fp64_total:
-            fp64_value = units * args.steps / (ms_fp64_total * 1e-3)
-            line["fp64_value"] = fp64_value
-            line["mixed_over_fp64"] = value / fp64_value
+        if ms_alt_total:
+            alt_value = units * args.steps / (ms_alt_total * 1e-3)
+            line[f"{W.alt_name}_value"] = alt_value
+            line[f"{W.alt_name}_ms_per_step"] = ms_alt_total / args.steps
+            line.update(W.ratios(value, alt_value))
         line["roofline"] = {
             "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
             "frac": achieved / peaks["hbm_gbs"], "traffic": profile_traffic(dom["kernel"].split("<")[0], W.name),

@@ -111,15 +111,23 @@ __device__ __forceinline__ T& tri(T* A, int lda, bool upper, int i, int j) {
 
 // ---------------------------------------------------------------------------
 // Blocked right-looking Cholesky of one matrix per thread block (n <= NT).
+// Per panel of NB columns: thread t factors row t's panel entries in registers
+// (chol_panel_steps), every row publishes them to shared memory, and the
+// trailing lower triangle A22 -= P P^T is computed by all threads in 4x8 tiles
+// distributed evenly over the triangle (a row-per-thread update would leave
+// the last rows with most of the work). Each element still receives
+// fma(-L(i,r), L(j,r), a) for r ascending, the unblocked order.
 template <typename T, int NB, int NT, int CW>
 struct BlockedCholShared {
     CholShared<T, NB> p;
-    T L[CW][NB + 1];     // panel rows j0..j0+CW-1 for the trailing update
+    T P[NT][NB + 1];     // panel entries of every row
 };
 
 template <typename T, int NB, int NT, int CW, int CB>
 __device__ int blocked_potrf(T* __restrict__ A, int n, int lda, bool upper, BlockedCholShared<T, NB, NT, CW>& sh) {
     constexpr int NW = NT / 32;
+    // tile rows x columns; 2 rows when the block size leaves 64 registers a thread (FP64)
+    constexpr int TR = (NT >= 1024 && sizeof(T) == 8) ? 2 : 4, TC = 8, G = 8 / TR;
     const int tid = threadIdx.x;
     for (int k0 = 0; k0 < n; k0 += NB) {
         const int nbp = min(NB, n - k0);
@@ -133,38 +141,51 @@ __device__ int blocked_potrf(T* __restrict__ A, int n, int lda, bool upper, Bloc
 #pragma unroll
             for (int c = 0; c < NB; ++c)
                 if (c < nbp && k0 + c <= tid) tri(A, lda, upper, tid, k0 + c) = a[c];
+#pragma unroll
+            for (int c = 0; c < NB; ++c) sh.P[tid][c] = a[c];
         }
         if (info) return info;
-        // trailing update of the lower triangle: A(i, j) -= sum_r L(i, r) L(j, r), j <= i
-        for (int j0 = k0 + nbp; j0 < n; j0 += CW) {
-            const int cw = min(CW, n - j0);
-            __syncthreads();   // previous readers of sh.L done
-            if (tid >= j0 && tid < j0 + cw) {
-#pragma unroll
-                for (int r = 0; r < NB; ++r) sh.L[tid - j0][r] = a[r];
-            }
-            __syncthreads();
-            if (tid >= j0 && tid < n) {
-                const int cmax = min(cw, tid - j0 + 1);   // columns j0 .. min(j0+cw-1, tid)
-                for (int c0 = 0; c0 < cmax; c0 += CB) {
-                    T acc[CB];
-#pragma unroll
-                    for (int c = 0; c < CB; ++c) acc[c] = (c0 + c < cmax) ? tri(A, lda, upper, tid, j0 + c0 + c) : T(0);
-                    static_for<0, NB>([&](auto rc) {
-                        constexpr int r = decltype(rc)::value;
-                        if (r < nbp) {
-                            const T l = a[r];
-#pragma unroll
-                            for (int c = 0; c < CB; ++c) acc[c] = fma_rn(-l, sh.L[c0 + c][r], acc[c]);
-                        }
-                    });
-#pragma unroll
-                    for (int c = 0; c < CB; ++c)
-                        if (c0 + c < cmax) tri(A, lda, upper, tid, j0 + c0 + c) = acc[c];
-                }
-            }
-        }
         __syncthreads();
+        // trailing lower triangle: rows/columns m0..n-1, square 8x8 blocks (bj <= bi),
+        // each split into G work items of TR rows
+        const int m0 = k0 + nbp;
+        const int T8 = (n - m0 + 7) / 8;
+        const int items = G * T8 * (T8 + 1) / 2;
+        for (int w = tid; w < items; w += NT) {
+            const int blk = w / G, h = w % G;
+            int bi = (int)((sqrtf(8.0f * blk + 1.0f) - 1.0f) * 0.5f);
+            while ((bi + 1) * (bi + 2) / 2 <= blk) ++bi;
+            while (bi * (bi + 1) / 2 > blk) --bi;
+            const int bj = blk - bi * (bi + 1) / 2;
+            const int i0 = m0 + 8 * bi + TR * h, j0 = m0 + 8 * bj;
+            T acc[TR][TC];
+#pragma unroll
+            for (int ii = 0; ii < TR; ++ii)
+#pragma unroll
+                for (int jj = 0; jj < TC; ++jj) {
+                    const int i = i0 + ii, j = j0 + jj;
+                    acc[ii][jj] = (i < n && j <= i) ? tri(A, lda, upper, i, j) : T(0);
+                }
+            for (int r = 0; r < nbp; ++r) {
+                T li[TR], lj[TC];
+#pragma unroll
+                for (int ii = 0; ii < TR; ++ii) li[ii] = sh.P[min(i0 + ii, NT - 1)][r];
+#pragma unroll
+                for (int jj = 0; jj < TC; ++jj) lj[jj] = sh.P[min(j0 + jj, NT - 1)][r];
+#pragma unroll
+                for (int ii = 0; ii < TR; ++ii)
+#pragma unroll
+                    for (int jj = 0; jj < TC; ++jj) acc[ii][jj] = fma_rn(-li[ii], lj[jj], acc[ii][jj]);
+            }
+#pragma unroll
+            for (int ii = 0; ii < TR; ++ii)
+#pragma unroll
+                for (int jj = 0; jj < TC; ++jj) {
+                    const int i = i0 + ii, j = j0 + jj;
+                    if (i < n && j <= i) tri(A, lda, upper, i, j) = acc[ii][jj];
+                }
+        }
+        __syncthreads();   // trailing entries visible before the next panel loads them
     }
     return 0;
 }

@@ -23,7 +23,7 @@ magma_int_t chol_fixed(bool upper, int n, int nrhs, T** A, int lda, T** B, int l
 }
 
 // Variable size: instances are counting-sorted into size buckets on the
-// device; each bucket's kernel walks its own list (largest bucket first).
+// device; each bucket's kernel walks its own list, the buckets concurrently.
 template <typename T>
 magma_int_t chol_var(bool upper, const int* n, const int* nrhs, T** A, const int* lda, T** B, const int* ldb,
                      int* info, int batch, int max_n, int max_nrhs, bool factor, bool solve, magma_queue_t queue) {
@@ -36,10 +36,14 @@ magma_int_t chol_var(bool upper, const int* n, const int* nrhs, T** A, const int
     magma_int_t rc = bucketize(n, batch, kCholEdges, kCholBuckets, queue->stream, ws, &counts, &lists);
     if (rc) return rc;
     LuSizes sz{0, 0, 0, 0, 0, n, n, lda, ldb, nrhs};
+    // buckets are independent: each runs on its own auxiliary stream
+    if ((rc = queue_fork(queue))) return rc;
     for (int b = top; b >= 0; --b) {
         WorkList wl{lists + (size_t)b * batch, counts + b, 0};
-        chol_bucket<T>(b, wl, batch, true, sz, upper, A, B, info, factor, solve, max_nrhs, queue->stream);
+        chol_bucket<T>(b, wl, batch, true, sz, upper, A, B, info, factor, solve, max_nrhs,
+                       queue_aux(queue, top - b));
     }
+    queue_join(queue);
     return launch_status();
 }
 

@@ -91,9 +91,10 @@ potrs_small_kernel(WorkList wl, LuSizes sz, bool upper, T** dA_array, T** dB_arr
 
 // ---- blocked potrf / potrs, one matrix per block ----
 template <typename T, int NB, int NT, int CW, int CB>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, (NT <= 128 ? 4 : NT == 256 ? 2 : 1))
 potrf_blocked_kernel(WorkList wl, LuSizes sz, bool upper, T** dA_array, int* info_array) {
-    __shared__ BlockedCholShared<T, NB, NT, CW> sh;
+    extern __shared__ __align__(16) unsigned char potrf_smem[];
+    BlockedCholShared<T, NB, NT, CW>& sh = *reinterpret_cast<BlockedCholShared<T, NB, NT, CW>*>(potrf_smem);
     for (int w = blockIdx.x; w < wl.size(); w += gridDim.x) {
         const int id = wl.at(w);
         const int n = sz.get_n(id), lda = sz.get_lda(id);
@@ -119,9 +120,9 @@ potrs_blocked_kernel(WorkList wl, LuSizes sz, bool upper, T** dA_array, T** dB_a
 // ---------------------------------------------------------------------------
 // Launchers. Each bucket launcher covers instances with n in (lo, hi].
 template <typename K>
-static int grid_for(K kernel, int threads, int items_upper_bound, bool bounded) {
+static int grid_for(K kernel, int threads, int items_upper_bound, bool bounded, size_t smem = 0) {
     if (!bounded) return max(1, items_upper_bound);
-    const int res = resident_blocks((const void*)kernel, threads, 0);
+    const int res = resident_blocks((const void*)kernel, threads, smem);
     return max(1, min(items_upper_bound, res));
 }
 
@@ -162,7 +163,9 @@ template <typename T, int NB, int NT, int CW, int CB>
 static void launch_potrf_blocked(const WorkList& wl, int bound, bool persistent, const LuSizes& sz, bool upper,
                                  T** A, int* info, cudaStream_t s) {
     auto k = potrf_blocked_kernel<T, NB, NT, CW, CB>;
-    k<<<grid_for(k, NT, bound, persistent), NT, 0, s>>>(wl, sz, upper, A, info);
+    const int smem = (int)sizeof(BlockedCholShared<T, NB, NT, CW>);
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    k<<<grid_for(k, NT, bound, persistent, smem), NT, smem, s>>>(wl, sz, upper, A, info);
 }
 
 template <typename T, int NT>

@@ -22,6 +22,11 @@ struct magma_queue {
     size_t       ws_bytes;
     // host-pinned staging word used by routines that must read one value back
     int*         h_flag;
+    // auxiliary streams for independent work (size buckets), created on first use
+    cudaStream_t aux[4];
+    cudaEvent_t  ev_fork;
+    cudaEvent_t  ev_join[4];
+    bool         aux_ready;
 };
 
 namespace mb200 {
@@ -31,6 +36,18 @@ namespace mb200 {
 // in use by enqueued work) -- callers that capture CUDA graphs reserve the
 // workspace once before capture with magma_queue_reserve_workspace().
 void* queue_workspace(magma_queue_t queue, size_t bytes);
+
+// Fork/join of the queue's auxiliary streams: queue_fork makes every auxiliary
+// stream wait for the work enqueued so far on the queue's stream, queue_aux(i)
+// names one, and queue_join makes the queue's stream wait for all of them. Work
+// that is independent (one size bucket per auxiliary stream) then runs
+// concurrently, inside CUDA-graph capture too (the fork and join are event
+// edges). The streams are created on the first fork, which therefore has to
+// happen outside capture (the eager call that also sizes the workspace).
+constexpr int kAuxStreams = 4;
+magma_int_t queue_fork(magma_queue_t queue);
+inline cudaStream_t queue_aux(magma_queue_t queue, int i) { return queue->aux[i % kAuxStreams]; }
+void queue_join(magma_queue_t queue);
 
 // Records a CUDA launch error as a MAGMA error code (0 when none).
 inline magma_int_t launch_status() {

@@ -38,8 +38,10 @@ static magma_int_t lu_var(LuOp op, bool trans, const int* m, const int* n, const
                                 &counts, &lists);
     if (rc) return rc;
     const LuSizes sz{0, 0, 0, 0, 0, m, n, lda, ldb, nrhs};
-    cudaStream_t s = queue->stream;
+    // buckets are independent: each runs on its own auxiliary stream
+    if ((rc = queue_fork(queue))) return rc;
     for (int b = top; b >= 0; --b) {
+        cudaStream_t s = queue_aux(queue, top - b);
         const WorkList wl{lists + (size_t)b * batch, counts + b, 0};
         const int e = kLuEdges[b];
         if (e <= 64) {
@@ -51,9 +53,10 @@ static magma_int_t lu_var(LuOp op, bool trans, const int* m, const int* n, const
             if (!rc && op != LuOp::Getrf)
                 rc = getrs_blocked<T>(wl, batch, true, trans, sz, e, max_nrhs, A, ipiv, B, s);
         }
-        if (rc) return rc;
+        if (rc) break;
     }
-    return launch_status();
+    queue_join(queue);
+    return rc ? rc : launch_status();
 }
 
 // Device-side checks of two size arrays: some a < 0 -> code_a, some b < 0 -> code_b.

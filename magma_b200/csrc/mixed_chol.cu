@@ -387,22 +387,29 @@ magma_int_t dsposv_var(const int* n, const int* nrhs, double** A, const int* lda
     magma_int_t rc = bucketize(n, batch, kCholEdges, kCholBuckets, s, bws_n, &counts, &lists);
     if (rc) return rc;
     const LuSizes sz32{0, 0, 0, 0, 0, n, n, ws.ldsa, nullptr, nullptr};
+    // buckets are independent: each bucket's three stages run in order on its own auxiliary stream
+    if ((rc = queue_fork(queue))) return rc;
     for (int b = top; b >= 0; --b) {
+        cudaStream_t sb = queue_aux(queue, top - b);
         const WorkList wl{lists + (size_t)b * batch, counts + b, 0};
-        bucket_stage(kCholEdges[b], 0, wl, batch, n, nrhs, A, lda, B, ldb, X, ldx, S, ws, iter, s);
-        chol_bucket<float>(b, wl, batch, true, sz32, false, S, nullptr, ws.sinfo, true, false, 0, s);
-        bucket_stage(kCholEdges[b], 1, wl, batch, n, nrhs, A, lda, B, ldb, X, ldx, S, ws, iter, s);
+        bucket_stage(kCholEdges[b], 0, wl, batch, n, nrhs, A, lda, B, ldb, X, ldx, S, ws, iter, sb);
+        chol_bucket<float>(b, wl, batch, true, sz32, false, S, nullptr, ws.sinfo, true, false, 0, sb);
+        bucket_stage(kCholEdges[b], 1, wl, batch, n, nrhs, A, lda, B, ldb, X, ldx, S, ws, iter, sb);
     }
+    queue_join(queue);
     if ((rc = launch_status())) return rc;
     // FP64 fallback for the instances that set fkey: X = B, then dpotrf + dpotrs on A, X
     rc = bucketize(ws.fkey, batch, kCholEdges, kCholBuckets, s, bws_f, &counts, &lists);
     if (rc) return rc;
     const LuSizes sz64{0, 0, 0, 0, 0, n, n, lda, ldx, nrhs};
+    if ((rc = queue_fork(queue))) return rc;
     for (int b = top; b >= 0; --b) {
+        cudaStream_t sb = queue_aux(queue, top - b);
         const WorkList wl{lists + (size_t)b * batch, counts + b, 0};
-        copy_rhs_vkernel<<<std::min(batch, 1184), 256, 0, s>>>(wl, n, nrhs, B, ldb, X, ldx);
-        chol_bucket<double>(b, wl, batch, true, sz64, false, A, X, info, true, true, max_nrhs, s);
+        copy_rhs_vkernel<<<std::min(batch, 1184), 256, 0, sb>>>(wl, n, nrhs, B, ldb, X, ldx);
+        chol_bucket<double>(b, wl, batch, true, sz64, false, A, X, info, true, true, max_nrhs, sb);
     }
+    queue_join(queue);
     return launch_status();
 }
 

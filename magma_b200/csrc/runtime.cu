@@ -117,6 +117,7 @@ void magma_queue_create_internal(magma_device_t device, magma_queue_t* queue_ptr
     q->ws = nullptr;
     q->ws_bytes = 0;
     q->h_flag = nullptr;
+    q->aux_ready = false;
     cudaSetDevice(device);
     cudaStreamCreateWithFlags(&q->stream, cudaStreamNonBlocking);
     *queue_ptr = q;
@@ -135,6 +136,7 @@ void magma_queue_create_from_cuda_internal(magma_device_t device, cudaStream_t s
     q->ws = nullptr;
     q->ws_bytes = 0;
     q->h_flag = nullptr;
+    q->aux_ready = false;
     *queue_ptr = q;
 }
 
@@ -143,6 +145,14 @@ void magma_queue_destroy_internal(magma_queue_t queue, const char*, const char*,
     cudaStreamSynchronize(queue->stream);
     if (queue->ws) cudaFree(queue->ws);
     if (queue->h_flag) cudaFreeHost(queue->h_flag);
+    if (queue->aux_ready) {
+        for (int i = 0; i < mb200::kAuxStreams; ++i) {
+            cudaStreamSynchronize(queue->aux[i]);
+            cudaStreamDestroy(queue->aux[i]);
+            cudaEventDestroy(queue->ev_join[i]);
+        }
+        cudaEventDestroy(queue->ev_fork);
+    }
     if (queue->own_stream) cudaStreamDestroy(queue->stream);
     delete queue;
 }
@@ -236,6 +246,30 @@ void magma_iset_pointer(magma_int_t** out, magma_int_t* in, magma_int_t lda, mag
 }  // extern "C"
 
 namespace mb200 {
+magma_int_t queue_fork(magma_queue_t queue) {
+    if (!queue->aux_ready) {
+        bool ok = cudaEventCreateWithFlags(&queue->ev_fork, cudaEventDisableTiming) == cudaSuccess;
+        for (int i = 0; i < kAuxStreams && ok; ++i)
+            ok = cudaStreamCreateWithFlags(&queue->aux[i], cudaStreamNonBlocking) == cudaSuccess &&
+                 cudaEventCreateWithFlags(&queue->ev_join[i], cudaEventDisableTiming) == cudaSuccess;
+        if (!ok) {
+            cudaGetLastError();
+            return MAGMA_ERR_UNKNOWN;
+        }
+        queue->aux_ready = true;
+    }
+    cudaEventRecord(queue->ev_fork, queue->stream);
+    for (int i = 0; i < kAuxStreams; ++i) cudaStreamWaitEvent(queue->aux[i], queue->ev_fork, 0);
+    return MAGMA_SUCCESS;
+}
+
+void queue_join(magma_queue_t queue) {
+    for (int i = 0; i < kAuxStreams; ++i) {
+        cudaEventRecord(queue->ev_join[i], queue->aux[i]);
+        cudaStreamWaitEvent(queue->stream, queue->ev_join[i], 0);
+    }
+}
+
 void* queue_workspace(magma_queue_t queue, size_t bytes) {
     if (bytes <= queue->ws_bytes) return queue->ws;
     // round up to 2 MiB so that small growth steps do not reallocate
