@@ -230,16 +230,8 @@ __device__ void blocked_potrs(const T* __restrict__ A, int n, int lda, bool uppe
                 }
             }
             __syncthreads();
-            if (t >= j1 && t < n) {
-#pragma unroll
-                for (int kk = 0; kk < 32; ++kk) {
-                    if (j0 + kk < j1) {
-                        const T l = L(t, j0 + kk);
-#pragma unroll
-                        for (int r = 0; r < R; ++r) b[r] = fma_rn(-sh.sb[kk][r], l, b[r]);
-                    }
-                }
-            }
+            if (t >= j1 && t < n)
+                block_update<T, R, false>(b, sh.sb, j1 - j0, [&](int q) { return L(t, j0 + q); });
         }
         // backward: L^T x = y, blocks descending (column sweep of U = L^T)
         for (int J = nblk - 1; J >= 0; --J) {
@@ -264,16 +256,8 @@ __device__ void blocked_potrs(const T* __restrict__ A, int n, int lda, bool uppe
                 }
             }
             __syncthreads();
-            if (t < j0) {
-#pragma unroll
-                for (int kk = 31; kk >= 0; --kk) {
-                    if (j0 + kk < j1) {
-                        const T u = L(j0 + kk, t);
-#pragma unroll
-                        for (int r = 0; r < R; ++r) b[r] = fma_rn(-sh.sb[kk][r], u, b[r]);
-                    }
-                }
-            }
+            if (t < j0)
+                block_update<T, R, true>(b, sh.sb, j1 - j0, [&](int q) { return L(j0 + q, t); });
         }
         if (t < n) {
 #pragma unroll

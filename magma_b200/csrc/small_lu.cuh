@@ -100,6 +100,30 @@ template <typename T> __device__ __forceinline__ typename Vec2<T>::type make_vec
 template <> __device__ __forceinline__ double2 make_vec2<double>(double x, double y) { return make_double2(x, y); }
 template <> __device__ __forceinline__ float2 make_vec2<float>(float x, float y) { return make_float2(x, y); }
 
+// b[r] -= sb[kk][r] * f(kk) for the cnt (<= 32) entries of one 32-row block, as
+// single fma's in ascending kk (or descending when DESC). The factor entries
+// are loaded in groups of 16 with clamped, always-valid indices, so a group's
+// loads are issued together instead of one load -> fma dependency per entry.
+template <typename T, int R, bool DESC, typename F>
+__device__ __forceinline__ void block_update(T (&b)[R], const T (&sb)[32][R], int cnt, F&& f) {
+    constexpr int G = 16;
+#pragma unroll
+    for (int g = 0; g < 32; g += G) {
+        const int base = DESC ? 32 - G - g : g;
+        T v[G];
+#pragma unroll
+        for (int q = 0; q < G; ++q) v[q] = f(min(base + q, cnt - 1));
+#pragma unroll
+        for (int qq = 0; qq < G; ++qq) {
+            const int q = DESC ? G - 1 - qq : qq;
+            if (base + q < cnt) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) b[r] = fma_rn(-sb[base + q][r], v[q], b[r]);
+            }
+        }
+    }
+}
+
 // Shared memory one matrix needs.
 template <typename T, int NC, int NW>
 struct SmallLuShared {
