@@ -1,0 +1,277 @@
+// lu_tc.cu -- FP32-accurate batched LU with the trailing matrix resident in
+// tensor memory and its updates on the tensor cores (tcgen05, kind::tf32).
+//
+// Used by the mixed-precision solve (magma_dsgesv_batched) for n <= 256, n a
+// multiple of 32, in place of conversion + FP32 CUDA-core LU. One CTA per SM
+// walks the batch; per instance:
+//   1. thread t reads row t of the FP64 matrix once, converts it to FP32 into
+//      TMEM (rows 0..127: lanes 0..127, columns 0..255; rows 128..255: the same
+//      lanes, columns 256..511 -- the whole 256 KB of TMEM holds the matrix),
+//      and forms ||A||_inf and the overflow test on the way (dlag2s + dlange);
+//   2. for each 32-column panel: the panel is read from TMEM into registers and
+//      factored with the register pivot steps of small_lu.cuh (rows never move;
+//      each thread tracks its row's LAPACK position); a row chosen as a pivot
+//      is final and is stored to the output at its position; the pivot rows'
+//      trailing entries are gathered to shared memory and solved with L11
+//      (U12), and the trailing update A22 -= L21 U12 runs on the tensor cores
+//      as three TF32 products per K step (lo*hi + hi*lo + hi*hi of the split
+//      operands, accumulating in FP32 in TMEM), which carries ~21 bits of each
+//      product -- single-precision quality, enough for FP64 refinement to
+//      converge for kappa up to ~1e6 as with a CUDA-core FP32 LU.
+// The CUDA cores do the pivoting while the tensor cores do ~80% of the flops;
+// the FP64 matrix is read from HBM once and the factors written once.
+// Every wait on the tensor core is bounded: on time-out the kernel raises an
+// error flag, frees its TMEM and returns.
+#include "internal.h"
+#include "small_lu.cuh"
+#include "tc_ptx.cuh"
+#include "lu_tc.h"
+#include <cfloat>
+#include <climits>
+
+namespace mb200 {
+
+constexpr int kTcNT = 256;        // threads = matrix rows (n <= 256)
+constexpr int kTcTrail = 224;     // trailing columns of the first panel at n = 256
+
+struct TcLuSmem {
+    float A[2][2][128 * 32];        // L21 operand: [row half][hi, lo], K-major canonical (16 KB each)
+    float B[2][kTcTrail * 32];      // U12 operand: [hi, lo], K-major canonical (28 KB each)
+    float Ug[32][kTcTrail + 1];     // pivot rows' trailing entries; U12 after the solve
+    float L11[32][33];
+    SmallLuShared<float, 32, 8> lu;
+    double red[kTcNT / 32];
+    unsigned long long mbar;
+    uint32_t tmem_base;
+};
+
+// Float index of (row, k) in a K-major no-swizzle operand: 8x4 core matrices of
+// 128 bytes; K-adjacent core matrices 128 bytes apart (LBO), row groups 1024 (SBO).
+__device__ __forceinline__ int kmajor(int row, int k) {
+    return (((row >> 3) * 8 + (k >> 2)) * 8 + (row & 7)) * 4 + (k & 3);
+}
+constexpr uint32_t kLbo = 128, kSbo = 1024;
+
+// U12 = L11^-1 A12 for column c of sh.Ug (unit lower L11), rows in groups of 8.
+__device__ __forceinline__ void tc_trsm_column(TcLuSmem& sh, int c) {
+#pragma unroll 1
+    for (int q0 = 0; q0 < 32; q0 += 8) {
+        float x[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) x[r] = sh.Ug[q0 + r][c];
+        for (int rr = 0; rr < q0; ++rr) {
+            const float u = sh.Ug[rr][c];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) x[r] = fmaf(sh.L11[q0 + r][rr], -u, x[r]);
+        }
+        static_for<0, 8>([&](auto rc) {
+            constexpr int rr = decltype(rc)::value;
+#pragma unroll
+            for (int r = rr + 1; r < 8; ++r) x[r] = fmaf(sh.L11[q0 + r][q0 + rr], -x[rr], x[r]);
+        });
+#pragma unroll
+        for (int r = 0; r < 8; ++r) sh.Ug[q0 + r][c] = x[r];
+    }
+}
+
+__global__ void __launch_bounds__(kTcNT, 1)
+lu_tf32x3_kernel(TcLuArgs g) {
+    extern __shared__ unsigned char tc_smem_raw[];
+    // 1024-byte alignment of the operand buffers (descriptors address 16-byte units)
+    const uint32_t raw = tc::smem_addr(tc_smem_raw);
+    TcLuSmem& sh = *reinterpret_cast<TcLuSmem*>(tc_smem_raw + (((raw + 1023u) & ~1023u) - raw));
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5, half = t >> 7;
+    const int n = g.n;
+    const uint32_t mbar = tc::smem_addr(&sh.mbar);
+    if (w == 0) {
+        tc::tmem_alloc(tc::smem_addr(&sh.tmem_base), 512);
+        tc::tmem_relinquish();
+    }
+    if (t == 0) {
+        tc::mbar_init(mbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tbase = sh.tmem_base;
+    // this thread's lane (row t): lane field 32*(w%4) + lane (implicit), column base half*256
+    const uint32_t trow = tbase + (uint32_t(32 * (w & 3)) << 16) + uint32_t(half * 256);
+    uint32_t phase = 0;
+    bool failed = false;
+    for (int id = blockIdx.x; id < g.batch && !failed; id += gridDim.x) {
+        const double* A = g.dA[id];
+        float* S = g.SA + (size_t)id * n * n;
+        // ---- 1. FP64 row -> FP32 TMEM, row sums, overflow ----
+        double rs = 0.0;
+        bool ovf = false;
+        for (int c0 = 0; c0 < n; c0 += 32) {
+            float v[32];
+#pragma unroll
+            for (int c = 0; c < 32; ++c) {
+                const double a = (t < n) ? A[t + (size_t)(c0 + c) * g.lda] : 0.0;
+                rs += fabs(a);
+                ovf |= !(fabs(a) <= (double)FLT_MAX);
+                v[c] = (float)a;
+            }
+            tc::tmem_st32(trow + c0, v);
+        }
+        tc::wait_st();
+        for (int off = 16; off > 0; off >>= 1) rs = fmax(rs, __shfl_xor_sync(kFullMask, rs, off));
+        if (lane == 0) sh.red[w] = rs;
+        tc::fence_before_sync();
+        const int any_ovf = __syncthreads_or(ovf);
+        tc::fence_after_sync();
+        if (t == 0) {
+            double m = 0.0;
+            for (int k = 0; k < kTcNT / 32; ++k) m = fmax(m, sh.red[k]);
+            g.anrm[id] = m;
+            g.iter[id] = any_ovf ? -2 : 0;
+            if (any_ovf) g.fail_list[atomicAdd(g.fail_count, 1)] = id;
+        }
+        if (any_ovf) {          // block-uniform: the FP64 fallback takes this instance
+            __syncthreads();
+            continue;
+        }
+        // ---- 2. panels ----
+        int pos = (t < n) ? t : INT_MAX / 2;
+        int info = 0;
+        for (int k0 = 0; k0 < n && !failed; k0 += 32) {
+            float a[32];
+            tc::tmem_ld32(trow + k0, a);
+            tc::wait_ld();
+            int my_ipiv = 0;
+            lu_panel_steps<float, 32, kTcNT / 32>(a, n, 32, 32, k0, t, pos, my_ipiv, info, sh.lu);
+            if (t >= k0 && t < k0 + 32) g.ipiv[id][t] = my_ipiv;
+            const bool piv = (t < n) && pos >= k0 && pos < k0 + 32;
+            const int ncols = n - k0 - 32;
+            tc::tmem_st32(trow + k0, a);   // this row's panel entries, kept until it is stored
+            if (piv) {
+#pragma unroll
+                for (int c = 0; c < 32; ++c) sh.L11[pos - k0][c] = a[c];
+            }
+            // a pivot row is final: columns left of the panel from TMEM, the panel from
+            // registers; its trailing entries go to shared memory for the U12 solve
+            if (__any_sync(kFullMask, piv)) {
+                for (int c0 = 0; c0 < k0; c0 += 32) {
+                    float v[32];
+                    tc::tmem_ld32(trow + c0, v);
+                    tc::wait_ld();
+                    if (piv) {
+#pragma unroll
+                        for (int c = 0; c < 32; ++c) S[pos + (size_t)(c0 + c) * n] = v[c];
+                    }
+                }
+                for (int c0 = k0 + 32; c0 < n; c0 += 32) {
+                    float v[32];
+                    tc::tmem_ld32(trow + c0, v);
+                    tc::wait_ld();
+                    if (piv) {
+#pragma unroll
+                        for (int c = 0; c < 32; ++c) sh.Ug[pos - k0][c0 - k0 - 32 + c] = v[c];
+                    }
+                }
+            }
+            if (piv) {
+#pragma unroll
+                for (int c = 0; c < 32; ++c) S[pos + (size_t)(k0 + c) * n] = a[c];
+            }
+            tc::wait_st();
+            __syncthreads();
+            if (ncols <= 0) break;
+            for (int c = t; c < ncols; c += kTcNT) tc_trsm_column(sh, c);
+            __syncthreads();
+            // U12 rows to the output, and the split B operand
+            for (int idx = t; idx < 32 * ncols; idx += kTcNT) {
+                const int r = idx & 31, c = idx >> 5;
+                S[(k0 + r) + (size_t)(k0 + 32 + c) * n] = sh.Ug[r][c];
+            }
+            for (int f = t; f < 32 * ncols; f += kTcNT) {
+                const int k = (f & 3) | (((f >> 5) & 7) << 2);
+                const int c = ((f >> 2) & 7) | ((f >> 8) << 3);
+                float hi, lo;
+                tc::split_tf32(sh.Ug[k][c], hi, lo);
+                sh.B[0][f] = hi;
+                sh.B[1][f] = lo;
+            }
+            // A operand: this row's multipliers (zero for rows already placed)
+            {
+                const bool live = (t < n) && pos >= k0 + 32;
+                const int r = t & 127;
+#pragma unroll
+                for (int kq = 0; kq < 8; ++kq) {
+                    float4 h4, l4;
+                    tc::split_tf32(live ? a[4 * kq + 0] : 0.0f, h4.x, l4.x);
+                    tc::split_tf32(live ? a[4 * kq + 1] : 0.0f, h4.y, l4.y);
+                    tc::split_tf32(live ? a[4 * kq + 2] : 0.0f, h4.z, l4.z);
+                    tc::split_tf32(live ? a[4 * kq + 3] : 0.0f, h4.w, l4.w);
+                    *reinterpret_cast<float4*>(&sh.A[half][0][kmajor(r, 4 * kq)]) = h4;
+                    *reinterpret_cast<float4*>(&sh.A[half][1][kmajor(r, 4 * kq)]) = l4;
+                }
+            }
+            tc::fence_proxy_async_smem();
+            tc::fence_before_sync();
+            __syncthreads();
+            if (t == 0) {
+                tc::fence_after_sync();
+                const uint32_t idesc = tc::idesc_tf32(128, ncols, true);   // D += (-L21) U12
+                const int halves = (n + 127) / 128;
+                for (int h = 0; h < halves; ++h) {
+                    const uint32_t d = tbase + uint32_t(h * 256 + k0 + 32);
+#pragma unroll
+                    for (int s = 0; s < 4; ++s) {   // K = 32 in steps of 8 (two core matrices)
+                        const uint64_t ah = tc::smem_desc(tc::smem_addr(&sh.A[h][0][s * 64]), kLbo, kSbo);
+                        const uint64_t al = tc::smem_desc(tc::smem_addr(&sh.A[h][1][s * 64]), kLbo, kSbo);
+                        const uint64_t bh = tc::smem_desc(tc::smem_addr(&sh.B[0][s * 64]), kLbo, kSbo);
+                        const uint64_t bl = tc::smem_desc(tc::smem_addr(&sh.B[1][s * 64]), kLbo, kSbo);
+                        tc::mma_tf32(d, al, bh, idesc, true);
+                        tc::mma_tf32(d, ah, bl, idesc, true);
+                        tc::mma_tf32(d, ah, bh, idesc, true);
+                    }
+                }
+                tc::commit(mbar);
+            }
+            // bounded wait for the update (about 4 s)
+            bool done = false;
+            const long long t0 = clock64();
+            while (!(done = tc::mbar_try_wait(mbar, phase)) && clock64() - t0 < (1ll << 33)) {
+            }
+            phase ^= 1u;
+            if (__syncthreads_or(!done)) {
+                failed = true;
+                if (t == 0) atomicExch(g.err, 1);
+            }
+            tc::fence_after_sync();
+        }
+        if (t == 0) g.sinfo[id] = info;
+        if (failed && t == 0) {
+            // hand this instance and the rest of this block's share to the FP64 fallback
+            for (int j = id; j < g.batch; j += gridDim.x) {
+                g.iter[j] = -3;
+                g.fail_list[atomicAdd(g.fail_count, 1)] = j;
+            }
+        }
+        __syncthreads();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (w == 0) tc::tmem_dealloc(tbase, 512);
+}
+
+bool lu_tc_supported(int n) { return n >= 32 && n <= 256 && n % 32 == 0; }
+
+size_t lu_tc_smem_bytes() { return sizeof(TcLuSmem) + 1024; }
+
+magma_int_t lu_tc_launch(const TcLuArgs& args, cudaStream_t s) {
+    const int smem = (int)lu_tc_smem_bytes();
+    cudaFuncSetAttribute(lu_tf32x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    int sms = 0, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = std::max(1, std::min(args.batch, sms));
+    lu_tf32x3_kernel<<<grid, kTcNT, smem, s>>>(args);
+    return launch_status();
+}
+
+}  // namespace mb200

@@ -1,0 +1,24 @@
+// lu_tc.h -- host interface of the TMEM-resident tensor-core LU (lu_tc.cu).
+#pragma once
+#include "internal.h"
+
+namespace mb200 {
+
+struct TcLuArgs {
+    int n, batch, lda;
+    double** dA;       // FP64 inputs (read only)
+    float* SA;         // FP32 LU factors, instance i at SA + i*n*n, ld n
+    int** ipiv;        // pivots (1-based)
+    int* sinfo;        // FP32 getrf info
+    double* anrm;      // ||A||_inf
+    int* iter;         // -2 on overflow of the conversion, else 0
+    int* fail_count;   // instances for the FP64 fallback
+    int* fail_list;
+    int* err;          // set to 1 when a tensor-core wait timed out
+};
+
+bool lu_tc_supported(int n);
+size_t lu_tc_smem_bytes();
+magma_int_t lu_tc_launch(const TcLuArgs& args, cudaStream_t s);
+
+}  // namespace mb200

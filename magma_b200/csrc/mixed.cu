@@ -23,6 +23,8 @@
 #include "batched_kernels.h"
 #include "getrs_blocked.cuh"
 #include "mixed_refine.cuh"
+#include "lu_tc.h"
+#include <cstdlib>
 #include "lu_sizes.h"
 #include "vbatched.h"
 #include <cfloat>
@@ -40,6 +42,7 @@ struct MixedWs {
     float* R;           // batch * n * R floats (single-precision right-hand sides)
     int* fail_count;    // 1
     int* fail_list;     // batch
+    int* err;           // 1: a tensor-core wait timed out (the instances went to the fallback)
 };
 
 static size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
@@ -47,7 +50,8 @@ static size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
 static size_t mixed_ws_bytes(int n, int batch, int R) {
     return align_up(sizeof(float) * (size_t)batch * n * n) + align_up(sizeof(float*) * batch) +
            align_up(sizeof(int) * batch) + align_up(sizeof(double) * batch) +
-           align_up(sizeof(float) * (size_t)batch * n * R) + align_up(sizeof(int)) + align_up(sizeof(int) * batch);
+           align_up(sizeof(float) * (size_t)batch * n * R) + align_up(sizeof(int)) + align_up(sizeof(int) * batch) +
+           align_up(sizeof(int));
 }
 
 static MixedWs carve(void* base, int n, int batch, int R) {
@@ -59,7 +63,8 @@ static MixedWs carve(void* base, int n, int batch, int R) {
     w.anrm = reinterpret_cast<double*>(p);    p += align_up(sizeof(double) * batch);
     w.R = reinterpret_cast<float*>(p);        p += align_up(sizeof(float) * (size_t)batch * n * R);
     w.fail_count = reinterpret_cast<int*>(p); p += align_up(sizeof(int));
-    w.fail_list = reinterpret_cast<int*>(p);
+    w.fail_list = reinterpret_cast<int*>(p);  p += align_up(sizeof(int) * batch);
+    w.err = reinterpret_cast<int*>(p);
     return w;
 }
 
@@ -245,6 +250,17 @@ static void launch_refine(int n, int nrhs, double** A, int lda, int** ipiv, doub
 
 bool dsgesv_supported(int n) { return n <= 512; }
 
+// The tensor-core LU serves n = 96..256 in steps of 32 (smaller orders use the
+// register kernels); MAGMA_B200_TENSOR_CORE_LU=0 in the environment selects
+// the CUDA-core FP32 LU instead (read once).
+static bool use_tensor_core_lu(int n) {
+    static const bool enabled = [] {
+        const char* e = std::getenv("MAGMA_B200_TENSOR_CORE_LU");
+        return !(e && e[0] == '0');
+    }();
+    return enabled && n > 64 && lu_tc_supported(n);
+}
+
 magma_int_t dsgesv_batched(int n, int nrhs, double** dA, int lda, int** ipiv, double** dB, int ldb, double** dX,
                            int ldx, int* iter, int* info, int batch, magma_queue_t queue) {
     constexpr int R = 4;
@@ -256,16 +272,23 @@ magma_int_t dsgesv_batched(int n, int nrhs, double** dA, int lda, int** ipiv, do
     cudaMemsetAsync(info, 0, sizeof(int) * batch, s);
     cudaMemsetAsync(iter, 0, sizeof(int) * batch, s);
     cudaMemsetAsync(w.fail_count, 0, sizeof(int), s);
-    // 1. conversion + norm
-    if (n <= 128) dlag2s_norm_kernel<128><<<batch, 128, 0, s>>>(n, dA, lda, w, iter);
-    else dlag2s_norm_kernel<256><<<batch, 256, 0, s>>>(n, dA, lda, w, iter);
-    // 2. single-precision LU of SA, pivots straight into the caller's ipiv
-    const WorkList all{nullptr, nullptr, batch};
-    const LuSizes szs{n, n, n, n, R, nullptr, nullptr, nullptr, nullptr, nullptr};
-    magma_int_t rc = small_lu_supported(n, n)
-                         ? getrf_small<float>(all, batch, false, szs, n, n, w.SA_ptr, ipiv, w.sinfo, s)
-                         : getrf_blocked<float>(all, batch, false, szs, n, w.SA_ptr, ipiv, w.sinfo, s);
-    if (rc) return rc;
+    magma_int_t rc = 0;
+    if (use_tensor_core_lu(n)) {
+        // 1+2. conversion, norm and an FP32-accurate LU on the tensor cores, TMEM-resident
+        cudaMemsetAsync(w.err, 0, sizeof(int), s);
+        const TcLuArgs args{n, batch, lda, dA, w.SA, ipiv, w.sinfo, w.anrm, iter, w.fail_count, w.fail_list, w.err};
+        if ((rc = lu_tc_launch(args, s))) return rc;
+    } else {
+        // 1. conversion + norm
+        if (n <= 128) dlag2s_norm_kernel<128><<<batch, 128, 0, s>>>(n, dA, lda, w, iter);
+        else dlag2s_norm_kernel<256><<<batch, 256, 0, s>>>(n, dA, lda, w, iter);
+        // 2. single-precision LU of SA, pivots straight into the caller's ipiv
+        const WorkList all{nullptr, nullptr, batch};
+        const LuSizes szs{n, n, n, n, R, nullptr, nullptr, nullptr, nullptr, nullptr};
+        rc = small_lu_supported(n, n) ? getrf_small<float>(all, batch, false, szs, n, n, w.SA_ptr, ipiv, w.sinfo, s)
+                                      : getrf_blocked<float>(all, batch, false, szs, n, w.SA_ptr, ipiv, w.sinfo, s);
+        if (rc) return rc;
+    }
     // 3. refinement
     if (n <= 64) launch_refine<64, R>(n, nrhs, dA, lda, ipiv, dB, ldb, dX, ldx, w, iter, batch, s);
     else if (n <= 128) launch_refine<128, R>(n, nrhs, dA, lda, ipiv, dB, ldb, dX, ldx, w, iter, batch, s);

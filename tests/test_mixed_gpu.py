@@ -69,3 +69,24 @@ def test_dsgesv_rhs_counts(cuda, n, nrhs):
     be = T.backward_error(A_np, X.cpu().numpy(), B_np, n)
     assert be.max() <= 1e-14, (be.max(), it)
     assert (it.cpu().numpy() >= 0).mean() > 0.5
+
+
+@pytest.mark.parametrize("n", [96, 128, 160, 224, 256])
+def test_dsgesv_tensor_core_lu(cuda, n):
+    """Orders 96..256 in steps of 32 factor on the tensor cores (TMEM-resident LU, split
+    TF32): with kappa up to 1e6 the refinement must converge as from an FP32 LU, and
+    where it does the single-precision pivots are LAPACK's on all but rare near-ties."""
+    import magma_b200 as mb
+    batch = 40
+    A_np, B_np, kap = T.svd_logrand(batch, n, 1e2, 1e6, nrhs=4, seed=500 + n)
+    A, B = dev(A_np, cuda), dev(B_np, cuda)
+    X, ipiv, it, info = mb.dsgesv_batched(A, B)
+    X, it, ipiv = X.cpu().numpy(), it.cpu().numpy(), ipiv.cpu().numpy()
+    be = T.backward_error(A_np, X, B_np, n)
+    assert be.max() <= 1e-14, (be.max(), it)
+    assert (it >= 0).mean() >= 0.9, it
+    assert it[it >= 0].max() <= 8, it
+    O = A_np.copy()
+    oip, _ = oracle.dgetrf_batched(O, n)
+    same = [np.array_equal(ipiv[i], oip[i]) for i in range(batch) if it[i] >= 0]
+    assert np.mean(same) >= 0.8, np.mean(same)
