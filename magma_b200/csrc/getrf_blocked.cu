@@ -18,7 +18,8 @@ constexpr int blocked_min_blocks() {
 template <typename T, int NB, int NT, int CW, int CB>
 __global__ void __launch_bounds__(NT, (blocked_min_blocks<T, NT>()))
 getrf_blocked_kernel(WorkList wl, LuSizes sz, T** dA_array, int** ipiv_array, int* info_array) {
-    __shared__ BlockedLuShared<T, NB, NT, CW> sh;
+    extern __shared__ __align__(16) unsigned char getrf_smem[];
+    BlockedLuShared<T, NB, NT, CW>& sh = *reinterpret_cast<BlockedLuShared<T, NB, NT, CW>*>(getrf_smem);
     for (int w = blockIdx.x; w < wl.size(); w += gridDim.x) {
         const int id = wl.at(w);
         const int m = sz.get_m(id), n = sz.get_n(id), lda = sz.get_lda(id);
@@ -45,16 +46,18 @@ getrs_blocked_kernel(WorkList wl, LuSizes sz, bool trans, T** dA_array, int** ip
 bool blocked_lu_supported(int max_m) { return max_m <= 1024; }
 
 template <typename K>
-static int blocked_grid(K kernel, int threads, int bound, bool persistent) {
+static int blocked_grid(K kernel, int threads, int bound, bool persistent, size_t smem = 0) {
     if (!persistent) return std::max(1, bound);
-    return std::max(1, std::min(bound, resident_blocks((const void*)kernel, threads, 0)));
+    return std::max(1, std::min(bound, resident_blocks((const void*)kernel, threads, smem)));
 }
 
 template <typename T, int NB, int NT, int CW, int CB>
 static void launch_getrf_blocked(const WorkList& wl, int bound, bool persistent, const LuSizes& sz, T** A, int** ipiv,
                                  int* info, cudaStream_t s) {
     auto k = getrf_blocked_kernel<T, NB, NT, CW, CB>;
-    k<<<blocked_grid(k, NT, bound, persistent), NT, 0, s>>>(wl, sz, A, ipiv, info);
+    const int smem = (int)sizeof(BlockedLuShared<T, NB, NT, CW>);
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    k<<<blocked_grid(k, NT, bound, persistent, smem), NT, smem, s>>>(wl, sz, A, ipiv, info);
 }
 
 template <typename T>
