@@ -291,6 +291,26 @@ magma_int_t magma_dposv_vbatched_max_nocheck(magma_uplo_t uplo, magma_int_t* n, 
                                              magma_int_t max_n, magma_int_t max_nrhs, magma_queue_t queue);
 
 /* ------------------------------------------------------------------------
+ * Kernel-variant tuning (no reference counterpart; takes the role of the
+ * reference's static tables control/batched_kernel_param.h and
+ * magmablas/gemm_config/*.h). The table holds 9 values: the GEMM tile variant
+ * (0: 64x64, 1: 32x32, 2: 16x16) for max(M,N) <= 16, <= 32, <= 64 and larger,
+ * first for FP64 then FP32, and 1/0 for the tensor-core LU in
+ * magma_dsgesv_batched (n = 96..256, step 32). Defaults are built in;
+ * MAGMA_B200_TUNING=<file> loads a saved table at first use. Variants of one
+ * family compute bit-identical results; tuning changes speed only. Not to be
+ * called while other calls of this library are in flight.
+ * magma_b200_autotune times every variant on the queue's device with synthetic
+ * problems and keeps the fastest (synchronises the queue). tuning_get returns
+ * the number of values (9) and fills `values` when count >= 9; tuning_set
+ * returns MAGMA_ERR_ILLEGAL_VALUE for a wrong count or an out-of-range value. */
+magma_int_t magma_b200_autotune(magma_queue_t queue);
+magma_int_t magma_b200_tuning_get(magma_int_t* values, magma_int_t count);
+magma_int_t magma_b200_tuning_set(const magma_int_t* values, magma_int_t count);
+magma_int_t magma_b200_tuning_save(const char* path);
+magma_int_t magma_b200_tuning_load(const char* path);
+
+/* ------------------------------------------------------------------------
  * Batched GEMM: C_i = alpha op(A_i) op(B_i) + beta C_i (C not read when beta == 0,
  * magmablas/gemm_template_device.cuh:197). Checks as
  * magmablas/dgemm_batched_core.cu:180-213 (transA -1, transB -2, m -3, n -4, k -5,

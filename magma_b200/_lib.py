@@ -27,6 +27,7 @@ MagmaLeft, MagmaRight = 141, 142
 
 MAGMA_SUCCESS = 0
 MAGMA_ERR_NOT_SUPPORTED = -103
+MAGMA_ERR_ILLEGAL_VALUE = -104
 MAGMA_ERR_DEVICE_ALLOC = -113
 
 # name -> (restype, argtypes). Every symbol declared in include/magma_b200.h
@@ -97,6 +98,12 @@ SIGNATURES: dict[str, tuple] = {
     "magmablas_sgemm_vbatched_nocheck": (None, [_i, _i, _p, _p, _p, _f, _p, _p, _p, _p, _f, _p, _p, _i, _p]),
     "magma_dsposv_vbatched": (_i, [_i, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _i, _p]),
     "magma_dsposv_vbatched_max_nocheck": (_i, [_i, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _i, _i, _i, _p]),
+    # kernel-variant tuning
+    "magma_b200_autotune": (_i, [_p]),
+    "magma_b200_tuning_get": (_i, [_p, _i]),
+    "magma_b200_tuning_set": (_i, [_p, _i]),
+    "magma_b200_tuning_save": (_i, [_s]),
+    "magma_b200_tuning_load": (_i, [_s]),
     # request loop (include/magma_b200_serve.h)
     "magma_b200_server_create": (_i, [_i, _sz, _i, _i, C.POINTER(_p)]),
     "magma_b200_server_submit": (_i, [_p, _i, _i, _i, _p, _i, _p, _i, _p, _i, C.c_longlong]),

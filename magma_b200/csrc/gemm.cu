@@ -2,16 +2,22 @@
 //
 // Replaces magmablas_{d,s}gemm_batched_core (magmablas/dgemm_batched_core.cu:161-436) and
 // magmablas_{d,s}gemm_vbatched_core (magmablas/dgemm_vbatched_core.cu:28-266). One
-// thread block computes one 64x64 tile of one instance's C with 256 threads (4x4
-// outputs each); op(A) and op(B) are staged through shared memory in K chunks of
-// 16, transposed at load time so the inner loop always reads contiguous vectors,
-// with the next chunk prefetched into registers while the current one is used.
-// Instances are laid out along grid.x as (instance, tile) pairs sized by the
-// largest instance; tiles past an instance's own size exit at once.
+// thread block computes one BM x BN tile of one instance's C (three tile shapes:
+// 64x64 with 256 threads, 32x32 and 16x16 with 64 threads); op(A) and op(B) are
+// staged through shared memory in K chunks of 16, transposed at load time so the
+// inner loop always reads contiguous vectors, with the next chunk prefetched into
+// registers while the current one is used. Every shape accumulates each output
+// over K in the same order, so the shapes give bit-identical results. Variable-size
+// batches are bucketed by max(M, N) on the device; each bucket runs the tile shape
+// the tuning table names for it (tuning.h), on its own auxiliary stream, with
+// (instance, tile) pairs along grid.x sized by the bucket's edge; tiles past an
+// instance's own size exit at once.
 // Epilogue as the reference (magmablas/gemm_template_device.cuh:197-227): C is not
 // read when beta == 0.
 #include "internal.h"
 #include "vbatched.h"
+#include "tuning.h"
+#include "lu_sizes.h"
 #include <algorithm>
 
 namespace mb200 {
@@ -27,18 +33,34 @@ struct GemmSizes {
     __device__ __forceinline__ int LDC(int i) const { return ldc_arr ? ldc_arr[i] : ldc; }
 };
 
-template <typename T, bool TA, bool TB>
-__global__ void __launch_bounds__(256)
+// One tile shape of the kernel: BM x BN tile of C, TM x TN outputs per thread.
+template <int BM_, int BN_, int TM_, int TN_>
+struct GemmTile {
+    static constexpr int BM = BM_, BN = BN_, BK = 16, TM = TM_, TN = TN_;
+    static constexpr int NT = (BM / TM) * (BN / TN);
+    static constexpr int EA = BM * BK / NT, EB = BK * BN / NT;   // staged elements per thread
+};
+// The variants the tuning table chooses between (index = variant id).
+using GemmTile0 = GemmTile<64, 64, 4, 4>;   // 256 threads
+using GemmTile1 = GemmTile<32, 32, 4, 4>;   // 64 threads
+using GemmTile2 = GemmTile<16, 16, 2, 2>;   // 64 threads
+constexpr int kGemmVariants = 3;
+
+template <typename T, bool TA, bool TB, typename S>
+__global__ void __launch_bounds__(S::NT)
 gemm_tile_kernel(GemmSizes g, T alpha, const T* const* __restrict__ A_arr, const T* const* __restrict__ B_arr, T beta,
-                 T** __restrict__ C_arr, int tiles_m, int tiles_n) {
-    constexpr int BM = 64, BN = 64, BK = 16, TM = 4, TN = 4, NT = 256;
+                 T** __restrict__ C_arr, int tiles_m, int tiles_n, WorkList wl) {
+    constexpr int BM = S::BM, BN = S::BN, BK = S::BK, TM = S::TM, TN = S::TN, NT = S::NT;
+    constexpr int EA = S::EA, EB = S::EB;
     // rows padded by one element: the K-fastest staging stores would otherwise
     // hit one bank 16 times
     __shared__ T sA[BK][BM + 1];
     __shared__ T sB[BK][BN + 1];
     const int tiles = tiles_m * tiles_n;
-    const int id = blockIdx.x / tiles;
-    const int t = blockIdx.x - id * tiles;
+    const int w = blockIdx.x / tiles;
+    if (w >= wl.size()) return;
+    const int id = wl.at(w);
+    const int t = blockIdx.x - w * tiles;
     const int i0 = (t / tiles_n) * BM, j0 = (t % tiles_n) * BN;
     const int m = g.M(id), n = g.N(id), k = g.K(id);
     if (i0 >= m || j0 >= n) return;
@@ -57,11 +79,11 @@ gemm_tile_kernel(GemmSizes g, T alpha, const T* const* __restrict__ A_arr, const
 #pragma unroll
         for (int j = 0; j < TN; ++j) acc[i][j] = T(0);
 
-    // each thread stages 4 elements of the A chunk and 4 of the B chunk
-    T ra[4], rb[4];
+    // each thread stages EA elements of the A chunk and EB of the B chunk
+    T ra[EA], rb[EB];
     auto load_chunk = [&](int k0) {
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
+        for (int e = 0; e < EA; ++e) {
             const int idx = tid + e * NT;
             int r, c;
             if (!TA) { r = idx % BM; c = idx / BM; } else { c = idx % BK; r = idx / BK; }
@@ -69,7 +91,7 @@ gemm_tile_kernel(GemmSizes g, T alpha, const T* const* __restrict__ A_arr, const
             ra[e] = (gi < m && gk < k) ? (TA ? A[gk + (size_t)gi * lda] : A[gi + (size_t)gk * lda]) : T(0);
         }
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
+        for (int e = 0; e < EB; ++e) {
             const int idx = tid + e * NT;
             int c, j;
             if (!TB) { c = idx % BK; j = idx / BK; } else { j = idx % BN; c = idx / BN; }
@@ -79,14 +101,14 @@ gemm_tile_kernel(GemmSizes g, T alpha, const T* const* __restrict__ A_arr, const
     };
     auto store_chunk = [&]() {
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
+        for (int e = 0; e < EA; ++e) {
             const int idx = tid + e * NT;
             int r, c;
             if (!TA) { r = idx % BM; c = idx / BM; } else { c = idx % BK; r = idx / BK; }
             sA[c][r] = ra[e];
         }
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
+        for (int e = 0; e < EB; ++e) {
             const int idx = tid + e * NT;
             int c, j;
             if (!TB) { c = idx % BK; j = idx / BK; } else { j = idx % BN; c = idx / BN; }
@@ -126,19 +148,76 @@ gemm_tile_kernel(GemmSizes g, T alpha, const T* const* __restrict__ A_arr, const
     }
 }
 
+template <typename T, typename S>
+static magma_int_t gemm_launch_tile(bool TA, bool TB, const GemmSizes& g, T alpha, const T* const* A, const T* const* B,
+                                    T beta, T** C, const WorkList& wl, int bound, int max_m, int max_n,
+                                    cudaStream_t s) {
+    const int tiles_m = ceildiv(max_m, S::BM), tiles_n = ceildiv(max_n, S::BN);
+    const long blocks = (long)bound * tiles_m * tiles_n;
+    if (blocks > 0x7fffffffL) return MAGMA_ERR_NOT_SUPPORTED;
+    const dim3 grid((unsigned)blocks);
+    if (!TA && !TB) gemm_tile_kernel<T, false, false, S><<<grid, S::NT, 0, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n, wl);
+    else if (!TA && TB) gemm_tile_kernel<T, false, true, S><<<grid, S::NT, 0, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n, wl);
+    else if (TA && !TB) gemm_tile_kernel<T, true, false, S><<<grid, S::NT, 0, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n, wl);
+    else gemm_tile_kernel<T, true, true, S><<<grid, S::NT, 0, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n, wl);
+    return 0;
+}
+
+template <typename T>
+static magma_int_t gemm_launch_variant(int variant, magma_trans_t ta, magma_trans_t tb, const GemmSizes& g, T alpha,
+                                       const T* const* A, const T* const* B, T beta, T** C, const WorkList& wl,
+                                       int bound, int max_m, int max_n, cudaStream_t s) {
+    const bool TA = (ta != MagmaNoTrans), TB = (tb != MagmaNoTrans);   // real types: ConjTrans == Trans
+    switch (variant) {
+        case 1: return gemm_launch_tile<T, GemmTile1>(TA, TB, g, alpha, A, B, beta, C, wl, bound, max_m, max_n, s);
+        case 2: return gemm_launch_tile<T, GemmTile2>(TA, TB, g, alpha, A, B, beta, C, wl, bound, max_m, max_n, s);
+        default: return gemm_launch_tile<T, GemmTile0>(TA, TB, g, alpha, A, B, beta, C, wl, bound, max_m, max_n, s);
+    }
+}
+
+// Size buckets of max(M, N): the tuning table names a tile variant per bucket.
+static const int kGemmEdges[kGemmBuckets] = {16, 32, 64, 1 << 30};
+
+static int gemm_bucket_of(int mn) {
+    for (int b = 0; b < kGemmBuckets; ++b)
+        if (mn <= kGemmEdges[b]) return b;
+    return kGemmBuckets - 1;
+}
+
+// Fixed size: one launch with the bucket's variant.
 template <typename T>
 static magma_int_t gemm_launch(magma_trans_t ta, magma_trans_t tb, const GemmSizes& g, T alpha, const T* const* A,
                                const T* const* B, T beta, T** C, int batch, int max_m, int max_n, cudaStream_t s) {
-    const int tiles_m = ceildiv(max_m, 64), tiles_n = ceildiv(max_n, 64);
-    const long blocks = (long)batch * tiles_m * tiles_n;
-    if (blocks > 0x7fffffffL) return MAGMA_ERR_NOT_SUPPORTED;
-    const bool TA = (ta != MagmaNoTrans), TB = (tb != MagmaNoTrans);   // real types: ConjTrans == Trans
-    const dim3 grid((unsigned)blocks);
-    if (!TA && !TB) gemm_tile_kernel<T, false, false><<<grid, 256, 0, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n);
-    else if (!TA && TB) gemm_tile_kernel<T, false, true><<<grid, 256, 0, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n);
-    else if (TA && !TB) gemm_tile_kernel<T, true, false><<<grid, 256, 0, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n);
-    else gemm_tile_kernel<T, true, true><<<grid, 256, 0, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n);
-    return launch_status();
+    const int v = tuning().gemm_variant[sizeof(T) == 8 ? 0 : 1][gemm_bucket_of(std::max(max_m, max_n))];
+    const WorkList all{nullptr, nullptr, batch};
+    magma_int_t rc = gemm_launch_variant<T>(v, ta, tb, g, alpha, A, B, beta, C, all, batch, max_m, max_n, s);
+    return rc ? rc : launch_status();
+}
+
+// Variable size: instances bucketed by max(M, N) on the device, each bucket on its own
+// auxiliary stream with its variant's tile (grid sized by the bucket's edge).
+template <typename T>
+static magma_int_t gemm_launch_var(magma_trans_t ta, magma_trans_t tb, const GemmSizes& g, T alpha, const T* const* A,
+                                   const T* const* B, T beta, T** C, int batch, int max_m, int max_n,
+                                   magma_queue_t queue) {
+    const int top = gemm_bucket_of(std::max(max_m, max_n));
+    int* ws = static_cast<int*>(queue_workspace(queue, sizeof(int) * bucketize_ws_ints(batch, kGemmBuckets)));
+    if (!ws) return MAGMA_ERR_DEVICE_ALLOC;
+    int *counts, *lists;
+    int edges[kGemmBuckets];
+    for (int b = 0; b < kGemmBuckets; ++b) edges[b] = std::min(kGemmEdges[b], std::max(max_m, max_n));
+    magma_int_t rc = bucketize2(g.m_arr, g.n_arr, batch, edges, kGemmBuckets, queue->stream, ws, &counts, &lists);
+    if (rc) return rc;
+    if ((rc = queue_fork(queue))) return rc;
+    const int* var = tuning().gemm_variant[sizeof(T) == 8 ? 0 : 1];
+    for (int b = top; b >= 0 && !rc; --b) {
+        const WorkList wl{lists + (size_t)b * batch, counts + b, 0};
+        const int em = std::min(edges[b], max_m), en = std::min(edges[b], max_n);
+        rc = gemm_launch_variant<T>(var[b], ta, tb, g, alpha, A, B, beta, C, wl, batch, em, en,
+                                    queue_aux(queue, top - b));
+    }
+    queue_join(queue);
+    return rc ? rc : launch_status();
 }
 
 static bool bad_trans(magma_trans_t t) { return t != MagmaNoTrans && t != MagmaTrans && t != MagmaConjTrans; }
@@ -174,7 +253,7 @@ static void gemm_vbatched_max_nocheck(magma_trans_t ta, magma_trans_t tb, int* m
                                       int* ldc, int batch, int max_m, int max_n, int max_k, magma_queue_t queue) {
     if (max_m <= 0 || max_n <= 0 || max_k <= 0 || batch <= 0) return;
     GemmSizes g{0, 0, 0, 0, 0, 0, m, n, k, lda, ldb, ldc};
-    gemm_launch<T>(ta, tb, g, alpha, A, B, beta, C, batch, max_m, max_n, queue->stream);
+    gemm_launch_var<T>(ta, tb, g, alpha, A, B, beta, C, batch, max_m, max_n, queue);
 }
 
 // magmablas/vbatched_check.cu:48-100 (gemm checker): transA -1, transB -2, m -3, n -4, k -5,

@@ -24,7 +24,7 @@
 #include "getrs_blocked.cuh"
 #include "mixed_refine.cuh"
 #include "lu_tc.h"
-#include <cstdlib>
+#include "tuning.h"
 #include "lu_sizes.h"
 #include "vbatched.h"
 #include <cfloat>
@@ -251,15 +251,9 @@ static void launch_refine(int n, int nrhs, double** A, int lda, int** ipiv, doub
 bool dsgesv_supported(int n) { return n <= 512; }
 
 // The tensor-core LU serves n = 96..256 in steps of 32 (smaller orders use the
-// register kernels); MAGMA_B200_TENSOR_CORE_LU=0 in the environment selects
-// the CUDA-core FP32 LU instead (read once).
-static bool use_tensor_core_lu(int n) {
-    static const bool enabled = [] {
-        const char* e = std::getenv("MAGMA_B200_TENSOR_CORE_LU");
-        return !(e && e[0] == '0');
-    }();
-    return enabled && n > 64 && lu_tc_supported(n);
-}
+// register kernels) unless the tuning table turns it off (it starts from
+// MAGMA_B200_TENSOR_CORE_LU=0 in the environment, or magma_b200_autotune measures).
+static bool use_tensor_core_lu(int n) { return tuning().mixed_tc_lu && n > 64 && lu_tc_supported(n); }
 
 magma_int_t dsgesv_batched(int n, int nrhs, double** dA, int lda, int** ipiv, double** dB, int ldb, double** dX,
                            int ldx, int* iter, int* info, int batch, magma_queue_t queue) {

@@ -1,0 +1,21 @@
+// tuning.h -- the kernel-variant table the dispatchers read, and its autotuner
+// (tuning.cu). Takes the role of the reference's static tuning tables
+// (control/batched_kernel_param.h, magmablas/gemm_config/*.h, tuned for one GPU)
+// with a table measured on the device it runs on.
+#pragma once
+#include "internal.h"
+
+namespace mb200 {
+
+constexpr int kGemmBuckets = 4;   // max(M, N) <= 16, <= 32, <= 64, larger
+
+struct TuningTable {
+    int gemm_variant[2][kGemmBuckets];   // [FP64, FP32][bucket]: tile variant (0: 64x64, 1: 32x32, 2: 16x16)
+    int mixed_tc_lu;                     // 1: tensor-core LU in the mixed solve for n = 96..256, step 32
+};
+
+const TuningTable& tuning();   // defaults, or the file named by MAGMA_B200_TUNING, or the last autotune/set
+TuningTable& tuning_mut();
+constexpr int kTuningValues = 2 * kGemmBuckets + 1;
+
+}  // namespace mb200

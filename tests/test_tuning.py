@@ -1,0 +1,104 @@
+"""The kernel-variant tuning table (magma_b200_tuning_* / magma_b200_autotune).
+
+CPU part: get / set / save / load round trips and argument checks (host only).
+GPU part: every GEMM tile variant gives bit-identical results, and the
+autotuner runs and leaves a valid table."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from magma_b200 import _lib
+
+N_VALUES = 9
+
+
+def _get(lib):
+    v = (C.c_int * N_VALUES)()
+    assert lib.magma_b200_tuning_get(v, N_VALUES) == N_VALUES
+    return list(v)
+
+
+def _set(lib, vals):
+    arr = (C.c_int * len(vals))(*vals)
+    return lib.magma_b200_tuning_set(arr, len(vals))
+
+
+def test_tuning_roundtrip(tmp_path):
+    lib = _lib.load()
+    assert lib.magma_b200_tuning_get(None, 0) == N_VALUES           # size query
+    orig = _get(lib)
+    try:
+        new = [0, 1, 2, 0, 2, 1, 0, 0, 0]
+        assert _set(lib, new) == 0 and _get(lib) == new
+        f = tmp_path / "tune.txt"
+        assert lib.magma_b200_tuning_save(str(f).encode()) == 0
+        assert f.read_text().split()[0] == "magma_b200_tuning_v1"
+        assert _set(lib, orig) == 0 and _get(lib) == orig
+        assert lib.magma_b200_tuning_load(str(f).encode()) == 0 and _get(lib) == new
+        # rejected: wrong count, out-of-range values, unreadable or malformed files
+        assert _set(lib, new[:-1]) == _lib.MAGMA_ERR_ILLEGAL_VALUE
+        assert _set(lib, [3] + new[1:]) == _lib.MAGMA_ERR_ILLEGAL_VALUE
+        assert _set(lib, new[:-1] + [2]) == _lib.MAGMA_ERR_ILLEGAL_VALUE
+        assert lib.magma_b200_tuning_load(str(tmp_path / "missing").encode()) == _lib.MAGMA_ERR_ILLEGAL_VALUE
+        bad = tmp_path / "bad.txt"
+        bad.write_text("magma_b200_tuning_v1\n0 1 2\n")
+        assert lib.magma_b200_tuning_load(str(bad).encode()) == _lib.MAGMA_ERR_ILLEGAL_VALUE
+        assert _get(lib) == new
+    finally:
+        _set(lib, orig)
+
+
+@pytest.mark.gpu
+def test_gemm_variants_bit_identical(cuda):
+    import torch
+
+    import magma_b200 as mb
+    from magma_b200 import testing as T
+    from magma_b200.api import VarBatch
+    lib = _lib.load()
+    orig = _get(lib)
+    M, N, K = T.gemm_sizes(600, 1, 100, seed=9)
+    rng = np.random.default_rng(4)
+    outs = {}
+    try:
+        for prec, dt in (("d", torch.float64), ("s", torch.float32)):
+            As = [rng.standard_normal((int(k), int(m))) for m, k in zip(M, K)]
+            Bs = [rng.standard_normal((int(n), int(k))) for k, n in zip(K, N)]
+            Cs = [rng.standard_normal((int(n), int(m))) for m, n in zip(M, N)]
+            for v in range(3):
+                vals = list(orig)
+                for b in range(4):
+                    vals[(0 if prec == "d" else 4) + b] = v
+                assert _set(lib, vals) == 0
+                gA, gB, gC = VarBatch(As, cuda, dt), VarBatch(Bs, cuda, dt), VarBatch(Cs, cuda, dt)
+                mb.gemm_vbatched(gA, gB, gC, M, N, K, M, K, M, alpha=1.0, beta=0.5)
+                torch.cuda.synchronize()
+                outs[(prec, v)] = gC.buf.cpu().numpy()
+            assert np.array_equal(outs[(prec, 0)], outs[(prec, 1)])
+            assert np.array_equal(outs[(prec, 0)], outs[(prec, 2)])
+            # and the result is right (FP64 reference)
+            ref = [a.T @ b.T + 0.5 * c.T for a, b, c in zip(As, Bs, Cs)]
+            got = VarBatch(Cs, cuda, dt)
+            got.buf = torch.from_numpy(outs[(prec, 0)])
+            tol = 1e-12 if prec == "d" else 1e-4
+            for r, g in zip(ref, got.unpack()):
+                assert np.abs(g.T - r).max() <= tol * max(1.0, np.abs(r).max()) * 128
+    finally:
+        _set(lib, orig)
+
+
+@pytest.mark.gpu
+def test_autotune_runs(cuda, tmp_path):
+    from magma_b200.api import default_queue
+    lib = _lib.load()
+    orig = _get(lib)
+    try:
+        q = default_queue()
+        assert lib.magma_b200_autotune(q.handle) == 0
+        vals = _get(lib)
+        assert all(0 <= v <= 2 for v in vals[:8]) and vals[8] in (0, 1)
+        f = tmp_path / "tuned.txt"
+        assert lib.magma_b200_tuning_save(str(f).encode()) == 0
+    finally:
+        _set(lib, orig)
