@@ -191,7 +191,7 @@ class C3Mixed:
         return 8 * n * n + 2 * 8 * n * r + 4 * n
 
     def launches_per_step(self):
-        return 6   # dlag2s+norm, sgetrf, refine, fallback getrf, copy, fallback getrs
+        return 5   # tensor-core LU, refine, fallback getrf, copy, fallback getrs
 
     def step(self, q, i):
         n = self.n
@@ -239,24 +239,34 @@ class C3Mixed:
         return {"bwd_err_max_mixed": be_mixed, "bwd_err_max_fp64": be_64, "iter_hist": hist}
 
     def dominant_kernel(self, q, stream, reps=5):
-        """The FP32 LU (getrf_blocked_kernel<float>) alone: magma_sgetrf_batched on a float copy."""
-        from magma_b200.api import ptr_array
-
+        """Per-stage device times of the mixed step (queue stage timing: CUDA events the
+        library records on its stream between the LU, refinement and fallback stages);
+        the roofline is quoted for the dominant stage."""
         t = self.torch
-        SA0 = self.A0.float()
-        SA = SA0.clone()
-        pS = ptr_array(SA)
-        n = self.n
-
-        def one(i):
-            q.lib.magma_sgetrf_batched(n, n, vp(pS), n, vp(self.pP), vp(self.info), self.batch, q.handle)
-        one(0)
-        t.cuda.synchronize()
-        ms = timed(stream, one, reps) / reps
-        alg_bytes = self.batch * (2 * 4 * n * n + 4 * n)
-        flops = self.batch * (2.0 / 3.0) * n ** 3
-        return {"kernel": "getrf_blocked_kernel<float,32,256> (magma_sgetrf_batched)", "ms": ms,
-                "alg_bytes": alg_bytes, "tflops": flops / ms / 1e9}
+        n, r, batch = self.n, self.nrhs, self.batch
+        assert q.lib.magma_b200_stage_timing(q.handle, 1) == 0
+        acc = [0.0, 0.0, 0.0]
+        buf = (C.c_float * 8)()
+        for i in range(reps):
+            self.restore(i)
+            self.step(q, i)
+            k = q.lib.magma_b200_stage_times(q.handle, buf, 8)
+            assert k == 3, k
+            for j in range(3):
+                acc[j] += buf[j] / reps
+        q.lib.magma_b200_stage_timing(q.handle, 0)
+        it = self.iter.cpu().clamp(min=0).to(t.float64)
+        passes = float((it + 1).sum())
+        lu_flops = batch * (2.0 / 3.0) * n ** 3
+        refine_bytes = passes * 12.0 * n * n + batch * 16.0 * n * r
+        stages = {"lu_ms": acc[0], "refine_ms": acc[1], "fallback_ms": acc[2]}
+        if acc[1] >= acc[0]:
+            return {"kernel": "dsgesv_refine_kernel<256,4> (FP32 solves + FP64 residuals)", "ms": acc[1],
+                    "alg_bytes": refine_bytes, "tflops": None, "stages": stages,
+                    "alg_note": "12 n^2 B per refinement pass (A in FP64 + LU in FP32), passes = iter + 1"}
+        return {"kernel": "lu_tf32x3_kernel (tcgen05 split-TF32 LU, TMEM-resident)", "ms": acc[0],
+                "alg_flops": lu_flops, "tflops": lu_flops / acc[0] / 1e9, "stages": stages,
+                "alg_bytes": batch * (8.0 * n * n + 4.0 * n * n + 4 * n)}
 
     def e2e_setup(self):
         t = self.torch
@@ -953,12 +963,25 @@ def main():
             line[f"{W.alt_name}_value"] = alt_value
             line[f"{W.alt_name}_ms_per_step"] = ms_alt_total / args.steps
             line.update(W.ratios(value, alt_value))
-        line["roofline"] = {
-            "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-            "frac": achieved / peaks["hbm_gbs"], "traffic": profile_traffic(dom["kernel"].split("<")[0], W.name),
-            "kernel": dom["kernel"], "kernel_ms": dom["ms"], "alg_bytes_per_launch": dom["alg_bytes"],
-            "peak_src": peaks["src"],
-        }
+        if "alg_flops" in dom:   # a tensor-core stage: quoted against the measured dense BF16 peak
+            tf = dom["alg_flops"] / (dom["ms"] * 1e-3) / 1e12
+            line["roofline"] = {
+                "bound": "tensor", "achieved": tf, "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
+                "frac": tf / peaks["bf16_tflops"], "traffic": profile_traffic(dom["kernel"].split(" ")[0], W.name),
+                "kernel": dom["kernel"], "kernel_ms": dom["ms"], "alg_flops_per_launch": dom["alg_flops"],
+                "peak_src": peaks["src"],
+            }
+        else:
+            line["roofline"] = {
+                "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"],
+                "traffic": profile_traffic(dom["kernel"].split("<")[0].split(" ")[0], W.name),
+                "kernel": dom["kernel"], "kernel_ms": dom["ms"], "alg_bytes_per_launch": dom["alg_bytes"],
+                "peak_src": peaks["src"],
+            }
+        for key in ("stages", "alg_note"):
+            if key in dom:
+                line["roofline"][key] = dom[key]
         if dom.get("tflops"):
             line["roofline"]["kernel_tflops"] = dom["tflops"]
         line["e2e"] = {"value": units * ke / (ms_e2e * 1e-3), "unit": W.unit, "h2d_bytes_per_step": W.h2d,

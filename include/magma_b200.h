@@ -73,6 +73,15 @@ cudaStream_t magma_queue_get_cuda_stream(magma_queue_t queue);
  * it before capturing batched calls into a CUDA graph. */
 magma_int_t  magma_queue_reserve_workspace(magma_queue_t queue, size_t bytes);
 
+/* No reference counterpart (the reference's timers are host wall clocks around
+ * whole calls). With stage timing on, multi-kernel routines record CUDA events
+ * on the queue's stream at their stage boundaries -- magma_dgesv_batched
+ * (n > 64): getrf, getrs; magma_dsgesv_batched: LU, refinement, FP64 fallback --
+ * and magma_b200_stage_times returns the last such call's stage durations in ms
+ * (waits for its last event; returns the number of stages written, <= max). */
+magma_int_t  magma_b200_stage_timing(magma_queue_t queue, magma_int_t enable);
+magma_int_t  magma_b200_stage_times(magma_queue_t queue, float* ms, magma_int_t max);
+
 #define magma_queue_create(device, queue_ptr) \
         magma_queue_create_internal(device, queue_ptr, __func__, __FILE__, __LINE__)
 #define magma_queue_create_from_cuda(device, stream, cublas, cusparse, queue_ptr) \

@@ -49,6 +49,8 @@ SIGNATURES: dict[str, tuple] = {
     "magma_queue_get_device": (_i, [_p]),
     "magma_queue_get_cuda_stream": (_p, [_p]),
     "magma_queue_reserve_workspace": (_i, [_p, _sz]),
+    "magma_b200_stage_timing": (_i, [_p, _i]),
+    "magma_b200_stage_times": (_i, [_p, _p, _i]),
     "magma_setvector_internal": (None, [_i, _i, _p, _i, _p, _i, _p, _s, _s, _i]),
     "magma_getvector_internal": (None, [_i, _i, _p, _i, _p, _i, _p, _s, _s, _i]),
     "magma_setvector_async_internal": (None, [_i, _i, _p, _i, _p, _i, _p, _s, _s, _i]),

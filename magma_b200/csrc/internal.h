@@ -27,6 +27,10 @@ struct magma_queue {
     cudaEvent_t  ev_fork;
     cudaEvent_t  ev_join[4];
     bool         aux_ready;
+    // optional stage timing (magma_b200_stage_timing): events at stage boundaries
+    bool         stage_on;
+    int          stage_n;
+    cudaEvent_t  stage_ev[8];
 };
 
 namespace mb200 {
@@ -48,6 +52,11 @@ constexpr int kAuxStreams = 4;
 magma_int_t queue_fork(magma_queue_t queue);
 inline cudaStream_t queue_aux(magma_queue_t queue, int i) { return queue->aux[i % kAuxStreams]; }
 void queue_join(magma_queue_t queue);
+
+// Stage timing: when enabled on the queue, multi-kernel routines record an event
+// on the queue's stream before their first stage and after each stage.
+void queue_stage_begin(magma_queue_t queue);
+void queue_stage_mark(magma_queue_t queue);
 
 // Records a CUDA launch error as a MAGMA error code (0 when none).
 inline magma_int_t launch_status() {

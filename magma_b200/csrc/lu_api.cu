@@ -80,10 +80,14 @@ magma_int_t gesv_impl(const char* name, const char* getrf_name, const char* getr
         return gesv_small<T>(wl, batchCount, false, sz, n, nrhs, dA_array, dipiv_array, dB_array, dinfo_array,
                              queue->stream);
     }
+    queue_stage_begin(queue);   // stages: getrf, getrs
     info = getrf_impl<T>(getrf_name, n, n, dA_array, ldda, dipiv_array, dinfo_array, batchCount, queue);
     if (info != MAGMA_SUCCESS) return info;
-    return getrs_impl<T>(getrs_name, MagmaNoTrans, n, nrhs, dA_array, ldda, dipiv_array, dB_array, lddb,
+    queue_stage_mark(queue);
+    info = getrs_impl<T>(getrs_name, MagmaNoTrans, n, nrhs, dA_array, ldda, dipiv_array, dB_array, lddb,
                          batchCount, queue);
+    queue_stage_mark(queue);
+    return info;
 }
 
 }  // namespace

@@ -267,6 +267,7 @@ magma_int_t dsgesv_batched(int n, int nrhs, double** dA, int lda, int** ipiv, do
     cudaMemsetAsync(iter, 0, sizeof(int) * batch, s);
     cudaMemsetAsync(w.fail_count, 0, sizeof(int), s);
     magma_int_t rc = 0;
+    queue_stage_begin(queue);   // stages: LU, refinement, FP64 fallback
     if (use_tensor_core_lu(n)) {
         // 1+2. conversion, norm and an FP32-accurate LU on the tensor cores, TMEM-resident
         cudaMemsetAsync(w.err, 0, sizeof(int), s);
@@ -283,12 +284,14 @@ magma_int_t dsgesv_batched(int n, int nrhs, double** dA, int lda, int** ipiv, do
                                       : getrf_blocked<float>(all, batch, false, szs, n, w.SA_ptr, ipiv, w.sinfo, s);
         if (rc) return rc;
     }
+    queue_stage_mark(queue);
     // 3. refinement
     if (n <= 64) launch_refine<64, R>(n, nrhs, dA, lda, ipiv, dB, ldb, dX, ldx, w, iter, batch, s);
     else if (n <= 128) launch_refine<128, R>(n, nrhs, dA, lda, ipiv, dB, ldb, dX, ldx, w, iter, batch, s);
     else if (n <= 256) launch_refine<256, R>(n, nrhs, dA, lda, ipiv, dB, ldb, dX, ldx, w, iter, batch, s);
     else launch_refine<512, R>(n, nrhs, dA, lda, ipiv, dB, ldb, dX, ldx, w, iter, batch, s);
     if ((rc = launch_status())) return rc;
+    queue_stage_mark(queue);
     // 4. FP64 fallback on the listed instances (the list length stays on the device)
     const WorkList failed{w.fail_list, w.fail_count, 0};
     const LuSizes szd{n, n, lda, ldx, nrhs, nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -298,6 +301,7 @@ magma_int_t dsgesv_batched(int n, int nrhs, double** dA, int lda, int** ipiv, do
     copy_rhs_kernel<<<std::min(batch, 1184), 256, 0, s>>>(failed, n, nrhs, dB, ldb, dX, ldx);
     rc = small_lu_supported(n, n) ? getrs_small<double>(failed, batch, true, false, szd, n, nrhs, dA, ipiv, dX, s)
                                   : getrs_blocked<double>(failed, batch, true, false, szd, n, nrhs, dA, ipiv, dX, s);
+    queue_stage_mark(queue);
     return rc ? rc : launch_status();
 }
 

@@ -5,6 +5,7 @@
 // implementation is the library's own (no cuBLAS/cuSPARSE handles are
 // created: the batched path does not use them).
 #include "internal.h"
+#include <algorithm>
 
 #include <atomic>
 #include <cstdlib>
@@ -118,6 +119,8 @@ void magma_queue_create_internal(magma_device_t device, magma_queue_t* queue_ptr
     q->ws_bytes = 0;
     q->h_flag = nullptr;
     q->aux_ready = false;
+    q->stage_on = false;
+    q->stage_n = 0;
     cudaSetDevice(device);
     cudaStreamCreateWithFlags(&q->stream, cudaStreamNonBlocking);
     *queue_ptr = q;
@@ -137,6 +140,8 @@ void magma_queue_create_from_cuda_internal(magma_device_t device, cudaStream_t s
     q->ws_bytes = 0;
     q->h_flag = nullptr;
     q->aux_ready = false;
+    q->stage_on = false;
+    q->stage_n = 0;
     *queue_ptr = q;
 }
 
@@ -153,6 +158,8 @@ void magma_queue_destroy_internal(magma_queue_t queue, const char*, const char*,
         }
         cudaEventDestroy(queue->ev_fork);
     }
+    if (queue->stage_on)
+        for (int i = 0; i < 8; ++i) cudaEventDestroy(queue->stage_ev[i]);
     if (queue->own_stream) cudaStreamDestroy(queue->stream);
     delete queue;
 }
@@ -263,6 +270,17 @@ magma_int_t queue_fork(magma_queue_t queue) {
     return MAGMA_SUCCESS;
 }
 
+void queue_stage_begin(magma_queue_t queue) {
+    if (!queue->stage_on) return;
+    queue->stage_n = 0;
+    queue_stage_mark(queue);
+}
+
+void queue_stage_mark(magma_queue_t queue) {
+    if (!queue->stage_on || queue->stage_n >= 8) return;
+    cudaEventRecord(queue->stage_ev[queue->stage_n++], queue->stream);
+}
+
 void queue_join(magma_queue_t queue) {
     for (int i = 0; i < kAuxStreams; ++i) {
         cudaEventRecord(queue->ev_join[i], queue->aux[i]);
@@ -290,3 +308,34 @@ void* queue_workspace(magma_queue_t queue, size_t bytes) {
     return p;
 }
 }  // namespace mb200
+
+extern "C" {
+
+magma_int_t magma_b200_stage_timing(magma_queue_t queue, magma_int_t enable) {
+    if (!queue) return -1;
+    if (enable && !queue->stage_on) {
+        for (int i = 0; i < 8; ++i)
+            if (cudaEventCreate(&queue->stage_ev[i]) != cudaSuccess) {
+                cudaGetLastError();
+                return MAGMA_ERR_UNKNOWN;
+            }
+        queue->stage_on = true;
+    } else if (!enable && queue->stage_on) {
+        cudaStreamSynchronize(queue->stream);
+        for (int i = 0; i < 8; ++i) cudaEventDestroy(queue->stage_ev[i]);
+        queue->stage_on = false;
+    }
+    queue->stage_n = 0;
+    return MAGMA_SUCCESS;
+}
+
+magma_int_t magma_b200_stage_times(magma_queue_t queue, float* ms, magma_int_t max) {
+    if (!queue) return -1;
+    if (!queue->stage_on || queue->stage_n < 2) return 0;
+    const int k = std::min<int>(max, queue->stage_n - 1);
+    cudaEventSynchronize(queue->stage_ev[queue->stage_n - 1]);
+    for (int i = 0; i < k; ++i) cudaEventElapsedTime(&ms[i], queue->stage_ev[i], queue->stage_ev[i + 1]);
+    return k;
+}
+
+}  // extern "C"
