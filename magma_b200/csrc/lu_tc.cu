@@ -35,9 +35,14 @@ constexpr int kTcNT = 256;        // threads = matrix rows (n <= 256)
 constexpr int kTcTrail = 224;     // trailing columns of the first panel at n = 256
 
 struct TcLuSmem {
-    float A[2][2][128 * 32];        // L21 operand: [row half][hi, lo], K-major canonical (16 KB each)
+    // The L21 operand is built after the pivot rows' entries (Ug) have been solved and
+    // copied into the B operand, and the MMA that reads it completes before the next
+    // panel gathers into Ug, so the two share storage.
+    union {
+        float A[2][2][128 * 32];    // L21 operand: [row half][hi, lo], K-major canonical (16 KB each)
+        float Ug[32][kTcTrail + 1]; // pivot rows' trailing entries; U12 after the solve
+    };
     float B[2][kTcTrail * 32];      // U12 operand: [hi, lo], K-major canonical (28 KB each)
-    float Ug[32][kTcTrail + 1];     // pivot rows' trailing entries; U12 after the solve
     float L11[32][33];
     SmallLuShared<float, 32, 8> lu;
     double red[kTcNT / 32];
@@ -194,6 +199,7 @@ lu_tf32x3_kernel(TcLuArgs g) {
                 sh.B[0][f] = hi;
                 sh.B[1][f] = lo;
             }
+            __syncthreads();   // Ug fully read before the A operand overwrites it
             // A operand: this row's multipliers (zero for rows already placed)
             {
                 const bool live = (t < n) && pos >= k0 + 32;
@@ -262,6 +268,8 @@ lu_tf32x3_kernel(TcLuArgs g) {
 bool lu_tc_supported(int n) { return n >= 32 && n <= 256 && n % 32 == 0; }
 
 size_t lu_tc_smem_bytes() { return sizeof(TcLuSmem) + 1024; }
+// Two blocks of this kernel must never share an SM: each allocates all 512 TMEM columns.
+static_assert(2 * (sizeof(TcLuSmem) + 1024) > 228 * 1024, "one tensor-core LU block per SM");
 
 magma_int_t lu_tc_launch(const TcLuArgs& args, cudaStream_t s) {
     const int smem = (int)lu_tc_smem_bytes();
