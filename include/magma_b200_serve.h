@@ -5,7 +5,9 @@
  * accepts solve requests of any size n <= 1024 and RHS count as they arrive
  * and runs them with continuous batching: whatever has been admitted while
  * earlier work was on the GPU goes out as the next micro-batch, on one of
- * several CUDA streams, so batches overlap on the device. Admission is by a
+ * several CUDA streams, so batches overlap on the device. With two or more
+ * streams, requests of order n <= 128 and larger ones form separate batches on
+ * separate streams, so small solves do not wait for large ones. Admission is by a
  * device-memory budget: a request waits (FIFO) until its matrix, right-hand
  * sides and pivots fit in the server's arena, and its memory is released when
  * its result has been copied back. Results are bit-identical to solving the

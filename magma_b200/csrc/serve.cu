@@ -1,17 +1,21 @@
 // serve.cu -- continuous-batching request loop for batched LU / Cholesky solves
 // (include/magma_b200_serve.h). No counterpart in the reference.
 //
-// Three parties share the server state under one mutex:
-//   callers     submit requests into a FIFO (`pending`);
-//   dispatcher  admits requests from the head of the FIFO while their device memory
-//               (A, B, ipiv) fits in the arena (first-fit free list), takes everything
-//               admitted as one micro-batch, and launches it on a free stream slot:
-//               host->device copies, one metadata upload, one variable-size LU call
-//               (magma_dgesv_vbatched_max_nocheck) and one variable-size Cholesky call
-//               (magma_dposv_vbatched_max_nocheck), result copies back, an event;
-//   completer   waits for the oldest in-flight batch's event, publishes its results,
-//               frees their arena memory and the slot, and wakes the dispatcher.
-// With several slots, a batch's copies and kernels overlap the previous batch's.
+// Requests are split into two size classes (n <= 128 and larger) so that small
+// solves never wait behind the single-block factorisations of the largest ones;
+// each class has its own FIFO, stream slots and completion thread. The parties
+// share the server state under one mutex:
+//   callers     submit requests into their class's FIFO (`pending`);
+//   dispatcher  admits requests from the head of a FIFO while their device memory
+//               (A, B, ipiv) fits in the arena (first-fit free list, shared by both
+//               classes), takes everything admitted as one micro-batch, and launches
+//               it on a free stream slot of that class: host->device copies, one
+//               metadata upload, one variable-size LU call (magma_dgesv_vbatched_max_nocheck)
+//               and one variable-size Cholesky call (magma_dposv_vbatched_max_nocheck),
+//               result copies back, an event;
+//   completers  (one per class) wait for their class's oldest in-flight batch, publish
+//               its results, free their arena memory and the slot, and wake the dispatcher.
+// With several slots per class, a batch's copies and kernels overlap the previous one's.
 #include "internal.h"
 #include "vbatched.h"
 #include "../../include/magma_b200_serve.h"
@@ -110,7 +114,11 @@ struct Slot {
     char* d_meta = nullptr;
     std::vector<Request*> reqs;
     bool busy = false;
+    int cls = 0;              // size class this slot serves
 };
+
+constexpr int kClasses = 2;
+constexpr int kSmallN = 128;   // class 0: n <= kSmallN
 
 }  // namespace
 
@@ -123,15 +131,16 @@ struct magma_b200_server {
     MetaLayout meta{1};
     std::mutex mu;
     std::condition_variable cv_dispatch, cv_complete, cv_drain;
-    std::deque<Request*> pending;
-    std::deque<Slot*> inflight;
+    std::deque<Request*> pending[kClasses];
+    std::deque<Slot*> inflight[kClasses];
+    int nclasses = 1;
     std::vector<Request*> finished;
     long long submitted = 0, completed = 0, batches = 0;
     bool stop = false;
-    std::thread dispatcher, completer;
+    std::thread dispatcher, completer[kClasses];
 
     void dispatch_loop();
-    void complete_loop();
+    void complete_loop(int cls);
     void launch(Slot& s);
 };
 
@@ -197,24 +206,37 @@ void magma_b200_server::dispatch_loop() {
     std::unique_lock<std::mutex> lk(mu);
     for (;;) {
         Slot* free_slot = nullptr;
+        int cls = 0;
         cv_dispatch.wait(lk, [&] {
             if (stop) return true;
+            // the class whose head request is oldest among those that can go now
+            long long best = 0;
             free_slot = nullptr;
-            for (Slot& s : slots)
-                if (!s.busy) { free_slot = &s; break; }
-            if (!free_slot || pending.empty()) return false;
-            size_t off;   // can the head be admitted now?
-            if (!arena.alloc(pending.front()->bytes, &off)) return false;
-            arena.release(off, pending.front()->bytes);
-            return true;
+            for (int c = 0; c < nclasses; ++c) {
+                if (pending[c].empty()) continue;
+                Slot* fs = nullptr;
+                for (Slot& sl : slots)
+                    if (!sl.busy && sl.cls == c) { fs = &sl; break; }
+                if (!fs) continue;
+                size_t off;   // can the head be admitted now?
+                if (!arena.alloc(pending[c].front()->bytes, &off)) continue;
+                arena.release(off, pending[c].front()->bytes);
+                if (!free_slot || pending[c].front()->t_submit < best) {
+                    free_slot = fs;
+                    cls = c;
+                    best = pending[c].front()->t_submit;
+                }
+            }
+            return free_slot != nullptr;
         });
         if (stop) return;
         Slot& s = *free_slot;
         s.reqs.clear();
-        while (!pending.empty() && (int)s.reqs.size() < max_batch) {
-            Request* r = pending.front();
+        std::deque<Request*>& q = pending[cls];
+        while (!q.empty() && (int)s.reqs.size() < max_batch) {
+            Request* r = q.front();
             if (!arena.alloc(r->bytes, &r->off)) break;   // FIFO admission by memory budget
-            pending.pop_front();
+            q.pop_front();
             s.reqs.push_back(r);
         }
         s.busy = true;
@@ -222,23 +244,23 @@ void magma_b200_server::dispatch_loop() {
         lk.unlock();
         launch(s);
         lk.lock();
-        inflight.push_back(&s);
-        cv_complete.notify_one();
+        inflight[cls].push_back(&s);
+        cv_complete.notify_all();
     }
 }
 
-void magma_b200_server::complete_loop() {
+void magma_b200_server::complete_loop(int cls) {
     cudaSetDevice(device);
     std::unique_lock<std::mutex> lk(mu);
     for (;;) {
-        cv_complete.wait(lk, [&] { return stop || !inflight.empty(); });
-        if (inflight.empty() && stop) return;
-        Slot* s = inflight.front();
+        cv_complete.wait(lk, [&] { return stop || !inflight[cls].empty(); });
+        if (inflight[cls].empty() && stop) return;
+        Slot* s = inflight[cls].front();
         lk.unlock();
         cudaEventSynchronize(s->done);
         const long long t = now_ns();
         lk.lock();
-        inflight.pop_front();
+        inflight[cls].pop_front();
         int idx[2] = {0, 0};
         for (Request* r : s->reqs) {
             const int* info = reinterpret_cast<const int*>(s->h_meta + r->kind * meta.bytes + meta.info);
@@ -250,7 +272,7 @@ void magma_b200_server::complete_loop() {
         }
         s->reqs.clear();
         s->busy = false;
-        cv_dispatch.notify_one();
+        cv_dispatch.notify_all();
         cv_drain.notify_all();
     }
 }
@@ -288,8 +310,11 @@ magma_int_t magma_b200_server_create(magma_int_t device, size_t budget_bytes, ma
             return MAGMA_ERR_DEVICE_ALLOC;
         }
     }
+    // two size classes when there are at least two stream slots (slots alternate classes)
+    sv->nclasses = streams >= 2 ? kClasses : 1;
+    for (int i = 0; i < (int)sv->slots.size(); ++i) sv->slots[i].cls = i % sv->nclasses;
     sv->dispatcher = std::thread([sv] { sv->dispatch_loop(); });
-    sv->completer = std::thread([sv] { sv->complete_loop(); });
+    for (int c = 0; c < sv->nclasses; ++c) sv->completer[c] = std::thread([sv, c] { sv->complete_loop(c); });
     *out = sv;
     return MAGMA_SUCCESS;
 }
@@ -316,7 +341,7 @@ magma_int_t magma_b200_server_submit(magma_b200_server_t sv, magma_int_t kind, m
     {
         std::lock_guard<std::mutex> lk(sv->mu);
         r->t_submit = now_ns();
-        sv->pending.push_back(r);
+        sv->pending[(sv->nclasses > 1 && n > kSmallN) ? 1 : 0].push_back(r);
         ++sv->submitted;
     }
     sv->cv_dispatch.notify_one();
@@ -364,7 +389,8 @@ magma_int_t magma_b200_server_destroy(magma_b200_server_t sv) {
     sv->cv_dispatch.notify_all();
     sv->cv_complete.notify_all();
     if (sv->dispatcher.joinable()) sv->dispatcher.join();
-    if (sv->completer.joinable()) sv->completer.join();
+    for (auto& c : sv->completer)
+        if (c.joinable()) c.join();
     for (Slot& s : sv->slots) {
         if (s.queue) magma_queue_destroy_internal(s.queue, "server", __FILE__, __LINE__);
         if (s.stream) cudaStreamDestroy(s.stream);
