@@ -498,7 +498,7 @@ class C2GemmVbatched:
 
     def dominant_kernel(self, q, stream, reps=20):
         ms = timed_restore(stream, lambda i: self.step(q, i), self.restore, reps) / reps
-        return {"kernel": "gemm_vbatched_kernel<double> (magmablas_dgemm_vbatched_max_nocheck)", "ms": ms,
+        return {"kernel": "gemm_tile_kernel<double> (magmablas_dgemm_vbatched_max_nocheck, all buckets)", "ms": ms,
                 "alg_bytes": self.bytes64, "tflops": self.flops / ms / 1e9}
 
     def e2e_setup(self):

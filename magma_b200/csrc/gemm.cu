@@ -34,20 +34,21 @@ struct GemmSizes {
 };
 
 // One tile shape of the kernel: BM x BN tile of C, TM x TN outputs per thread.
-template <int BM_, int BN_, int TM_, int TN_>
+template <int BM_, int BN_, int TM_, int TN_, int MINB_D_, int MINB_F_>
 struct GemmTile {
-    static constexpr int BM = BM_, BN = BN_, BK = 16, TM = TM_, TN = TN_;
+    // MINB_D / MINB_F: resident blocks per SM the FP64 / FP32 register allocations are sized for
+    static constexpr int BM = BM_, BN = BN_, BK = 16, TM = TM_, TN = TN_, MINB_D = MINB_D_, MINB_F = MINB_F_;
     static constexpr int NT = (BM / TM) * (BN / TN);
     static constexpr int EA = BM * BK / NT, EB = BK * BN / NT;   // staged elements per thread
 };
 // The variants the tuning table chooses between (index = variant id).
-using GemmTile0 = GemmTile<64, 64, 4, 4>;   // 256 threads
-using GemmTile1 = GemmTile<32, 32, 4, 4>;   // 64 threads
-using GemmTile2 = GemmTile<16, 16, 2, 2>;   // 64 threads
+using GemmTile0 = GemmTile<64, 64, 4, 4, 2, 3>;     // 256 threads
+using GemmTile1 = GemmTile<32, 32, 4, 4, 10, 16>;   // 64 threads
+using GemmTile2 = GemmTile<16, 16, 2, 2, 16, 16>;   // 64 threads
 constexpr int kGemmVariants = 3;
 
 template <typename T, bool TA, bool TB, typename S>
-__global__ void __launch_bounds__(S::NT)
+__global__ void __launch_bounds__(S::NT, (sizeof(T) == 8 ? S::MINB_D : S::MINB_F))
 gemm_tile_kernel(GemmSizes g, T alpha, const T* const* __restrict__ A_arr, const T* const* __restrict__ B_arr, T beta,
                  T** __restrict__ C_arr, int tiles_m, int tiles_n, WorkList wl) {
     constexpr int BM = S::BM, BN = S::BN, BK = S::BK, TM = S::TM, TN = S::TN, NT = S::NT;

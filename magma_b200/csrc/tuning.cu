@@ -24,7 +24,7 @@ static std::once_flag g_once;
 
 // Built-in defaults: the table magma_b200_autotune measured on a B200.
 static void set_defaults(TuningTable& t) {
-    const int gemm[2][kGemmBuckets] = {{2, 1, 1, 1}, {2, 1, 0, 0}};
+    const int gemm[2][kGemmBuckets] = {{2, 1, 1, 1}, {2, 1, 1, 1}};
     for (int p = 0; p < 2; ++p)
         for (int b = 0; b < kGemmBuckets; ++b) t.gemm_variant[p][b] = gemm[p][b];
     const char* e = std::getenv("MAGMA_B200_TENSOR_CORE_LU");
