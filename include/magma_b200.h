@@ -190,6 +190,29 @@ magma_int_t magma_sgesv_batched(magma_int_t n, magma_int_t nrhs, float** dA_arra
                                 magma_int_t** dipiv_array, float** dB_array, magma_int_t lddb,
                                 magma_int_t* dinfo_array, magma_int_t batchCount, magma_queue_t queue);
 
+/* LU without pivoting and its solves: src/zgetrf_nopiv_batched.cpp:76-94 (m -1, n -2,
+ * ldda -4), src/zgetrs_nopiv_batched.cpp:89-113 (trans -1, n -2, nrhs -3, ldda -5,
+ * lddb -8; info_array set to 0), src/zgesv_nopiv_batched.cpp:87-104 (n -1, nrhs -2,
+ * ldda -4, lddb -6). info_array: first zero pivot (1-based); a zero pivot is not
+ * divided by. Same kernels (and sizes) as the pivoted forms. */
+magma_int_t magma_dgetrf_nopiv_batched(magma_int_t m, magma_int_t n, double** dA_array, magma_int_t ldda,
+                                       magma_int_t* info_array, magma_int_t batchCount, magma_queue_t queue);
+magma_int_t magma_dgetrs_nopiv_batched(magma_trans_t trans, magma_int_t n, magma_int_t nrhs, double** dA_array,
+                                       magma_int_t ldda, double** dB_array, magma_int_t lddb,
+                                       magma_int_t* info_array, magma_int_t batchCount, magma_queue_t queue);
+magma_int_t magma_dgesv_nopiv_batched(magma_int_t n, magma_int_t nrhs, double** dA_array, magma_int_t ldda,
+                                      double** dB_array, magma_int_t lddb, magma_int_t* info_array,
+                                      magma_int_t batchCount, magma_queue_t queue);
+
+/* Inverse from the getrf factors into a separate array: dinvA_i = inv(A_i).
+ * src/zgetri_outofplace_batched.cpp:82-220; checks n -1, ldda -3, lddia -6.
+ * info_array (may be NULL): 1-based index of the first exactly-zero U(i,i), else 0.
+ * Each column of the result is bit-identical to getrs applied to the matching
+ * unit vector. n <= 1024. */
+magma_int_t magma_dgetri_outofplace_batched(magma_int_t n, double** dA_array, magma_int_t ldda,
+                                            magma_int_t** dipiv_array, double** dinvA_array, magma_int_t lddia,
+                                            magma_int_t* info_array, magma_int_t batchCount, magma_queue_t queue);
+
 /* Mixed precision: FP32 LU + FP64 iterative refinement with FP64 fallback.
  * No batched counterpart in MAGMA 2.2; per instance it is magma_dsgesv_gpu
  * (src/zcgesv_gpu.cpp:144-365): stopping test max|R_j| <= max|X_j| ||A||_inf

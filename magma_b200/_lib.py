@@ -68,6 +68,10 @@ SIGNATURES: dict[str, tuple] = {
     "magma_dgetrs_vbatched_max_nocheck": (_i, [_i, _p, _p, _p, _p, _p, _p, _p, _i, _i, _i, _p]),
     "magma_dgesv_vbatched": (_i, [_p, _p, _p, _p, _p, _p, _p, _p, _i, _p]),
     "magma_dgesv_vbatched_max_nocheck": (_i, [_p, _p, _p, _p, _p, _p, _p, _p, _i, _i, _i, _p]),
+    "magma_dgetri_outofplace_batched": (_i, [_i, _p, _i, _p, _p, _i, _p, _i, _p]),
+    "magma_dgetrf_nopiv_batched": (_i, [_i, _i, _p, _i, _p, _i, _p]),
+    "magma_dgetrs_nopiv_batched": (_i, [_i, _i, _i, _p, _i, _p, _i, _p, _i, _p]),
+    "magma_dgesv_nopiv_batched": (_i, [_i, _i, _p, _i, _p, _i, _p, _i, _p]),
     "magma_sgetrf_batched": (_i, [_i, _i, _p, _i, _p, _p, _i, _p]),
     "magma_sgetrs_batched": (_i, [_i, _i, _i, _p, _i, _p, _p, _i, _i, _p]),
     "magma_sgesv_batched": (_i, [_i, _i, _p, _i, _p, _p, _i, _p, _i, _p]),

@@ -379,3 +379,47 @@ def dsposv_vbatched(A: "VarBatch", B: "VarBatch", n, nrhs, lda=None, ldb=None, m
     q.sync()
     del S
     return X, it[:batch], info[:batch]
+
+
+def dgetri_outofplace_batched(LU: torch.Tensor, ipiv: torch.Tensor, queue: Queue | None = None):
+    """inv(A_i) from getrf factors (column-major batch (batch, n, ld)). Returns (invA, info)."""
+    q = queue or default_queue()
+    batch, n, lda = LU.shape
+    inv = torch.empty((batch, n, n), dtype=torch.float64, device=LU.device)
+    info = torch.empty(batch, dtype=torch.int32, device=LU.device)
+    pA, pP, pI = ptr_array(LU), ptr_array(ipiv), ptr_array(inv)
+    _check(q.lib.magma_dgetri_outofplace_batched(n, _vp(pA), lda, _vp(pP), _vp(pI), n, _vp(info), batch, q.handle),
+           "magma_dgetri_outofplace_batched")
+    return inv, info
+
+
+def dgetrf_nopiv_batched(A: torch.Tensor, m: int | None = None, queue: Queue | None = None) -> torch.Tensor:
+    """LU without pivoting of each instance of A (batch, n, lda), in place. Returns info."""
+    q = queue or default_queue()
+    batch, n, lda = A.shape
+    m = lda if m is None else m
+    info = torch.empty(batch, dtype=torch.int32, device=A.device)
+    pA = ptr_array(A)
+    _check(q.lib.magma_dgetrf_nopiv_batched(m, n, _vp(pA), lda, _vp(info), batch, q.handle),
+           "magma_dgetrf_nopiv_batched")
+    return info
+
+
+def dgetrs_nopiv_batched(A: torch.Tensor, B: torch.Tensor, trans: bool = False, queue: Queue | None = None) -> None:
+    q = queue or default_queue()
+    batch, n, lda = A.shape
+    _, nrhs, ldb = B.shape
+    pA, pB = ptr_array(A), ptr_array(B)
+    _check(q.lib.magma_dgetrs_nopiv_batched(_trans(trans), n, nrhs, _vp(pA), lda, _vp(pB), ldb, None, batch,
+                                            q.handle), "magma_dgetrs_nopiv_batched")
+
+
+def dgesv_nopiv_batched(A: torch.Tensor, B: torch.Tensor, queue: Queue | None = None) -> torch.Tensor:
+    q = queue or default_queue()
+    batch, n, lda = A.shape
+    _, nrhs, ldb = B.shape
+    info = torch.empty(batch, dtype=torch.int32, device=A.device)
+    pA, pB = ptr_array(A), ptr_array(B)
+    _check(q.lib.magma_dgesv_nopiv_batched(n, nrhs, _vp(pA), lda, _vp(pB), ldb, _vp(info), batch, q.handle),
+           "magma_dgesv_nopiv_batched")
+    return info

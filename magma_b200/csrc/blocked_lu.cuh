@@ -85,8 +85,8 @@ __device__ void blocked_getrf(T* __restrict__ A, int m, int n, int lda, int* __r
         for (int c = 0; c < NB; ++c) a[c] = (live && c < nbp) ? A[tid + (size_t)(k0 + c) * lda] : T(0);
         int pos = (tid < m) ? tid : INT_MAX / 2;
         int my_ipiv = 0;
-        lu_panel_steps<T, NB, NW>(a, m, nbp, nbp, k0, tid, pos, my_ipiv, info, sh.lu);
-        if (tid >= k0 && tid < k0 + nbp) ipiv[tid] = my_ipiv;
+        lu_panel_steps<T, NB, NW>(a, m, nbp, nbp, k0, tid, pos, my_ipiv, info, sh.lu, ipiv == nullptr);
+        if (ipiv && tid >= k0 && tid < k0 + nbp) ipiv[tid] = my_ipiv;
         const bool pivot_row = live && pos < k0 + nbp;
         const bool displaced = live && pos != tid;
         // ---- 2. store the panel at the new positions; L11 and pivot sources to smem ----

@@ -24,7 +24,9 @@ getrf_blocked_kernel(WorkList wl, LuSizes sz, T** dA_array, int** ipiv_array, in
         const int id = wl.at(w);
         const int m = sz.get_m(id), n = sz.get_n(id), lda = sz.get_lda(id);
         int info = 0;
-        if (m > 0 && n > 0) blocked_getrf<T, NB, NT, CW, CB>(dA_array[id], m, n, lda, ipiv_array[id], info, sh);
+        if (m > 0 && n > 0)   // a null pivot array selects LU without pivoting (getrf_nopiv)
+            blocked_getrf<T, NB, NT, CW, CB>(dA_array[id], m, n, lda, ipiv_array ? ipiv_array[id] : nullptr, info,
+                                            sh);
         if (threadIdx.x == 0) info_array[id] = info;
         __syncthreads();
     }
@@ -38,7 +40,8 @@ getrs_blocked_kernel(WorkList wl, LuSizes sz, bool trans, T** dA_array, int** ip
         const int id = wl.at(w);
         const int n = sz.get_n(id), lda = sz.get_lda(id), ldb = sz.get_ldb(id), nrhs = sz.get_nrhs(id);
         if (n > 0 && nrhs > 0)
-            blocked_getrs<T, NT, R>(trans, dA_array[id], n, lda, ipiv_array[id], dB_array[id], nrhs, ldb, sh);
+            blocked_getrs<T, NT, R>(trans, dA_array[id], n, lda, ipiv_array ? ipiv_array[id] : nullptr,
+                                    dB_array[id], nrhs, ldb, sh);
         __syncthreads();
     }
 }

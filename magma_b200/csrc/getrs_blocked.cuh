@@ -72,7 +72,7 @@ template <typename T, int NT, int R>
 __device__ void blocked_getrs(bool trans, const T* __restrict__ A, int n, int lda, const int* __restrict__ ipiv,
                               T* __restrict__ B, int nrhs, int ldb, BlockedRsShared<T, NT, R>& sh) {
     const int t = threadIdx.x;
-    for (int k = t; k < n; k += NT) sh.ipiv[k] = ipiv[k];
+    for (int k = t; k < n; k += NT) sh.ipiv[k] = ipiv ? ipiv[k] : k + 1;   // no pivots: identity
     __syncthreads();
     const int fwd_idx = (t < n) ? laswp_target(sh.ipiv, n, t, false) : t;
     const int inv_idx = (t < n) ? laswp_target(sh.ipiv, n, t, true) : t;

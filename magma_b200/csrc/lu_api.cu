@@ -121,6 +121,31 @@ magma_int_t magma_dgesv_batched(magma_int_t n, magma_int_t nrhs, double** dA_arr
                              dipiv_array, dB_array, lddb, dinfo_array, batchCount, queue);
 }
 
+// LU without pivoting (src/zgetrf_nopiv_batched.cpp:76-94: m -1, n -2, ldda -4).
+// The same kernels as magma_dgetrf_batched with the pivot search replaced by the
+// diagonal; info_array = first zero pivot (1-based), which is then not divided by.
+magma_int_t magma_dgetrf_nopiv_batched(magma_int_t m, magma_int_t n, double** dA_array, magma_int_t ldda,
+                                       magma_int_t* info_array, magma_int_t batchCount, magma_queue_t queue) {
+    return getrf_impl<double>(__func__, m, n, dA_array, ldda, nullptr, info_array, batchCount, queue);
+}
+
+// src/zgetrs_nopiv_batched.cpp:89-113: trans -1, n -2, nrhs -3, ldda -5, lddb -8.
+// info_array is accepted for the reference's signature and set to 0.
+magma_int_t magma_dgetrs_nopiv_batched(magma_trans_t trans, magma_int_t n, magma_int_t nrhs, double** dA_array,
+                                       magma_int_t ldda, double** dB_array, magma_int_t lddb,
+                                       magma_int_t* info_array, magma_int_t batchCount, magma_queue_t queue) {
+    if (info_array && batchCount > 0) cudaMemsetAsync(info_array, 0, sizeof(magma_int_t) * batchCount, queue->stream);
+    return getrs_impl<double>(__func__, trans, n, nrhs, dA_array, ldda, nullptr, dB_array, lddb, batchCount, queue);
+}
+
+// src/zgesv_nopiv_batched.cpp:87-104: n -1, nrhs -2, ldda -4, lddb -6.
+magma_int_t magma_dgesv_nopiv_batched(magma_int_t n, magma_int_t nrhs, double** dA_array, magma_int_t ldda,
+                                      double** dB_array, magma_int_t lddb, magma_int_t* info_array,
+                                      magma_int_t batchCount, magma_queue_t queue) {
+    return gesv_impl<double>(__func__, "magma_dgetrf_nopiv_batched", "magma_dgetrs_nopiv_batched", n, nrhs, dA_array,
+                             ldda, nullptr, dB_array, lddb, info_array, batchCount, queue);
+}
+
 // Single precision: the s-variants MAGMA generates from the same z-templates
 // (src/zgetrf_batched.cpp:83, src/zgetrs_batched.cpp:87, src/zgesv_batched.cpp:93).
 magma_int_t magma_sgetrf_batched(magma_int_t m, magma_int_t n, float** dA_array, magma_int_t ldda,

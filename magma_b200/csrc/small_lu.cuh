@@ -144,10 +144,12 @@ struct SmallLuShared {
 // live rows, anything < k0 for finished rows, a huge value for tid >= m).
 // On return `pos` is the row's new position, the thread with tid == g holds
 // ipiv(g) (1-based) in `my_ipiv`, and `info` is g+1 of the first zero pivot.
+// With nopiv the row at position g is step g's pivot (getrf_nopiv): no search,
+// rows never change position.
 template <typename T, int NC, int NW>
 __device__ __forceinline__ void lu_panel_steps(T (&a)[NC], int m, int nsteps, int ncols, int k0, int tid, int& pos,
                                                int& my_ipiv, int& info,
-                                               SmallLuShared<T, NC, NW>& sh) {
+                                               SmallLuShared<T, NC, NW>& sh, bool nopiv = false) {
     (void)ncols;   // columns >= ncols hold zeros in every row, so their updates are no-ops
     const int lane = tid & 31;
     const int warp = tid >> 5;
@@ -158,10 +160,12 @@ __device__ __forceinline__ void lu_panel_steps(T (&a)[NC], int m, int nsteps, in
         constexpr int buf = k & 1;
         const int g = k0 + k;
         // ---- pivot search over rows still unchosen (pos >= g) ----
+        int p = g, s = g;
+        if (!nopiv) {
         const bool cand = (pos >= g && tid < m);
         PivotKey key = pivot_key(a[k], cand);
-        int p = cand ? pos : INT_MAX;
-        int s = warp_argmax(key, p, lane) + warp * 32;
+        p = cand ? pos : INT_MAX;
+        s = warp_argmax(key, p, lane) + warp * 32;
         if (NW > 1) {
             if (lane == 0) { sh.red_hi[buf][warp] = key.hi; sh.red_lo[buf][warp] = key.lo; sh.red_p[buf][warp] = p; sh.red_s[buf][warp] = s; }
             __syncthreads();
@@ -170,6 +174,7 @@ __device__ __forceinline__ void lu_panel_steps(T (&a)[NC], int m, int nsteps, in
             key = PivotKey{v ? sh.red_hi[buf][lane] : 0u, v ? sh.red_lo[buf][lane] : 0u};
             p = v ? sh.red_p[buf][lane] : INT_MAX;
             s = sh.red_s[buf][warp_argmax(key, p, lane)];
+        }
         }
         // ---- the pivot row publishes columns k..NC-1 (aligned pairs) ----
         constexpr int jw = k & ~1;
@@ -210,11 +215,11 @@ __device__ __forceinline__ void lu_panel_steps(T (&a)[NC], int m, int nsteps, in
 template <typename T, int NC, int NW>
 __device__ __forceinline__ void small_lu_factor(T (&a)[NC], int m, int n, int tid, int& pos,
                                                 int& my_ipiv, int& info,
-                                                SmallLuShared<T, NC, NW>& sh) {
+                                                SmallLuShared<T, NC, NW>& sh, bool nopiv = false) {
     pos = (tid < m) ? tid : INT_MAX / 2;
     info = 0;
     my_ipiv = 0;
-    lu_panel_steps<T, NC, NW>(a, m, min(m, n), n, 0, tid, pos, my_ipiv, info, sh);
+    lu_panel_steps<T, NC, NW>(a, m, min(m, n), n, 0, tid, pos, my_ipiv, info, sh, nopiv);
 }
 
 // Solve with the factors held in registers. Each thread holds its LU row at

@@ -55,9 +55,10 @@ getrf_small_kernel(WorkList wl, LuSizes sz, T** dA_array, int** ipiv_array, int*
         T a[NC];
         load_rows<T, NC, NW>(a, A, m, n, lda, tid);
         int pos, my_ipiv, info;
-        small_lu_factor<T, NC, NW>(a, m, n, tid, pos, my_ipiv, info, shm[local]);
+        // a null pivot array selects LU without pivoting (getrf_nopiv)
+        small_lu_factor<T, NC, NW>(a, m, n, tid, pos, my_ipiv, info, shm[local], ipiv_array == nullptr);
         store_rows<T, NC>(a, A, m, n, lda, tid, pos);
-        if (tid < min(m, n)) ipiv_array[id][tid] = my_ipiv;
+        if (ipiv_array && tid < min(m, n)) ipiv_array[id][tid] = my_ipiv;
         if (tid == 0) info_array[id] = info;
         mat_sync<NW>();
     }
@@ -84,9 +85,9 @@ gesv_small_kernel(WorkList wl, LuSizes sz, T** dA_array, int** ipiv_array, T** d
     T a[NC];
     load_rows<T, NC, NW>(a, A, n, n, lda, tid);
     int pos, my_ipiv, info;
-    small_lu_factor<T, NC, NW>(a, n, n, tid, pos, my_ipiv, info, shm[local]);
+    small_lu_factor<T, NC, NW>(a, n, n, tid, pos, my_ipiv, info, shm[local], ipiv_array == nullptr);
     store_rows<T, NC>(a, A, n, n, lda, tid, pos);
-    if (tid < n) ipiv_array[id][tid] = my_ipiv;
+    if (ipiv_array && tid < n) ipiv_array[id][tid] = my_ipiv;
     if (tid == 0) info_array[id] = info;
     // Thread tid's b entry (original row tid) belongs at position `pos` of P*b,
     // the same position its LU row landed at, so no permutation pass is needed.
@@ -115,7 +116,8 @@ template <typename T, int NC, int NW, int R>
 __device__ __forceinline__ void permute_rhs(T (&b)[R], const int* ipiv, int n, int tid,
                                             SmallLuShared<T, NC, NW>& sh, T* xch, bool inverse) {
     // idx = where the entry of original row tid sits after LAPACK's DLASWP
-    // (forward: k ascending; inverse: k descending).
+    // (forward: k ascending; inverse: k descending). No pivots: nothing moves.
+    if (!ipiv) return;
     int idx = tid;
     if (!inverse) {
         for (int k = 0; k < n; ++k) {
@@ -151,7 +153,7 @@ getrs_small_kernel(WorkList wl, LuSizes sz, T** dA_array, int** ipiv_array, T** 
     if (n <= 0 || nrhs <= 0) continue;
     const T* A = dA_array[id];
     T* B = dB_array[id];
-    const int* ipiv = ipiv_array[id];
+    const int* ipiv = ipiv_array ? ipiv_array[id] : nullptr;   // null: factors without pivoting
     T a[NC];
     load_rows<T, NC, NW>(a, A, n, n, lda, tid);
     SmallLuShared<T, NC, NW>& sh = shm[local];

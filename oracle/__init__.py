@@ -105,6 +105,16 @@ def dgetrf_batched(A: np.ndarray, m: int):
     return ipiv, info
 
 
+def dgetrf_nopiv_batched(A: np.ndarray, m: int):
+    """In-place LU without pivoting. Returns (ipiv = identity sequence, info)."""
+    batch, n, lda = A.shape
+    ipiv = np.zeros((batch, max(1, min(m, n))), np.int32)
+    info = np.zeros(batch, np.int32)
+    lib().oracle_dgetrf_nopiv_batched(m, n, _d(A), lda, C.c_long(n * lda), _i(ipiv), C.c_long(ipiv.shape[1]),
+                                      _i(info), batch)
+    return ipiv, info
+
+
 def dgetrs_batched(A: np.ndarray, ipiv: np.ndarray, B: np.ndarray, trans: bool = False):
     """Solve with the factors; B is (batch, nrhs, ldb), overwritten with X."""
     batch, n, lda = A.shape

@@ -40,15 +40,16 @@ static double pivot_key(double x) {
     return (v != v) ? -0.5 : v;
 }
 
-/* LAPACK 3.x dgetf2: unblocked right-looking LU with partial pivoting.
+/* LAPACK 3.x dgetf2: unblocked right-looking LU with partial pivoting
+ * (pivot = 0: no search, the diagonal is the pivot).
  * ipiv is 1-based; info = first zero pivot (1-based) or 0. */
-void oracle_dgetf2(int m, int n, double* a, int lda, int* ipiv, int* info) {
+static void getf2(int m, int n, double* a, int lda, int* ipiv, int* info, int pivot) {
     *info = 0;
     const int kmax = m < n ? m : n;
     for (int j = 0; j < kmax; ++j) {
         int jp = j;
         double best = pivot_key(A_(j, j));
-        for (int i = j + 1; i < m; ++i) {
+        for (int i = j + 1; pivot && i < m; ++i) {
             double v = pivot_key(A_(i, j));
             if (v > best) { best = v; jp = i; }
         }
@@ -74,6 +75,21 @@ void oracle_dgetf2(int m, int n, double* a, int lda, int* ipiv, int* info) {
             }
         }
     }
+}
+
+void oracle_dgetf2(int m, int n, double* a, int lda, int* ipiv, int* info) { getf2(m, n, a, lda, ipiv, info, 1); }
+
+/* The same elimination without pivoting (MAGMA's getrf_nopiv): step j's pivot is
+ * the diagonal entry; ipiv is filled with the identity sequence. */
+void oracle_dgetf2_nopiv(int m, int n, double* a, int lda, int* ipiv, int* info) {
+    getf2(m, n, a, lda, ipiv, info, 0);
+}
+
+void oracle_dgetrf_nopiv_batched(int m, int n, double* A, int lda, long strideA, int* ipiv, long strideP,
+                                 int* info, int batch) {
+#pragma omp parallel for schedule(dynamic)
+    for (int i = 0; i < batch; ++i)
+        oracle_dgetf2_nopiv(m, n, A + (size_t)i * strideA, lda, ipiv + (size_t)i * strideP, info + i);
 }
 
 /* LAPACK dlaswp on the rows of B: forward (k ascending) or inverse. */

@@ -1,0 +1,94 @@
+"""GPU tests of the batched out-of-place inverse (magma_dgetri_outofplace_batched).
+
+Each column of inv(A) is getrs applied to a unit vector, so the result is
+BIT-IDENTICAL to the oracle's dgetrs with B = I; A inv(A) = I to rounding; info
+reports the first exactly-zero U(i,i)."""
+import numpy as np
+import pytest
+
+import oracle
+from magma_b200 import testing as T
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(a, cuda):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).to(cuda)
+
+
+@pytest.mark.parametrize("n,batch", [(1, 5), (8, 40), (32, 40), (63, 20), (100, 12), (256, 6), (520, 2)])
+def test_getri_bit_identical(cuda, n, batch):
+    import magma_b200 as mb
+    A_np, _ = T.lu_uniform(batch, n, 1, seed=300 + n)
+    A = dev(A_np, cuda)
+    ipiv, info = mb.dgetrf_batched(A)
+    inv, iinfo = mb.dgetri_outofplace_batched(A, ipiv)
+    inv = inv.cpu().numpy()
+    LU, ip = A.cpu().numpy(), ipiv.cpu().numpy()
+    eye = np.tile(np.eye(n)[None], (batch, 1, 1))
+    O = eye.copy()
+    oracle.dgetrs_batched(LU.copy(), ip, O, trans=False)
+    assert np.array_equal(inv, O)
+    assert np.all(iinfo.cpu().numpy() == 0)
+    for b in range(batch):
+        Ar = A_np[b].T                      # row-major A
+        X = inv[b].T
+        assert np.abs(Ar @ X - np.eye(n)).max() <= 1e-9 * max(1.0, np.abs(X).max()) * n
+
+
+def test_getri_reports_zero_pivot(cuda):
+    import magma_b200 as mb
+    n = 40
+    A_np, _ = T.lu_uniform(3, n, 1, seed=9)
+    A_np[1, 7, :] = 0.0                      # zero column 7 -> U(8,8) = 0
+    A = dev(A_np, cuda)
+    ipiv, info = mb.dgetrf_batched(A)
+    _, iinfo = mb.dgetri_outofplace_batched(A, ipiv)
+    assert list(iinfo.cpu().numpy()) == [0, int(info[1]), 0]
+    assert int(info[1]) == 8
+
+
+# ------------------------------------------------------------------ LU without pivoting
+@pytest.mark.parametrize("n,nrhs,batch", [(1, 1, 5), (16, 2, 40), (32, 1, 40), (50, 3, 30), (64, 4, 20),
+                                          (100, 2, 10), (256, 4, 6), (600, 1, 2)])
+def test_gesv_nopiv_bit_identical(cuda, n, nrhs, batch):
+    """Factors, info and solutions bit-identical to the oracle's dgetf2 without pivoting
+    (diagonally dominant inputs keep the pivots away from zero)."""
+    import magma_b200 as mb
+    A_np, B_np = T.lu_uniform(batch, n, nrhs, seed=700 + n)
+    for i in range(n):
+        A_np[:, i, i] += n                    # column-major: entry (i, i)
+    A, B = dev(A_np, cuda), dev(B_np, cuda)
+    info = mb.dgesv_nopiv_batched(A, B)
+    O = A_np.copy()
+    oip, oinf = oracle.dgetrf_nopiv_batched(O, n)
+    OB = B_np.copy()
+    oracle.dgetrs_batched(O.copy(), oip, OB, trans=False)
+    assert np.array_equal(info.cpu().numpy(), oinf)
+    assert np.array_equal(A.cpu().numpy(), O)
+    assert np.array_equal(B.cpu().numpy(), OB)
+    assert T.backward_error(A_np, OB, B_np, n).max() < 30 * np.finfo(float).eps
+
+
+@pytest.mark.parametrize("n", [24, 130])
+def test_getrf_nopiv_zero_pivot_and_trans_solve(cuda, n):
+    import magma_b200 as mb
+    A_np, B_np = T.lu_uniform(3, n, 2, seed=41 + n)
+    for i in range(n):
+        A_np[:, i, i] += n
+    A_np[1, 4, :] = 0.0                        # zero column 4: the step-5 pivot of instance 1 is exactly 0
+    A = dev(A_np, cuda)
+    info = mb.dgetrf_nopiv_batched(A)
+    O = A_np.copy()
+    oip, oinf = oracle.dgetrf_nopiv_batched(O, n)
+    assert np.array_equal(info.cpu().numpy(), oinf) and oinf[1] == 5
+    assert np.array_equal(np.nan_to_num(A.cpu().numpy()), np.nan_to_num(O))
+    for trans in (False, True):
+        Bd = dev(B_np[[0, 2]], cuda)
+        mb.dgetrs_nopiv_batched(dev(O[[0, 2]], cuda), Bd, trans=trans)
+        OB = B_np[[0, 2]].copy()
+        oracle.dgetrs_batched(O[[0, 2]].copy(), oip[[0, 2]], OB, trans=trans)
+        if not trans:
+            assert np.array_equal(Bd.cpu().numpy(), OB)
+        assert np.abs(Bd.cpu().numpy() - OB).max() <= 64 * n * np.finfo(float).eps * max(1.0, np.abs(OB).max())
