@@ -90,3 +90,25 @@ def test_dsgesv_tensor_core_lu(cuda, n):
     oip, _ = oracle.dgetrf_batched(O, n)
     same = [np.array_equal(ipiv[i], oip[i]) for i in range(batch) if it[i] >= 0]
     assert np.mean(same) >= 0.8, np.mean(same)
+
+
+def test_dsgesv_tensor_core_lu_fallbacks(cuda):
+    """The tensor-core path (n = 128) hands overflowing, NaN and singular instances to the
+    FP64 fallback exactly as the CUDA-core path does."""
+    import magma_b200 as mb
+    n = 128
+    A_np, B_np = T.lu_uniform(5, n, 3, seed=23)
+    A_np[1, 3, 5] = 1e39                        # overflows single precision -> iter -2
+    A_np[2, 7, 9] = np.nan                      # NaN -> iter -2, FP64 getrf carries the NaN
+    A_np[3, 10, :] = 0.0                        # zero column 10 -> singular in both precisions
+    A = dev(A_np, cuda)
+    X, ipiv, it, info = mb.dsgesv_batched(A, dev(B_np, cuda))
+    it, info = it.cpu().numpy(), info.cpu().numpy()
+    assert it[0] >= 0 and it[4] >= 0
+    assert it[1] == -2 and it[2] == -2 and it[3] == -3
+    O = A_np[[1, 3]].copy()
+    oip, oinf = oracle.dgetrf_batched(O, n)
+    assert np.array_equal(A.cpu().numpy()[[1, 3]], O)
+    assert list(info[[1, 3]]) == list(oinf) and oinf[1] == 11
+    be = T.backward_error(A_np[[0, 1, 4]], X.cpu().numpy()[[0, 1, 4]], B_np[[0, 1, 4]], n)
+    assert be.max() <= 1e-14
