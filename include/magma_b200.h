@@ -204,6 +204,20 @@ magma_int_t magma_dgesv_nopiv_batched(magma_int_t n, magma_int_t nrhs, double** 
                                       double** dB_array, magma_int_t lddb, magma_int_t* info_array,
                                       magma_int_t batchCount, magma_queue_t queue);
 
+/* Random butterfly transformation (src/zgerbt_batched.cpp:118-190; checks gen -1,
+ * n -2, nrhs -3, ldda -5, lddb -7, also stored in *info): A_i <- U^T A_i V,
+ * B_i <- U^T B_i with the depth-2 butterflies built from the HOST vectors U and V
+ * (2n entries each; filled from a fixed-seed generator when gen is MagmaTrue).
+ * magma_dgesv_rbt_batched (src/zgesv_rbt_batched.cpp:81-170; n -1, nrhs -2,
+ * ldda -4, lddb -6): transform, LU without pivoting, solve, x = V y.
+ * n must be a multiple of 4 (MAGMA_ERR_NOT_SUPPORTED otherwise), n <= 1024. */
+magma_int_t magma_dgerbt_batched(magma_bool_t gen, magma_int_t n, magma_int_t nrhs, double** dA_array,
+                                 magma_int_t ldda, double** dB_array, magma_int_t lddb, double* U, double* V,
+                                 magma_int_t* info, magma_int_t batchCount, magma_queue_t queue);
+magma_int_t magma_dgesv_rbt_batched(magma_int_t n, magma_int_t nrhs, double** dA_array, magma_int_t ldda,
+                                    double** dB_array, magma_int_t lddb, magma_int_t* dinfo_array,
+                                    magma_int_t batchCount, magma_queue_t queue);
+
 /* Inverse from the getrf factors into a separate array: dinvA_i = inv(A_i).
  * src/zgetri_outofplace_batched.cpp:82-220; checks n -1, ldda -3, lddia -6.
  * info_array (may be NULL): 1-based index of the first exactly-zero U(i,i), else 0.

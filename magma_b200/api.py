@@ -423,3 +423,33 @@ def dgesv_nopiv_batched(A: torch.Tensor, B: torch.Tensor, queue: Queue | None = 
     _check(q.lib.magma_dgesv_nopiv_batched(n, nrhs, _vp(pA), lda, _vp(pB), ldb, _vp(info), batch, q.handle),
            "magma_dgesv_nopiv_batched")
     return info
+
+
+def dgerbt_batched(A: torch.Tensor, B: torch.Tensor, U=None, V=None, queue: Queue | None = None):
+    """A_i <- U^T A_i V, B_i <- U^T B_i (in place). Without U, V a butterfly is generated;
+    returns the (U, V) numpy vectors used (2n entries each)."""
+    import numpy as np
+
+    q = queue or default_queue()
+    batch, n, lda = A.shape
+    _, nrhs, ldb = B.shape
+    gen = U is None
+    hu = np.zeros(2 * n) if gen else np.ascontiguousarray(U, dtype=np.float64).copy()
+    hv = np.zeros(2 * n) if gen else np.ascontiguousarray(V, dtype=np.float64).copy()
+    info = C.c_int(0)
+    pA, pB = ptr_array(A), ptr_array(B)
+    _check(q.lib.magma_dgerbt_batched(1 if gen else 0, n, nrhs, _vp(pA), lda, _vp(pB), ldb, hu.ctypes.data,
+                                      hv.ctypes.data, C.byref(info), batch, q.handle), "magma_dgerbt_batched")
+    q.sync()
+    return hu, hv
+
+
+def dgesv_rbt_batched(A: torch.Tensor, B: torch.Tensor, queue: Queue | None = None) -> torch.Tensor:
+    q = queue or default_queue()
+    batch, n, lda = A.shape
+    _, nrhs, ldb = B.shape
+    info = torch.empty(batch, dtype=torch.int32, device=A.device)
+    pA, pB = ptr_array(A), ptr_array(B)
+    _check(q.lib.magma_dgesv_rbt_batched(n, nrhs, _vp(pA), lda, _vp(pB), ldb, _vp(info), batch, q.handle),
+           "magma_dgesv_rbt_batched")
+    return info

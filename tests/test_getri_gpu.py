@@ -92,3 +92,52 @@ def test_getrf_nopiv_zero_pivot_and_trans_solve(cuda, n):
         if not trans:
             assert np.array_equal(Bd.cpu().numpy(), OB)
         assert np.abs(Bd.cpu().numpy() - OB).max() <= 64 * n * np.finfo(float).eps * max(1.0, np.abs(OB).max())
+
+
+# ------------------------------------------------------------------ random butterfly transformation
+def _butterfly(n, w):
+    """Dense depth-2 butterfly W = L2 L1 from its 2n weights (numpy, FP64)."""
+    def level(order, ws):
+        h = order // 2
+        Bm = np.zeros((order, order))
+        for i in range(h):
+            Bm[i, i], Bm[i, h + i] = ws[i], ws[h + i]
+            Bm[h + i, i], Bm[h + i, h + i] = ws[i], -ws[h + i]
+        return Bm / np.sqrt(2.0)
+    L1 = level(n, w[:n])
+    L2 = np.zeros((n, n))
+    L2[:n // 2, :n // 2] = level(n // 2, w[n:n + n // 2])
+    L2[n // 2:, n // 2:] = level(n // 2, w[n + n // 2:])
+    return L2 @ L1
+
+
+@pytest.mark.parametrize("n", [8, 64, 100, 256])
+def test_gerbt_matches_dense_transform(cuda, n):
+    import magma_b200 as mb
+    A_np, B_np = T.lu_uniform(4, n, 3, seed=60 + n)
+    A, B = dev(A_np, cuda), dev(B_np, cuda)
+    u, v = mb.dgerbt_batched(A, B)
+    Uw, Vw = _butterfly(n, u), _butterfly(n, v)
+    for b in range(4):
+        ref = Uw.T @ A_np[b].T @ Vw
+        assert np.abs(A.cpu().numpy()[b].T - ref).max() <= 1e-13 * max(1.0, np.abs(ref).max())
+        rb = Uw.T @ B_np[b].T
+        assert np.abs(B.cpu().numpy()[b].T - rb).max() <= 1e-13 * max(1.0, np.abs(rb).max())
+
+
+@pytest.mark.parametrize("n", [16, 64, 128, 256])
+def test_gesv_rbt_solves_without_pivoting(cuda, n):
+    """RBT + LU without pivoting solves systems whose leading pivots are zero, where
+    LU without pivoting alone breaks down."""
+    import magma_b200 as mb
+    batch, nrhs = 12, 2
+    A_np, B_np = T.lu_uniform(batch, n, nrhs, seed=90 + n)
+    A_np[:, 0, 0] = 0.0                        # a zero first pivot: nopiv alone fails
+    A, B = dev(A_np, cuda), dev(B_np, cuda)
+    info = mb.dgesv_rbt_batched(A, B)
+    assert np.all(info.cpu().numpy() == 0)
+    be = T.backward_error(A_np, B.cpu().numpy(), B_np, n)
+    assert be.max() <= 1e-11, be.max()
+    A2 = dev(A_np, cuda)
+    info2 = mb.dgetrf_nopiv_batched(A2)
+    assert np.all(info2.cpu().numpy() == 1)    # the untransformed system has pivot 1 == 0
