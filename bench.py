@@ -18,6 +18,7 @@ Workloads (the default is the one the metric is quoted on):
   c5  the request loop: Poisson arrivals swept 1e3..1e5 req/s, 70% LU / 30% Cholesky,
       n log-uniform on [8, 1024], 1-16 RHS, 40 GB admission budget; throughput and
       p50/p99 latency at 1e4 req/s, the sweep beside.
+  qr  Householder QR: magma_dgeqrf_batched on 10,000 x (64x64), U[-1,1] (factorizations/s).
 
 Timing: W untimed steps, then exactly K steps between a barrier + device
 synchronisation on both sides, measured with CUDA events on the library's
@@ -728,8 +729,103 @@ class C4CholVbatched:
             f"{done} solves (first {sample} instances, re-run); LAPACK dpotrf + dpotrs (OpenBLAS 0.3.30, scipy) " \
             f"in an OpenMP loop, 1 BLAS thread each"
 
-WORKLOADS = {"c3": C3Mixed, "c1": C1DgesvSmall, "c2": C2GemmVbatched, "c4": C4CholVbatched}
-DEFAULT_STEPS = {"c3": (60, 5), "c1": (20000, 50), "c2": (50, 5), "c4": (20, 3), "c5": (3000, 200)}
+class QrBatched:
+    """Householder QR, 10,000 x (64x64) (magma_dgeqrf_batched)."""
+    name = "qr_dgeqrf_batched_10000x64x64"
+    unit = "factorizations/s"
+    dtype = "f64"
+    metric = "dgeqrf_batched factorizations/s (FP64)"
+    data = "synthetic: seeded U[-1,1] (splitmix64)"
+
+    def __init__(self, dev, batch=10000, m=64, n=64, seed=6):
+        import torch
+
+        from magma_b200 import testing as T
+        from magma_b200.api import ptr_array
+
+        self.torch, self.dev, self.batch, self.m, self.n = torch, dev, batch, m, n
+        self.A_np, _ = T.lu_uniform(batch, n, 1, seed=seed)
+        self.A0 = torch.from_numpy(self.A_np).to(dev)
+        self.A = torch.empty_like(self.A0)
+        self.tau = torch.zeros((batch, n), dtype=torch.float64, device=dev)
+        self.info = torch.zeros(batch, dtype=torch.int32, device=dev)
+        self.pA, self.pT = ptr_array(self.A), ptr_array(self.tau)
+        self.l2 = f"A ({8 * batch * m * n / 2**20:.0f} MiB) > L2, restored from a device copy between steps"
+
+    def units(self):
+        return self.batch
+
+    def config_extra(self):
+        return {"m": self.m, "n": self.n}
+
+    def bytes_per_unit(self):
+        return 2 * 8 * self.m * self.n + 8 * self.n
+
+    def flops_per_unit(self):
+        m, n = self.m, self.n
+        return 2 * m * n * n - 2 * n ** 3 / 3
+
+    def launches_per_step(self):
+        return 1
+
+    def restore(self, i):
+        self.A.copy_(self.A0)
+
+    def step(self, q, i):
+        return q.lib.magma_dgeqrf_batched(self.m, self.n, vp(self.pA), self.m, vp(self.pT), vp(self.info),
+                                          self.batch, q.handle)
+
+    def validate(self, q):
+        import oracle
+
+        self.restore(0)
+        self.step(q, 0)
+        q.sync()
+        k = 256
+        G = self.A[:k].cpu().numpy()
+        O = self.A_np[:k].copy()
+        tau_o = oracle.dgeqrf_batched(O, self.m)
+        return {"max_abs_diff_vs_oracle": float(abs(G - O).max()),
+                "tau_max_abs_diff_vs_oracle": float(abs(self.tau[:k].cpu().numpy() - tau_o).max())}
+
+    def dominant_kernel(self, q, stream, reps=50):
+        ms = timed_restore(stream, lambda i: self.step(q, i), self.restore, reps) / reps
+        fl = self.flops_per_unit() * self.batch
+        return {"kernel": "geqrf_small_kernel<64,64>", "ms": ms, "alg_bytes": self.bytes_per_unit() * self.batch,
+                "tflops": fl / (ms * 1e-3) / 1e12,
+                "alg_note": f"FP64 {fl / (ms * 1e-3) / 1e12:.2f} TFLOP/s of {FP64_NOMINAL_TFLOPS} nominal"}
+
+    def e2e_setup(self):
+        t = self.torch
+        self.hA = t.from_numpy(self.A_np).pin_memory()
+        self.hR = t.empty_like(self.hA).pin_memory()
+        self.hT = t.empty((self.batch, self.n), dtype=t.float64).pin_memory()
+        self.h2d = self.hA.numel() * 8
+        self.d2h = self.hR.numel() * 8 + self.hT.numel() * 8
+
+    def e2e_step(self, q, i):
+        self.A.copy_(self.hA, non_blocking=True)
+        self.step(q, i)
+        self.hR.copy_(self.A, non_blocking=True)
+        self.hT.copy_(self.tau, non_blocking=True)
+
+    def cpu_reference(self, seconds=10.0, nthreads=None):
+        import oracle
+
+        done, t_total = 0, 0.0
+        while t_total < seconds:
+            A = self.A_np.copy()
+            t0 = time.perf_counter()
+            oracle.lapack_dgeqrf_batched(A, self.m, nthreads=nthreads)
+            t_total += time.perf_counter() - t0
+            done += self.batch
+        return done / t_total, done, (nthreads or oracle.max_threads()), \
+            f"{done} factorizations (10,000-instance batches, same inputs); LAPACK dgeqrf (OpenBLAS 0.3.30, " \
+            f"scipy) in an OpenMP loop, 1 BLAS thread each"
+
+
+WORKLOADS = {"c3": C3Mixed, "c1": C1DgesvSmall, "c2": C2GemmVbatched, "c4": C4CholVbatched, "qr": QrBatched}
+DEFAULT_STEPS = {"c3": (60, 5), "c1": (20000, 50), "c2": (50, 5), "c4": (20, 3), "c5": (3000, 200), "qr": (200, 5)}
 
 
 # ---------------------------------------------------------------------- main
@@ -761,10 +857,11 @@ def run_reference(args, rank):
     from magma_b200 import testing as T
 
     nthreads = oracle.max_threads()
-    if args.workload not in ("c1", "c3"):
-        print(json.dumps({"impl": "reference", "unavailable": "the reference arm covers the c1 and c3 workloads; "
-                          "c2/c4 report their CPU LAPACK loop as cpu_baseline"}), flush=True)
+    if args.workload not in ("c1", "c3", "qr"):
+        print(json.dumps({"impl": "reference", "unavailable": "the reference arm covers the c1, c3 and qr "
+                          "workloads; c2/c4 report their CPU LAPACK loop as cpu_baseline"}), flush=True)
         return
+    metric, unit = METRIC, "solves/s"
     # each step gets fresh copies of the inputs, made outside the timed call
     if args.workload == "c3":
         sample = 256
@@ -774,6 +871,14 @@ def run_reference(args, rank):
         desc = f"{sample} instances per step (256x256, kappa in [1e2,1e6], 4 RHS); LAPACK dsgesv"
         cfg = {"workload": "c3_dsgesv_batched_2048x256_kappa1e2-1e6_nrhs4", "batch": sample, "n": 256, "nrhs": 4}
         dtype = C3Mixed.dtype
+    elif args.workload == "qr":
+        sample = 10000
+        A0, _ = T.lu_uniform(sample, 64, 1, seed=6)
+        prep = lambda: (A0.copy(), None)   # noqa: E731
+        fn = lambda a, b: oracle.lapack_dgeqrf_batched(a, 64, nthreads=nthreads)   # noqa: E731
+        desc = f"{sample} instances per step (64x64); LAPACK dgeqrf"
+        cfg = {"workload": QrBatched.name, "batch": sample, "m": 64, "n": 64}
+        dtype, metric, unit = QrBatched.dtype, QrBatched.metric, QrBatched.unit
     else:
         sample = 10000
         A0, B0 = T.lu_uniform(sample, 32, 1, seed=1)
@@ -794,13 +899,13 @@ def run_reference(args, rank):
     value = sample * args.steps / total
     del np
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+        "impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype, "data": "synthetic",
         "config": cfg,
-        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": nthreads, "kind": "reference",
+        "cpu_baseline": {"value": value, "unit": unit, "cores": nthreads, "kind": "reference",
                          "sample": desc + " (OpenBLAS 0.3.30, scipy) in an OpenMP loop, 1 BLAS thread each"},
-        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 

@@ -218,6 +218,14 @@ magma_int_t magma_dgesv_rbt_batched(magma_int_t n, magma_int_t nrhs, double** dA
                                     double** dB_array, magma_int_t lddb, magma_int_t* dinfo_array,
                                     magma_int_t batchCount, magma_queue_t queue);
 
+/* Householder QR: src/zgeqrf_batched.cpp:89-119 (info_array zeroed first; m -1, n -2,
+ * ldda -4). LAPACK's representation: R on and above the diagonal, the reflectors'
+ * vectors below it (unit leading entry implied), tau_i (min(m,n) entries) per
+ * instance. m <= 256, n <= 64 (MAGMA_ERR_NOT_SUPPORTED otherwise). */
+magma_int_t magma_dgeqrf_batched(magma_int_t m, magma_int_t n, double** dA_array, magma_int_t ldda,
+                                 double** dtau_array, magma_int_t* info_array, magma_int_t batchCount,
+                                 magma_queue_t queue);
+
 /* Inverse from the getrf factors into a separate array: dinvA_i = inv(A_i).
  * src/zgetri_outofplace_batched.cpp:82-220; checks n -1, ldda -3, lddia -6.
  * info_array (may be NULL): 1-based index of the first exactly-zero U(i,i), else 0.

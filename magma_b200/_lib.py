@@ -73,6 +73,7 @@ SIGNATURES: dict[str, tuple] = {
     "magma_dgetrs_nopiv_batched": (_i, [_i, _i, _i, _p, _i, _p, _i, _p, _i, _p]),
     "magma_dgesv_nopiv_batched": (_i, [_i, _i, _p, _i, _p, _i, _p, _i, _p]),
     "magma_dgerbt_batched": (_i, [_i, _i, _i, _p, _i, _p, _i, _p, _p, _p, _i, _p]),
+    "magma_dgeqrf_batched": (_i, [_i, _i, _p, _i, _p, _p, _i, _p]),
     "magma_dgesv_rbt_batched": (_i, [_i, _i, _p, _i, _p, _i, _p, _i, _p]),
     "magma_sgetrf_batched": (_i, [_i, _i, _p, _i, _p, _p, _i, _p]),
     "magma_sgetrs_batched": (_i, [_i, _i, _i, _p, _i, _p, _p, _i, _i, _p]),

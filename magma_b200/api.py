@@ -453,3 +453,16 @@ def dgesv_rbt_batched(A: torch.Tensor, B: torch.Tensor, queue: Queue | None = No
     _check(q.lib.magma_dgesv_rbt_batched(n, nrhs, _vp(pA), lda, _vp(pB), ldb, _vp(info), batch, q.handle),
            "magma_dgesv_rbt_batched")
     return info
+
+
+def dgeqrf_batched(A: torch.Tensor, m: int | None = None, queue: Queue | None = None) -> torch.Tensor:
+    """Householder QR of each (m x n) instance of A (batch, n, lda), in place. Returns tau."""
+    q = queue or default_queue()
+    batch, n, lda = A.shape
+    m = lda if m is None else m
+    tau = torch.zeros((batch, max(1, min(m, n))), dtype=torch.float64, device=A.device)
+    info = torch.empty(batch, dtype=torch.int32, device=A.device)
+    pA, pT = ptr_array(A), ptr_array(tau)
+    _check(q.lib.magma_dgeqrf_batched(m, n, _vp(pA), lda, _vp(pT), _vp(info), batch, q.handle),
+           "magma_dgeqrf_batched")
+    return tau

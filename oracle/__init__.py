@@ -115,6 +115,14 @@ def dgetrf_nopiv_batched(A: np.ndarray, m: int):
     return ipiv, info
 
 
+def dgeqrf_batched(A: np.ndarray, m: int):
+    """In-place Householder QR (dgeqr2 restatement) of a (batch, n, lda) batch. Returns tau."""
+    batch, n, lda = A.shape
+    tau = np.zeros((batch, max(1, min(m, n))))
+    lib().oracle_dgeqrf_batched(m, n, _d(A), lda, C.c_long(n * lda), _d(tau), C.c_long(tau.shape[1]), batch)
+    return tau
+
+
 def dgetrs_batched(A: np.ndarray, ipiv: np.ndarray, B: np.ndarray, trans: bool = False):
     """Solve with the factors; B is (batch, nrhs, ldb), overwritten with X."""
     batch, n, lda = A.shape
@@ -170,6 +178,15 @@ def lapack_dgesv_batched(A: np.ndarray, B: np.ndarray, nthreads: int | None = No
     _lapack().ref_dgesv_batched(n, nrhs, _d(A), lda, C.c_long(n * lda), _i(ipiv), C.c_long(n), _d(B), ldb,
                                 C.c_long(nrhs * ldb), _i(info), batch, nthreads or max_threads())
     return ipiv, info
+
+
+def lapack_dgeqrf_batched(A: np.ndarray, m: int, nthreads: int | None = None):
+    """LAPACK dgeqrf per instance, in place on a (batch, n, lda) batch; returns tau."""
+    batch, n, lda = A.shape
+    tau = np.zeros((batch, max(1, min(m, n))))
+    _lapack().ref_dgeqrf_batched(m, n, _d(A), lda, C.c_long(n * lda), _d(tau), C.c_long(tau.shape[1]), batch,
+                                 nthreads or max_threads())
+    return tau
 
 
 def lapack_dsgesv_batched(A: np.ndarray, B: np.ndarray, nthreads: int | None = None):

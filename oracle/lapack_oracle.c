@@ -92,6 +92,40 @@ void oracle_dgetrf_nopiv_batched(int m, int n, double* A, int lda, long strideA,
         oracle_dgetf2_nopiv(m, n, A + (size_t)i * strideA, lda, ipiv + (size_t)i * strideP, info + i);
 }
 
+/* LAPACK 3.x dgeqr2: Householder QR, dlarfg (beta = -sign(alpha) * hypot(alpha, ||x||),
+ * tau = (beta - alpha) / beta, v = x / (alpha - beta); tau = 0 when ||x|| = 0, no
+ * rescaling loop for tiny beta) and dlarf (w = v^T C, C -= tau v w^T) per column. */
+void oracle_dgeqr2(int m, int n, double* a, int lda, double* tau) {
+    const int kmax = m < n ? m : n;
+    for (int k = 0; k < kmax; ++k) {
+        double xs = 0.0;
+        for (int i = k + 1; i < m; ++i) xs = fma(A_(i, k), A_(i, k), xs);
+        const double alpha = A_(k, k);
+        double t = 0.0;
+        if (xs > 0.0) {
+            const double beta = -copysign(hypot(alpha, sqrt(xs)), alpha);
+            t = (beta - alpha) / beta;
+            const double scal = 1.0 / (alpha - beta);
+            for (int i = k + 1; i < m; ++i) A_(i, k) *= scal;
+            A_(k, k) = beta;
+        }
+        tau[k] = t;
+        if (t == 0.0) continue;
+        for (int j = k + 1; j < n; ++j) {
+            double w = A_(k, j);
+            for (int i = k + 1; i < m; ++i) w = fma(A_(i, k), A_(i, j), w);
+            A_(k, j) = fma(-t, w, A_(k, j));
+            for (int i = k + 1; i < m; ++i) A_(i, j) = fma(-t * A_(i, k), w, A_(i, j));
+        }
+    }
+}
+
+void oracle_dgeqrf_batched(int m, int n, double* A, int lda, long strideA, double* tau, long strideT, int batch) {
+#pragma omp parallel for schedule(dynamic)
+    for (int i = 0; i < batch; ++i)
+        oracle_dgeqr2(m, n, A + (size_t)i * strideA, lda, tau + (size_t)i * strideT);
+}
+
 /* LAPACK dlaswp on the rows of B: forward (k ascending) or inverse. */
 static void laswp(int n, int nrhs, double* b, int ldb, const int* ipiv, int inverse) {
     for (int t = 0; t < n; ++t) {

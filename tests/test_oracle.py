@@ -139,3 +139,30 @@ def test_oracle_cholesky_upper_is_transpose():
     i2 = oracle.dposv_vbatched(up, [b.copy()], [n], [1], [n], [n], solve=False, upper=True)
     assert i1[0] == 0 and i2[0] == 0
     assert np.array_equal(np.tril(lo[0].T), np.triu(up[0].T).T)
+
+
+@pytest.mark.parametrize("m,n", [(8, 8), (40, 17), (64, 64), (200, 50)])
+def test_oracle_geqr2_matches_lapack(m, n):
+    """The restated dgeqr2 agrees with LAPACK dgeqrf (numpy's qr, mode 'raw') to rounding:
+    same reflectors, same signs of R's diagonal, same tau."""
+    rng = np.random.default_rng(m * 1000 + n)
+    batch = 6
+    A = rng.uniform(-1, 1, (batch, n, m))          # column-major (batch, n, lda=m)
+    G = A.copy()
+    tau = oracle.dgeqrf_batched(G, m)
+    k = min(m, n)
+    for b in range(batch):
+        h, t = np.linalg.qr(A[b].T, mode="raw")    # h is LAPACK's column-major output
+        assert np.abs(G[b] - h).max() < 64 * m * EPS
+        assert np.abs(tau[b, :k] - t).max() < 64 * m * EPS
+
+
+def test_oracle_geqr2_matches_reference_loop():
+    """The restated dgeqr2 against the reference CPU loop (OpenBLAS dgeqrf per instance)."""
+    m, n = 64, 64
+    A, _ = T.lu_uniform(200, n, 1, seed=77)
+    G1, G2 = A.copy(), A.copy()
+    t1 = oracle.dgeqrf_batched(G1, m)
+    t2 = oracle.lapack_dgeqrf_batched(G2, m, nthreads=2)
+    assert np.abs(G1 - G2).max() < 64 * m * EPS
+    assert np.abs(t1 - t2).max() < 64 * m * EPS
