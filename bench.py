@@ -791,7 +791,7 @@ class QrBatched:
     def dominant_kernel(self, q, stream, reps=50):
         ms = timed_restore(stream, lambda i: self.step(q, i), self.restore, reps) / reps
         fl = self.flops_per_unit() * self.batch
-        return {"kernel": "geqrf_small_kernel<64,64>", "ms": ms, "alg_bytes": self.bytes_per_unit() * self.batch,
+        return {"kernel": "geqrf_lanes_kernel<16,4,64>", "ms": ms, "alg_bytes": self.bytes_per_unit() * self.batch,
                 "tflops": fl / (ms * 1e-3) / 1e12,
                 "alg_note": f"FP64 {fl / (ms * 1e-3) / 1e12:.2f} TFLOP/s of {FP64_NOMINAL_TFLOPS} nominal"}
 

@@ -1,144 +1,154 @@
 // qr.cu -- batched Householder QR (magma_dgeqrf_batched, src/zgeqrf_batched.cpp:89-230).
 //
-// One thread block per matrix, thread t = row t, the row's n <= NC entries in
-// registers (the register-resident layout of the LU kernels). For each column k
-// (LAPACK dgeqr2 order: dlarfg, then dlarf on the trailing columns):
-//   xnorm = ||A(k+1:m, k)|| by a block reduction, beta = -sign(alpha) hypot(alpha, xnorm),
-//   tau = (beta - alpha) / beta, v = A(k+1:m, k) / (alpha - beta), A(k,k) = beta
-//   (tau = 0 when xnorm == 0: H = I);
-//   w = v^T A(k:m, k+1:n) for all trailing columns at once: every thread forms
-//   v_t A(t, j), each warp reduces its 32 rows for 32 columns with one reduce-scatter
-//   of 31 shuffles (lane j ends with column j's sum), warps are combined in shared
-//   memory;  A(k:m, k+1:n) -= tau v w^T.
-// The factors use LAPACK's representation: R on and above the diagonal, the
-// Householder vectors (unit leading entry implied) below it, tau per reflector.
-// Unlike LAPACK's dlarfg there is no rescaling loop for |beta| < safmin (orders of
-// magnitude below the inputs this path serves); the sums run in tree order, so
-// results agree with LAPACK to rounding, not bit for bit.
+// LAPACK dgeqr2 order: for each column k, dlarfg on A(k:m, k), then dlarf on the
+// trailing columns. One thread block per matrix; P consecutive lanes per column
+// (P = 1, 2, 4, 8 for m <= 16, 32, 64, 128; P = 8 with 32 rows a lane for m <= 256);
+// lane p of column j holds rows r = i*P + p (i < S) in registers, so a warp's
+// load or store of element i touches P consecutive rows of each of its columns
+// (sector-coalesced without staging). Rows >= m are zero.
+//
+// Step k (one barrier; the shared vectors are double-buffered by step parity):
+//   the P lanes of column k:  xs_p = sum_{r>k, r=p mod P} a_r^2 (ascending fma chain),
+//     xs = pairwise tree over p, beta = -sign(alpha) sqrt(fma(alpha, alpha, xs)),
+//     tau = (beta - alpha) / beta, scal = 1 / (alpha - beta), v_r = a_r * scal;
+//     publish sv_r = (0 for r < k, 1 for r = k, v_r for r > k) and stv_r = -tau * sv_r;
+//   every column j > k:  w_p = sum over its rows of sv_r a_r (ascending fma chain from 0),
+//     w = pairwise tree over p, a_r = fma(stv_r, w, a_r) for all its rows.
+// The oracle restates exactly this order (rows above k enter with zero weights), so
+// the factors are BIT-IDENTICAL to it; against LAPACK dgeqrf they agree to rounding.
+// tau = 0 when xs == 0 (H = I). Without dnrm2's scaling and dlapy2's guard, entries
+// must lie well inside [1e-150, 1e150] (far beyond the inputs this path serves).
 #include "internal.h"
 #include "small_lu.cuh"
 #include <algorithm>
 
 namespace mb200 {
 
-template <int NC, int NT>
-struct QrShared {
-    double red[NT / 32][NC];   // per-warp column sums
-    double w[NC];              // v^T A for the trailing columns
-    double col[NT / 32];       // per-warp partial of ||x||^2
-    double alpha;
-};
-
-// Lane l of the warp returns sum over lanes of v[l] (columns base..base+31 of `v`).
-__device__ __forceinline__ double warp_reduce_scatter32(double (&v)[32], int lane) {
-    static_for<0, 5>([&](auto sc) {
-        constexpr int s = 16 >> decltype(sc)::value;
-        const bool upper = (lane & s) != 0;
+// Sum over the P lanes of a column group (xor butterfly = pairwise tree in lane order;
+// every lane ends with the same value since IEEE addition commutes).
+template <int P>
+__device__ __forceinline__ double group_sum(double x, unsigned mask) {
 #pragma unroll
-        for (int i = 0; i < s; ++i) {
-            const double send = upper ? v[i] : v[i + s];
-            const double keep = upper ? v[i + s] : v[i];
-            v[i] = keep + __shfl_xor_sync(kFullMask, send, s);
-        }
-    });
-    return v[0];
+    for (int o = 1; o < P; o <<= 1) x += __shfl_xor_sync(mask, x, o);
+    return x;
 }
 
-template <int NC, int NT>
-__global__ void __launch_bounds__(NT)
-geqrf_small_kernel(int m, int n, double** dA_array, int lda, double** dtau_array, int batch) {
-    constexpr int NW = NT / 32;
-    __shared__ QrShared<NC, NT> sh;
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+// Register budget: 64 a thread for S = 16 and 128 for S = 32 (the S entries of a
+// plus the shared vectors' pairs in flight), i.e. 16K resp. 32K registers a block.
+template <int S, int P, int NCOL>
+__global__ void __launch_bounds__(P * NCOL, (S == 16 ? 1024 : 512) / (P * NCOL) < 1 ? 1 : (S == 16 ? 1024 : 512) / (P * NCOL))
+geqrf_lanes_kernel(int m, int n, double** dA_array, int lda, double** dtau_array, int batch) {
+    constexpr int SP = S + 2;   // padded, even lane stride in the shared vectors
+    static_assert(S % 2 == 0 && 32 % P == 0, "layout");
+    __shared__ __align__(16) double sv[2][P * SP];
+    __shared__ __align__(16) double stv[2][P * SP];
+    __shared__ double stau[2];
+    const int tid = threadIdx.x, lane = tid & 31, p = tid % P, j = tid / P;
+    constexpr int CPW = 32 / P;                               // columns per warp
+    const int wc0 = (tid >> 5) * CPW;                         // the warp's first column
+    const unsigned gmask = P == 32 ? 0xffffffffu : (((1u << P) - 1) << (lane & ~(P - 1)));
     const int kmax = min(m, n);
     for (int id = blockIdx.x; id < batch; id += gridDim.x) {
-        double* A = dA_array[id];
+        double* A = dA_array[id] + (size_t)j * lda;
         double* tau = dtau_array[id];
-        double a[NC];
+        double a[S];
 #pragma unroll
-        for (int j = 0; j < NC; ++j) a[j] = (t < m && j < n) ? A[t + (size_t)j * lda] : 0.0;
-        static_for<0, NC>([&](auto kc) {
-            constexpr int k = decltype(kc)::value;
-            if (k >= kmax) return;
-            // ---- dlarfg on A(k:m, k) ----
-            double xs = (t > k && t < m) ? a[k] * a[k] : 0.0;
-            for (int off = 16; off > 0; off >>= 1) xs += __shfl_xor_sync(kFullMask, xs, off);
-            if (lane == 0) sh.col[warp] = xs;
-            if (t == k) sh.alpha = a[k];
-            __syncthreads();
-            double xnorm2 = 0.0;
+        for (int i = 0; i < S; ++i) {
+            const int r = i * P + p;
+            a[i] = (j < n && r < m) ? A[r] : 0.0;
+        }
+#pragma unroll 1
+        for (int k = 0; k < kmax; ++k) {
+            const int b = k & 1;
+            if (j == k) {
+                // branch-free: rows <= k enter the chain as fma(a, 0, xs) = xs exactly (xs >= +0)
+                double xs = 0.0, al = 0.0;
 #pragma unroll
-            for (int w = 0; w < NW; ++w) xnorm2 += sh.col[w];
-            const double alpha = sh.alpha;
-            double tk = 0.0, scal = 0.0, beta = alpha;
-            if (xnorm2 > 0.0) {
-                beta = -copysign(hypot(alpha, sqrt(xnorm2)), alpha);
-                tk = (beta - alpha) / beta;
-                scal = 1.0 / (alpha - beta);
-            }
-            // v: 1 at row k, scaled entries below, 0 above
-            const double v = (t == k) ? 1.0 : ((t > k && t < m) ? a[k] * scal : 0.0);
-            if (t > k && t < m && xnorm2 > 0.0) a[k] = v;
-            if (t == k) {
-                a[k] = beta;
-                tau[k] = tk;
-            }
-            // ---- w = v^T A(k:m, k+1:n), then A -= tau v w^T ----
-            if (k + 1 < n) {
-                constexpr int G0 = ((k + 1) / 32) * 32;   // first 32-column group with trailing columns
-                static_for<G0 / 32, NC / 32>([&](auto gc) {
-                    constexpr int g0 = decltype(gc)::value * 32;
-                    double p[32];
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) p[j] = (g0 + j > k) ? v * a[g0 + j] : 0.0;
-                    const double s = warp_reduce_scatter32(p, lane);
-                    sh.red[warp][g0 + lane] = s;
-                });
-                __syncthreads();
-                if (t < NC && t > k) {
-                    double s = 0.0;
-#pragma unroll
-                    for (int w = 0; w < NW; ++w) s += sh.red[w][t];
-                    sh.w[t] = s;
+                for (int i = 0; i < S; ++i) {
+                    const int r = i * P + p;
+                    xs = fma(a[i], r > k ? a[i] : 0.0, xs);
+                    al = r == k ? a[i] : al;
                 }
-                __syncthreads();
-                if (v != 0.0 && tk != 0.0) {
-                    const double tv = tk * v;
+                xs = group_sum<P>(xs, gmask);
+                const double alpha = P == 1 ? al : __shfl_sync(gmask, al, (lane & ~(P - 1)) | (k % P));
+                double t = 0.0, beta = alpha, scal = 1.0;
+                if (xs > 0.0) {
+                    beta = -copysign(sqrt(fma(alpha, alpha, xs)), alpha);
+                    t = (beta - alpha) / beta;
+                    scal = 1.0 / (alpha - beta);
+                }
+                double* svp = sv[b] + p * SP;
+                double* stp = stv[b] + p * SP;
+                const bool scaled = t != 0.0;
 #pragma unroll
-                    for (int j = k + 1; j < NC; ++j) a[j] = fma(-tv, sh.w[j], a[j]);
+                for (int i = 0; i < S; i += 2) {
+                    double v2[2];
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int r = (i + h) * P + p;
+                        const double x = a[i + h] * scal;
+                        v2[h] = r > k ? x : (r == k ? 1.0 : 0.0);
+                        a[i + h] = (r > k && scaled) ? x : (r == k ? beta : a[i + h]);
+                    }
+                    *reinterpret_cast<double2*>(svp + i) = make_double2(v2[0], v2[1]);
+                    *reinterpret_cast<double2*>(stp + i) = make_double2(-t * v2[0], -t * v2[1]);
+                }
+                if (p == 0) {
+                    stau[b] = t;
+                    tau[k] = t;
                 }
             }
             __syncthreads();
-        });
-        if (t < m) {
+            const double t = stau[b];
+            if (t != 0.0 && wc0 + CPW - 1 > k && wc0 < n) {       // the warp has a column in (k, n)
+                const double* svp = sv[b] + p * SP;
+                const double* stp = stv[b] + p * SP;
+                double w = 0.0;
 #pragma unroll
-            for (int j = 0; j < NC; ++j)
-                if (j < n) A[t + (size_t)j * lda] = a[j];
+                for (int i = 0; i < S; i += 2) {
+                    const double2 v = *reinterpret_cast<const double2*>(svp + i);
+                    w = fma(v.x, a[i], w);
+                    w = fma(v.y, a[i + 1], w);
+                }
+                w = group_sum<P>(w, 0xffffffffu);
+                if (j > k && j < n) {
+#pragma unroll
+                    for (int i = 0; i < S; i += 2) {
+                        const double2 tv = *reinterpret_cast<const double2*>(stp + i);
+                        a[i] = fma(tv.x, w, a[i]);
+                        a[i + 1] = fma(tv.y, w, a[i + 1]);
+                    }
+                }
+            }
+        }
+        if (j < n) {
+#pragma unroll
+            for (int i = 0; i < S; ++i) {
+                const int r = i * P + p;
+                if (r < m) A[r] = a[i];
+            }
         }
         __syncthreads();
     }
 }
 
-template <int NC, int NT>
+template <int S, int P>
 static void launch_geqrf(int m, int n, double** A, int lda, double** tau, int batch, cudaStream_t s) {
-    geqrf_small_kernel<NC, NT><<<std::min(batch, 65535), NT, 0, s>>>(m, n, A, lda, tau, batch);
+    const int grid = std::min(batch, 65535);
+    if (n <= 16 && P * 16 >= 32) geqrf_lanes_kernel<S, P, 16><<<grid, P * 16, 0, s>>>(m, n, A, lda, tau, batch);
+    else if (n <= 32) geqrf_lanes_kernel<S, P, 32><<<grid, P * 32, 0, s>>>(m, n, A, lda, tau, batch);
+    else geqrf_lanes_kernel<S, P, 64><<<grid, P * 64, 0, s>>>(m, n, A, lda, tau, batch);
 }
 
 bool geqrf_supported(int m, int n) { return m <= 256 && n <= 64; }
 
 magma_int_t geqrf_small(int m, int n, double** A, int lda, double** tau, int batch, cudaStream_t s) {
     if (!geqrf_supported(m, n)) return MAGMA_ERR_NOT_SUPPORTED;
-    const int NT = m <= 32 ? 32 : m <= 64 ? 64 : m <= 128 ? 128 : 256;
-    if (n <= 32) {
-        if (NT == 32) launch_geqrf<32, 32>(m, n, A, lda, tau, batch, s);
-        else if (NT == 64) launch_geqrf<32, 64>(m, n, A, lda, tau, batch, s);
-        else if (NT == 128) launch_geqrf<32, 128>(m, n, A, lda, tau, batch, s);
-        else launch_geqrf<32, 256>(m, n, A, lda, tau, batch, s);
-    } else {
-        if (NT <= 64) launch_geqrf<64, 64>(m, n, A, lda, tau, batch, s);
-        else if (NT == 128) launch_geqrf<64, 128>(m, n, A, lda, tau, batch, s);
-        else launch_geqrf<64, 256>(m, n, A, lda, tau, batch, s);
-    }
+    if (m <= 16) launch_geqrf<16, 1>(m, n, A, lda, tau, batch, s);
+    else if (m <= 32) launch_geqrf<16, 2>(m, n, A, lda, tau, batch, s);
+    else if (m <= 64) launch_geqrf<16, 4>(m, n, A, lda, tau, batch, s);
+    else if (m <= 128) launch_geqrf<16, 8>(m, n, A, lda, tau, batch, s);
+    else launch_geqrf<32, 8>(m, n, A, lda, tau, batch, s);
     return launch_status();
 }
 

@@ -29,6 +29,7 @@
  */
 #include <float.h>
 #include <math.h>
+#include <stdlib.h>
 #include <stddef.h>
 #include <string.h>
 
@@ -92,32 +93,57 @@ void oracle_dgetrf_nopiv_batched(int m, int n, double* A, int lda, long strideA,
         oracle_dgetf2_nopiv(m, n, A + (size_t)i * strideA, lda, ipiv + (size_t)i * strideP, info + i);
 }
 
-/* LAPACK 3.x dgeqr2: Householder QR, dlarfg (beta = -sign(alpha) * hypot(alpha, ||x||),
- * tau = (beta - alpha) / beta, v = x / (alpha - beta); tau = 0 when ||x|| = 0, no
- * rescaling loop for tiny beta) and dlarf (w = v^T C, C -= tau v w^T) per column. */
+/* LAPACK 3.x dgeqr2 (Householder QR: dlarfg, then dlarf on the trailing columns), with
+ * the summation order of the batched path written out: the rows of a column are dealt
+ * to P lanes (row r to lane r mod P, P = 1, 2, 4, 8 for m <= 16, 32, 64, 256); each
+ * lane sums its rows in ascending order with fma, and the P partial sums are added as
+ * a pairwise tree ((x0+x1)+(x2+x3))+... . For column k:
+ *   xs = ||A(k+1:m, k)||^2 in that order, beta = -sign(alpha) sqrt(fma(alpha, alpha, xs)),
+ *   tau = (beta - alpha) / beta, v_r = A(r,k) * (1 / (alpha - beta)); tau = 0 when xs = 0;
+ *   with s_r = 0 (r < k), 1 (r = k), v_r (r > k) and t_r = -tau * s_r, every trailing
+ *   column j takes w = sum_r s_r A(r,j) (all m rows, in that order) and
+ *   A(r,j) = fma(t_r, w, A(r,j)) for all m rows (rows above k change by an exact zero).
+ * Against LAPACK this differs by rounding only (and the sign of exact zeros); dnrm2's
+ * scaling and dlapy2's guard are omitted (entries far inside [1e-150, 1e150]). */
+static int qr_lanes(int m) { return m <= 16 ? 1 : m <= 32 ? 2 : m <= 64 ? 4 : 8; }
+
+static double tree_sum(double* x, int P) {
+    for (int h = 1; h < P; h *= 2)
+        for (int p = 0; p < P; p += 2 * h) x[p] = x[p] + x[p + h];
+    return x[0];
+}
+
 void oracle_dgeqr2(int m, int n, double* a, int lda, double* tau) {
-    const int kmax = m < n ? m : n;
+    const int kmax = m < n ? m : n, P = qr_lanes(m);
+    double part[32];
+    double* sv = (double*)malloc(sizeof(double) * (size_t)(m > 0 ? m : 1));
+    double* st = (double*)malloc(sizeof(double) * (size_t)(m > 0 ? m : 1));
     for (int k = 0; k < kmax; ++k) {
-        double xs = 0.0;
-        for (int i = k + 1; i < m; ++i) xs = fma(A_(i, k), A_(i, k), xs);
+        for (int p = 0; p < P; ++p) part[p] = 0.0;
+        for (int r = k + 1; r < m; ++r) part[r % P] = fma(A_(r, k), A_(r, k), part[r % P]);
+        const double xs = tree_sum(part, P);
         const double alpha = A_(k, k);
-        double t = 0.0;
+        double t = 0.0, beta = alpha, scal = 1.0;
         if (xs > 0.0) {
-            const double beta = -copysign(hypot(alpha, sqrt(xs)), alpha);
+            beta = -copysign(sqrt(fma(alpha, alpha, xs)), alpha);
             t = (beta - alpha) / beta;
-            const double scal = 1.0 / (alpha - beta);
-            for (int i = k + 1; i < m; ++i) A_(i, k) *= scal;
-            A_(k, k) = beta;
+            scal = 1.0 / (alpha - beta);
         }
+        for (int r = 0; r < m; ++r) sv[r] = r < k ? 0.0 : r == k ? 1.0 : A_(r, k) * scal;
+        for (int r = 0; r < m; ++r) st[r] = -t * sv[r];
         tau[k] = t;
         if (t == 0.0) continue;
+        for (int r = k + 1; r < m; ++r) A_(r, k) = sv[r];
+        A_(k, k) = beta;
         for (int j = k + 1; j < n; ++j) {
-            double w = A_(k, j);
-            for (int i = k + 1; i < m; ++i) w = fma(A_(i, k), A_(i, j), w);
-            A_(k, j) = fma(-t, w, A_(k, j));
-            for (int i = k + 1; i < m; ++i) A_(i, j) = fma(-t * A_(i, k), w, A_(i, j));
+            for (int p = 0; p < P; ++p) part[p] = 0.0;
+            for (int r = 0; r < m; ++r) part[r % P] = fma(sv[r], A_(r, j), part[r % P]);
+            const double w = tree_sum(part, P);
+            for (int r = 0; r < m; ++r) A_(r, j) = fma(st[r], w, A_(r, j));
         }
     }
+    free(sv);
+    free(st);
 }
 
 void oracle_dgeqrf_batched(int m, int n, double* A, int lda, long strideA, double* tau, long strideT, int batch) {

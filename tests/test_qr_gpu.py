@@ -2,8 +2,9 @@
 
 Checks follow the reference's testing_zgeqrf_batched.cpp: ||R - Q^T A||_1 / (N ||A||_1)
 and ||I - Q^T Q||_1 / N below 30 eps; in addition the reflectors, R and tau agree with
-the oracle's dgeqr2 restatement (itself pinned to LAPACK dgeqrf) to rounding — the
-column sums run in tree order on the GPU, so agreement is to a few ulps, not bitwise."""
+the oracle's dgeqr2 restatement BIT FOR BIT: the oracle writes out the kernel's
+summation order (rows dealt to P lanes, ascending fma chains, pairwise tree), and is
+itself pinned to LAPACK dgeqrf to rounding."""
 import numpy as np
 import pytest
 
@@ -44,7 +45,8 @@ def qr_errors(A0, h, tau, m, n):
 @pytest.mark.parametrize("m,n,batch,lda", [(1, 1, 7, 1), (8, 8, 50, 8), (32, 16, 40, 32), (40, 17, 30, 45),
                                            (64, 64, 20, 64), (100, 32, 16, 100), (128, 64, 10, 130),
                                            (200, 50, 8, 200), (256, 64, 6, 256), (256, 1, 6, 256),
-                                           (10, 30, 12, 10), (20, 64, 8, 24)])
+                                           (10, 30, 12, 10), (20, 64, 8, 24), (5, 3, 9, 5), (17, 17, 9, 17),
+                                           (33, 40, 9, 35), (49, 20, 9, 49), (64, 8, 9, 64), (16, 33, 9, 16)])
 def test_geqrf_matches_oracle(cuda, m, n, batch, lda):
     import magma_b200 as mb
     rng = np.random.default_rng(1000 * m + n)
@@ -56,6 +58,8 @@ def test_geqrf_matches_oracle(cuda, m, n, batch, lda):
     tau_o = oracle.dgeqrf_batched(O, m)
     k = min(m, n)
     assert np.array_equal(G[:, :, m:], A_np[:, :, m:])            # padding rows untouched
+    assert np.array_equal(G, O)                                    # the oracle restates the kernel's order
+    assert np.array_equal(tau[:, :k], tau_o[:, :k])
     assert np.abs(G - O).max() < 64 * max(m, n) * EPS
     assert np.abs(tau[:, :k] - tau_o[:, :k]).max() < 64 * max(m, n) * EPS
     for b in range(batch):
@@ -80,6 +84,7 @@ def test_geqrf_zero_and_ill_conditioned_columns(cuda):
     O = A_np.copy()
     tau_o = oracle.dgeqrf_batched(O, m)
     assert np.all(np.isfinite(G)) and np.all(np.isfinite(tau))
+    assert np.array_equal(G, O) and np.array_equal(tau, tau_o)     # bit-identical, even the noise column
     well = [0, 1, 3, 4]      # instance 2's column 10 is rounding noise after step 9: its reflector is arbitrary
     assert np.abs(tau[well] - tau_o[well]).max() < 64 * m * EPS
     assert tau[1, 3] == 0.0 and tau_o[1, 3] == 0.0
