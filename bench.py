@@ -19,6 +19,9 @@ Workloads (the default is the one the metric is quoted on):
       n log-uniform on [8, 1024], 1-16 RHS, 40 GB admission budget; throughput and
       p50/p99 latency at 1e4 req/s, the sweep beside.
   qr  Householder QR: magma_dgeqrf_batched on 10,000 x (64x64), U[-1,1] (factorizations/s).
+  getri  LU + out-of-place inverse (getrf + getri_outofplace) on 10,000 x (32x32) (inverses/s).
+  nopiv  gesv_nopiv_batched on 10,000 x (32x32) diagonally dominant, 1 RHS, with
+      gesv_rbt_batched on the same inputs beside (solves/s).
 
 Timing: W untimed steps, then exactly K steps between a barrier + device
 synchronisation on both sides, measured with CUDA events on the library's
@@ -824,8 +827,224 @@ class QrBatched:
             f"scipy) in an OpenMP loop, 1 BLAS thread each"
 
 
-WORKLOADS = {"c3": C3Mixed, "c1": C1DgesvSmall, "c2": C2GemmVbatched, "c4": C4CholVbatched, "qr": QrBatched}
-DEFAULT_STEPS = {"c3": (60, 5), "c1": (20000, 50), "c2": (50, 5), "c4": (20, 3), "c5": (3000, 200), "qr": (200, 5)}
+
+class _Flush:
+    """Writes a buffer larger than L2 (outside the timed brackets) so a restored input
+    that fits in L2 is read from HBM by the timed step."""
+
+    def __init__(self, torch, dev):
+        self.buf = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
+
+    def __call__(self):
+        self.buf.zero_()
+
+
+class GetriBatched:
+    """LU + out-of-place inverse, 10,000 x (32x32) (magma_dgetrf_batched +
+    magma_dgetri_outofplace_batched, timed together as testing_zgetri_batched.cpp:119-122)."""
+    name = "getri_dgetrf+dgetri_outofplace_batched_10000x32"
+    unit = "inverses/s"
+    dtype = "f64"
+    metric = "getrf + getri_outofplace inverses/s (FP64)"
+    data = "synthetic: seeded U[-1,1] (splitmix64)"
+
+    def __init__(self, dev, batch=10000, n=32, seed=8):
+        import torch
+
+        from magma_b200 import testing as T
+        from magma_b200.api import ptr_array
+
+        self.torch, self.dev, self.batch, self.n = torch, dev, batch, n
+        self.A_np, _ = T.lu_uniform(batch, n, 1, seed=seed)
+        self.A0 = torch.from_numpy(self.A_np).to(dev)
+        self.A = torch.empty_like(self.A0)
+        self.inv = torch.empty_like(self.A0)
+        self.ipiv = torch.zeros((batch, n), dtype=torch.int32, device=dev)
+        self.info = torch.zeros(batch, dtype=torch.int32, device=dev)
+        self.pA, self.pI, self.pP = ptr_array(self.A), ptr_array(self.inv), ptr_array(self.ipiv)
+        self.flush = _Flush(torch, dev)
+        self.l2 = "A restored, then a 252 MiB buffer written (L2 flushed) between steps"
+
+    def units(self):
+        return self.batch
+
+    def config_extra(self):
+        return {"n": self.n}
+
+    def bytes_per_unit(self):
+        n = self.n
+        return 3 * 8 * n * n + 4 * n + 4        # read A, write LU and inv(A), pivots, info
+
+    def launches_per_step(self):
+        return 3                                # getrf, getri set-up, getrs on I
+
+    def restore(self, i):
+        self.A.copy_(self.A0)
+        self.flush()
+
+    def step(self, q, i):
+        rc = q.lib.magma_dgetrf_batched(self.n, self.n, vp(self.pA), self.n, vp(self.pP), vp(self.info),
+                                        self.batch, q.handle)
+        return rc or q.lib.magma_dgetri_outofplace_batched(self.n, vp(self.pA), self.n, vp(self.pP), vp(self.pI),
+                                                           self.n, vp(self.info), self.batch, q.handle)
+
+    def validate(self, q):
+        import numpy as np
+
+        self.restore(0)
+        self.step(q, 0)
+        q.sync()
+        k = 200
+        X = self.inv[:k].cpu().numpy()
+        res = max(float(np.abs(self.A_np[b].T @ X[b].T - np.eye(self.n)).max()) for b in range(k))
+        return {"max_abs_A_invA_minus_I": res, "infos_nonzero": int((self.info != 0).sum())}
+
+    def dominant_kernel(self, q, stream, reps=50):
+        ms = timed_restore(stream, lambda i: self.step(q, i), self.restore, reps) / reps
+        fl = 2 * self.n ** 3 * self.batch
+        return {"kernel": "getrf+getri (gesv_small_kernel, getri_setup_kernel, getrs_small_kernel)", "ms": ms,
+                "alg_bytes": self.bytes_per_unit() * self.batch, "tflops": fl / (ms * 1e-3) / 1e12,
+                "alg_note": "the whole step (3 launches); 2 n^3 flops per inverse"}
+
+    def e2e_setup(self):
+        t = self.torch
+        self.hA = t.from_numpy(self.A_np).pin_memory()
+        self.hX = t.empty_like(self.hA).pin_memory()
+        self.hI = t.empty(self.batch, dtype=t.int32).pin_memory()
+        self.h2d = self.hA.numel() * 8
+        self.d2h = self.hX.numel() * 8 + self.hI.numel() * 4
+
+    def e2e_step(self, q, i):
+        self.A.copy_(self.hA, non_blocking=True)
+        self.step(q, i)
+        self.hX.copy_(self.inv, non_blocking=True)
+        self.hI.copy_(self.info, non_blocking=True)
+
+    def cpu_reference(self, seconds=10.0, nthreads=None):
+        import oracle
+
+        done, t_total = 0, 0.0
+        while t_total < seconds:
+            A = self.A_np.copy()
+            t0 = time.perf_counter()
+            oracle.lapack_dgetri_batched(A, nthreads=nthreads)
+            t_total += time.perf_counter() - t0
+            done += self.batch
+        return done / t_total, done, (nthreads or oracle.max_threads()), \
+            f"{done} inverses (10,000-instance batches, same inputs); LAPACK dgetrf + dgetri (OpenBLAS 0.3.30, " \
+            f"scipy) in an OpenMP loop, 1 BLAS thread each"
+
+
+class NopivBatched:
+    """LU without pivoting + solve, 10,000 x (32x32), 1 RHS (magma_dgesv_nopiv_batched), with
+    the random-butterfly solve (magma_dgesv_rbt_batched) on the same inputs as the second arm."""
+    name = "nopiv_dgesv_nopiv_batched_10000x32_nrhs1"
+    unit = "solves/s"
+    dtype = "f64"
+    metric = "gesv_nopiv_batched solves/s (FP64; gesv_rbt_batched beside)"
+    data = "synthetic: seeded U[-1,1] (splitmix64) + 32 on the diagonal (no pivoting needed)"
+    alt_name = "rbt"
+
+    def __init__(self, dev, batch=10000, n=32, nrhs=1, seed=9):
+        import torch
+
+        from magma_b200 import testing as T
+        from magma_b200.api import ptr_array
+
+        self.torch, self.dev, self.batch, self.n, self.nrhs = torch, dev, batch, n, nrhs
+        self.A_np, self.B_np = T.lu_uniform(batch, n, nrhs, seed=seed)
+        for i in range(n):
+            self.A_np[:, i, i] += n
+        self.A0 = torch.from_numpy(self.A_np).to(dev)
+        self.B0 = torch.from_numpy(self.B_np).to(dev)
+        self.A, self.B = torch.empty_like(self.A0), torch.empty_like(self.B0)
+        self.info = torch.zeros(batch, dtype=torch.int32, device=dev)
+        self.pA, self.pB = ptr_array(self.A), ptr_array(self.B)
+        self.flush = _Flush(torch, dev)
+        self.l2 = "A, B restored, then a 252 MiB buffer written (L2 flushed) between steps"
+
+    def units(self):
+        return self.batch
+
+    def config_extra(self):
+        return {"n": self.n, "nrhs": self.nrhs}
+
+    def bytes_per_unit(self):
+        n, r = self.n, self.nrhs
+        return 2 * 8 * n * n + 2 * 8 * n * r + 4
+
+    def launches_per_step(self):
+        return 1
+
+    def restore(self, i):
+        self.A.copy_(self.A0)
+        self.B.copy_(self.B0)
+        self.flush()
+
+    restore_alt = restore
+
+    def step(self, q, i):
+        return q.lib.magma_dgesv_nopiv_batched(self.n, self.nrhs, vp(self.pA), self.n, vp(self.pB), self.n,
+                                               vp(self.info), self.batch, q.handle)
+
+    def step_alt(self, q, i):
+        return q.lib.magma_dgesv_rbt_batched(self.n, self.nrhs, vp(self.pA), self.n, vp(self.pB), self.n,
+                                             vp(self.info), self.batch, q.handle)
+
+    def ratios(self, value, alt_value):
+        return {"rbt_over_nopiv": alt_value / value}
+
+    def validate(self, q):
+        from magma_b200 import testing as T
+
+        out = {}
+        for tag, fn in (("nopiv", self.step), ("rbt", self.step_alt)):
+            self.restore(0)
+            fn(q, 0)
+            q.sync()
+            out[f"bwd_err_max_{tag}"] = float(T.backward_error(self.A_np, self.B.cpu().numpy(), self.B_np,
+                                                               self.n).max())
+        return out
+
+    def dominant_kernel(self, q, stream, reps=50):
+        ms = timed_restore(stream, lambda i: self.step(q, i), self.restore, reps) / reps
+        return {"kernel": "gesv_small_kernel<double,32,1,1> (no pivoting)", "ms": ms,
+                "alg_bytes": self.bytes_per_unit() * self.batch, "tflops": None}
+
+    def e2e_setup(self):
+        t = self.torch
+        self.hA = t.from_numpy(self.A_np).pin_memory()
+        self.hB = t.from_numpy(self.B_np).pin_memory()
+        self.hX = t.empty_like(self.hB).pin_memory()
+        self.hI = t.empty(self.batch, dtype=t.int32).pin_memory()
+        self.h2d = self.hA.numel() * 8 + self.hB.numel() * 8
+        self.d2h = self.hX.numel() * 8 + self.hI.numel() * 4
+
+    def e2e_step(self, q, i):
+        self.A.copy_(self.hA, non_blocking=True)
+        self.B.copy_(self.hB, non_blocking=True)
+        self.step(q, i)
+        self.hX.copy_(self.B, non_blocking=True)
+        self.hI.copy_(self.info, non_blocking=True)
+
+    def cpu_reference(self, seconds=10.0, nthreads=None):
+        import oracle
+
+        done, t_total = 0, 0.0
+        while t_total < seconds:
+            A, B = self.A_np.copy(), self.B_np.copy()
+            t0 = time.perf_counter()
+            oracle.lapack_dgesv_batched(A, B, nthreads=nthreads)
+            t_total += time.perf_counter() - t0
+            done += self.batch
+        return done / t_total, done, (nthreads or oracle.max_threads()), \
+            f"{done} solves (10,000-instance batches, same inputs); LAPACK dgesv (OpenBLAS 0.3.30, scipy; " \
+            f"the CPU check of testing_zgesv_nopiv_batched.cpp) in an OpenMP loop, 1 BLAS thread each"
+
+
+WORKLOADS = {"c3": C3Mixed, "c1": C1DgesvSmall, "c2": C2GemmVbatched, "c4": C4CholVbatched, "qr": QrBatched, "getri": GetriBatched,
+             "nopiv": NopivBatched}
+DEFAULT_STEPS = {"c3": (60, 5), "c1": (20000, 50), "c2": (50, 5), "c4": (20, 3), "c5": (3000, 200), "qr": (200, 5), "getri": (200, 5), "nopiv": (200, 5)}
 
 
 # ---------------------------------------------------------------------- main
@@ -857,9 +1076,9 @@ def run_reference(args, rank):
     from magma_b200 import testing as T
 
     nthreads = oracle.max_threads()
-    if args.workload not in ("c1", "c3", "qr"):
-        print(json.dumps({"impl": "reference", "unavailable": "the reference arm covers the c1, c3 and qr "
-                          "workloads; c2/c4 report their CPU LAPACK loop as cpu_baseline"}), flush=True)
+    if args.workload not in ("c1", "c3", "qr", "getri", "nopiv"):
+        print(json.dumps({"impl": "reference", "unavailable": "the reference arm covers the c1, c3, qr, getri "
+                          "and nopiv workloads; c2/c4 report their CPU LAPACK loop as cpu_baseline"}), flush=True)
         return
     metric, unit = METRIC, "solves/s"
     # each step gets fresh copies of the inputs, made outside the timed call
@@ -871,6 +1090,24 @@ def run_reference(args, rank):
         desc = f"{sample} instances per step (256x256, kappa in [1e2,1e6], 4 RHS); LAPACK dsgesv"
         cfg = {"workload": "c3_dsgesv_batched_2048x256_kappa1e2-1e6_nrhs4", "batch": sample, "n": 256, "nrhs": 4}
         dtype = C3Mixed.dtype
+    elif args.workload == "getri":
+        sample = 10000
+        A0, _ = T.lu_uniform(sample, 32, 1, seed=8)
+        prep = lambda: (A0.copy(), None)   # noqa: E731
+        fn = lambda a, b: oracle.lapack_dgetri_batched(a, nthreads=nthreads)   # noqa: E731
+        desc = f"{sample} instances per step (32x32); LAPACK dgetrf + dgetri"
+        cfg = {"workload": GetriBatched.name, "batch": sample, "n": 32}
+        dtype, metric, unit = GetriBatched.dtype, GetriBatched.metric, GetriBatched.unit
+    elif args.workload == "nopiv":
+        sample = 10000
+        A0, B0 = T.lu_uniform(sample, 32, 1, seed=9)
+        for i in range(32):
+            A0[:, i, i] += 32
+        prep = lambda: (A0.copy(), B0.copy())   # noqa: E731
+        fn = lambda a, b: oracle.lapack_dgesv_batched(a, b, nthreads=nthreads)   # noqa: E731
+        desc = f"{sample} instances per step (32x32 diagonally dominant, 1 RHS); LAPACK dgesv"
+        cfg = {"workload": NopivBatched.name, "batch": sample, "n": 32, "nrhs": 1}
+        dtype, metric, unit = NopivBatched.dtype, NopivBatched.metric, NopivBatched.unit
     elif args.workload == "qr":
         sample = 10000
         A0, _ = T.lu_uniform(sample, 64, 1, seed=6)

@@ -189,6 +189,16 @@ def lapack_dgeqrf_batched(A: np.ndarray, m: int, nthreads: int | None = None):
     return tau
 
 
+def lapack_dgetri_batched(A: np.ndarray, nthreads: int | None = None):
+    """LAPACK dgetrf + dgetri per instance, in place (A becomes inv(A)); returns (ipiv, info)."""
+    batch, n, lda = A.shape
+    ipiv = np.zeros((batch, n), np.int32)
+    info = np.zeros(batch, np.int32)
+    _lapack().ref_dgetri_batched(n, _d(A), lda, C.c_long(n * lda), _i(ipiv), C.c_long(n), _i(info), batch,
+                                 nthreads or max_threads())
+    return ipiv, info
+
+
 def lapack_dsgesv_batched(A: np.ndarray, B: np.ndarray, nthreads: int | None = None):
     """LAPACK dsgesv per instance; returns (X, ipiv, iter, info)."""
     batch, n, lda = A.shape

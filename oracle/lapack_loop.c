@@ -31,6 +31,7 @@ typedef void (*sgemm_t)(const char*, const char*, const int*, const int*, const 
 typedef void (*dsgesv_t)(const int*, const int*, double*, const int*, int*, const double*, const int*,
                          double*, const int*, double*, float*, int*, int*);
 typedef void (*geqrf_t)(const int*, const int*, double*, const int*, double*, double*, const int*, int*);
+typedef void (*getri_t)(const int*, double*, const int*, const int*, double*, const int*, int*);
 typedef void (*setthreads_t)(int);
 
 static getrf_t p_dgetrf;
@@ -42,6 +43,7 @@ static dgemm_t p_dgemm;
 static sgemm_t p_sgemm;
 static dsgesv_t p_dsgesv;
 static geqrf_t p_dgeqrf;
+static getri_t p_dgetri;
 static setthreads_t p_setthreads;
 
 /* Returns 0 on success, -1 if the library or a symbol is missing. */
@@ -57,9 +59,10 @@ int lapack_loop_init(const char* path) {
     p_sgemm = (sgemm_t)dlsym(h, "scipy_sgemm_");
     p_dsgesv = (dsgesv_t)dlsym(h, "scipy_dsgesv_");
     p_dgeqrf = (geqrf_t)dlsym(h, "scipy_dgeqrf_");
+    p_dgetri = (getri_t)dlsym(h, "scipy_dgetri_");
     p_setthreads = (setthreads_t)dlsym(h, "scipy_openblas_set_num_threads");
     if (!p_dgetrf || !p_dgetrs || !p_dgesv || !p_dpotrf || !p_dpotrs || !p_dgemm || !p_sgemm ||
-        !p_dsgesv || !p_dgeqrf || !p_setthreads)
+        !p_dsgesv || !p_dgeqrf || !p_dgetri || !p_setthreads)
         return -1;
     p_setthreads(1);
     return 0;
@@ -156,6 +159,22 @@ void ref_dgeqrf_batched(int m, int n, double* A, int lda, long sA, double* tau, 
         for (int i = 0; i < batch; ++i) {
             int info = 0;
             p_dgeqrf(&m, &n, A + (size_t)i * sA, &lda, tau + (size_t)i * sT, work, &lwork, &info);
+        }
+    }
+}
+
+/* dgetrf + dgetri per instance, in place (testing_zgetri_batched.cpp:140-160). */
+void ref_dgetri_batched(int n, double* A, int lda, long sA, int* ipiv, long sP, int* info, int batch,
+                        int nthreads) {
+#pragma omp parallel num_threads(nthreads)
+    {
+        int lwork = 64 * (n > 0 ? n : 1);
+        double* work = (double*)__builtin_alloca(sizeof(double) * (size_t)lwork);
+#pragma omp for schedule(dynamic)
+        for (int i = 0; i < batch; ++i) {
+            p_dgetrf(&n, &n, A + (size_t)i * sA, &lda, ipiv + (size_t)i * sP, info + i);
+            int inf2 = 0;
+            if (info[i] == 0) p_dgetri(&n, A + (size_t)i * sA, &lda, ipiv + (size_t)i * sP, work, &lwork, &inf2);
         }
     }
 }

@@ -166,3 +166,12 @@ def test_oracle_geqr2_matches_reference_loop():
     t2 = oracle.lapack_dgeqrf_batched(G2, m, nthreads=2)
     assert np.abs(G1 - G2).max() < 64 * m * EPS
     assert np.abs(t1 - t2).max() < 64 * m * EPS
+
+
+def test_reference_loop_getri_is_the_inverse():
+    A, _ = T.lu_uniform(50, 24, 1, seed=5)
+    X = A.copy()
+    ipiv, info = oracle.lapack_dgetri_batched(X, nthreads=2)
+    assert np.all(info == 0)
+    for b in range(50):
+        assert np.abs(A[b].T @ X[b].T - np.eye(24)).max() < 1e-10
