@@ -433,6 +433,112 @@ void magmablas_sgemm_vbatched_nocheck(magma_trans_t transA, magma_trans_t transB
                                       float const* const* dB_array, magma_int_t* lddb, float beta, float** dC_array,
                                       magma_int_t* lddc, magma_int_t batchCount, magma_queue_t queue);
 
+/* Variable-size SYRK on one triangle: C = alpha op(A) op(A)^T + beta C (uplo part only).
+ * include/magma_zvbatched.h:202-243, magmablas/zsyrk_vbatched.cpp; checks as
+ * magmablas/vbatched_check.cu:186-262 (uplo -1, trans -2, n -3, k -4, ldda -7,
+ * lddc -10, batchCount -11). n, k, ldda, lddc: device arrays of batchCount+1 entries. */
+void magmablas_dsyrk_vbatched(magma_uplo_t uplo, magma_trans_t trans, magma_int_t* n, magma_int_t* k, double alpha,
+                              double const* const* dA_array, magma_int_t* ldda, double beta, double** dC_array,
+                              magma_int_t* lddc, magma_int_t batchCount, magma_queue_t queue);
+void magmablas_dsyrk_vbatched_max_nocheck(magma_uplo_t uplo, magma_trans_t trans, magma_int_t* n, magma_int_t* k,
+                                          double alpha, double const* const* dA_array, magma_int_t* ldda,
+                                          double beta, double** dC_array, magma_int_t* lddc, magma_int_t batchCount,
+                                          magma_int_t max_n, magma_int_t max_k, magma_queue_t queue);
+void magmablas_dsyrk_vbatched_max(magma_uplo_t uplo, magma_trans_t trans, magma_int_t* n, magma_int_t* k,
+                                  double alpha, double const* const* dA_array, magma_int_t* ldda, double beta,
+                                  double** dC_array, magma_int_t* lddc, magma_int_t batchCount, magma_int_t max_n,
+                                  magma_int_t max_k, magma_queue_t queue);
+void magmablas_dsyrk_vbatched_nocheck(magma_uplo_t uplo, magma_trans_t trans, magma_int_t* n, magma_int_t* k,
+                                      double alpha, double const* const* dA_array, magma_int_t* ldda, double beta,
+                                      double** dC_array, magma_int_t* lddc, magma_int_t batchCount,
+                                      magma_queue_t queue);
+void magmablas_ssyrk_vbatched(magma_uplo_t uplo, magma_trans_t trans, magma_int_t* n, magma_int_t* k, float alpha,
+                              float const* const* dA_array, magma_int_t* ldda, float beta, float** dC_array,
+                              magma_int_t* lddc, magma_int_t batchCount, magma_queue_t queue);
+void magmablas_ssyrk_vbatched_max_nocheck(magma_uplo_t uplo, magma_trans_t trans, magma_int_t* n, magma_int_t* k,
+                                          float alpha, float const* const* dA_array, magma_int_t* ldda, float beta,
+                                          float** dC_array, magma_int_t* lddc, magma_int_t batchCount,
+                                          magma_int_t max_n, magma_int_t max_k, magma_queue_t queue);
+void magmablas_ssyrk_vbatched_max(magma_uplo_t uplo, magma_trans_t trans, magma_int_t* n, magma_int_t* k,
+                                  float alpha, float const* const* dA_array, magma_int_t* ldda, float beta,
+                                  float** dC_array, magma_int_t* lddc, magma_int_t batchCount, magma_int_t max_n,
+                                  magma_int_t max_k, magma_queue_t queue);
+void magmablas_ssyrk_vbatched_nocheck(magma_uplo_t uplo, magma_trans_t trans, magma_int_t* n, magma_int_t* k,
+                                      float alpha, float const* const* dA_array, magma_int_t* ldda, float beta,
+                                      float** dC_array, magma_int_t* lddc, magma_int_t batchCount,
+                                      magma_queue_t queue);
+
+/* Variable-size triangular solve op(A) X = alpha B / X op(A) = alpha B (X overwrites B)
+ * and triangular multiply B = alpha op(A) B / alpha B op(A).
+ * include/magma_zvbatched.h:324-450, magmablas/ztrsm_vbatched.cpp:21-215,
+ * magmablas/ztrmm_vbatched.cpp:21-90; checks as magmablas/vbatched_check.cu:134-181 and
+ * :785-833 (side -1, uplo -2, transA -3, diag -4, m -5, n -6, ldda -9, lddb -11,
+ * batchCount -12). m, n, ldda, lddb: device arrays of batchCount+1 entries. */
+void magmablas_dtrsm_vbatched(magma_side_t side, magma_uplo_t uplo, magma_trans_t transA, magma_diag_t diag,
+                              magma_int_t* m, magma_int_t* n, double alpha, double** dA_array, magma_int_t* ldda,
+                              double** dB_array, magma_int_t* lddb, magma_int_t batchCount, magma_queue_t queue);
+void magmablas_dtrsm_vbatched_max_nocheck(magma_side_t side, magma_uplo_t uplo, magma_trans_t transA,
+                                          magma_diag_t diag, magma_int_t* m, magma_int_t* n, double alpha,
+                                          double** dA_array, magma_int_t* ldda, double** dB_array, magma_int_t* lddb,
+                                          magma_int_t batchCount, magma_int_t max_m, magma_int_t max_n,
+                                          magma_queue_t queue);
+void magmablas_dtrsm_vbatched_max(magma_side_t side, magma_uplo_t uplo, magma_trans_t transA, magma_diag_t diag,
+                                  magma_int_t* m, magma_int_t* n, double alpha, double** dA_array, magma_int_t* ldda,
+                                  double** dB_array, magma_int_t* lddb, magma_int_t batchCount, magma_int_t max_m,
+                                  magma_int_t max_n, magma_queue_t queue);
+void magmablas_dtrsm_vbatched_nocheck(magma_side_t side, magma_uplo_t uplo, magma_trans_t transA, magma_diag_t diag,
+                                      magma_int_t* m, magma_int_t* n, double alpha, double** dA_array,
+                                      magma_int_t* ldda, double** dB_array, magma_int_t* lddb,
+                                      magma_int_t batchCount, magma_queue_t queue);
+void magmablas_strsm_vbatched(magma_side_t side, magma_uplo_t uplo, magma_trans_t transA, magma_diag_t diag,
+                              magma_int_t* m, magma_int_t* n, float alpha, float** dA_array, magma_int_t* ldda,
+                              float** dB_array, magma_int_t* lddb, magma_int_t batchCount, magma_queue_t queue);
+void magmablas_strsm_vbatched_max_nocheck(magma_side_t side, magma_uplo_t uplo, magma_trans_t transA,
+                                          magma_diag_t diag, magma_int_t* m, magma_int_t* n, float alpha,
+                                          float** dA_array, magma_int_t* ldda, float** dB_array, magma_int_t* lddb,
+                                          magma_int_t batchCount, magma_int_t max_m, magma_int_t max_n,
+                                          magma_queue_t queue);
+void magmablas_strsm_vbatched_max(magma_side_t side, magma_uplo_t uplo, magma_trans_t transA, magma_diag_t diag,
+                                  magma_int_t* m, magma_int_t* n, float alpha, float** dA_array, magma_int_t* ldda,
+                                  float** dB_array, magma_int_t* lddb, magma_int_t batchCount, magma_int_t max_m,
+                                  magma_int_t max_n, magma_queue_t queue);
+void magmablas_strsm_vbatched_nocheck(magma_side_t side, magma_uplo_t uplo, magma_trans_t transA, magma_diag_t diag,
+                                      magma_int_t* m, magma_int_t* n, float alpha, float** dA_array,
+                                      magma_int_t* ldda, float** dB_array, magma_int_t* lddb, magma_int_t batchCount,
+                                      magma_queue_t queue);
+void magmablas_dtrmm_vbatched(magma_side_t side, magma_uplo_t uplo, magma_trans_t transA, magma_diag_t diag,
+                              magma_int_t* m, magma_int_t* n, double alpha, double** dA_array, magma_int_t* ldda,
+                              double** dB_array, magma_int_t* lddb, magma_int_t batchCount, magma_queue_t queue);
+void magmablas_dtrmm_vbatched_max_nocheck(magma_side_t side, magma_uplo_t uplo, magma_trans_t transA,
+                                          magma_diag_t diag, magma_int_t* m, magma_int_t* n, double alpha,
+                                          double** dA_array, magma_int_t* ldda, double** dB_array, magma_int_t* lddb,
+                                          magma_int_t batchCount, magma_int_t max_m, magma_int_t max_n,
+                                          magma_queue_t queue);
+void magmablas_dtrmm_vbatched_max(magma_side_t side, magma_uplo_t uplo, magma_trans_t transA, magma_diag_t diag,
+                                  magma_int_t* m, magma_int_t* n, double alpha, double** dA_array, magma_int_t* ldda,
+                                  double** dB_array, magma_int_t* lddb, magma_int_t batchCount, magma_int_t max_m,
+                                  magma_int_t max_n, magma_queue_t queue);
+void magmablas_dtrmm_vbatched_nocheck(magma_side_t side, magma_uplo_t uplo, magma_trans_t transA, magma_diag_t diag,
+                                      magma_int_t* m, magma_int_t* n, double alpha, double** dA_array,
+                                      magma_int_t* ldda, double** dB_array, magma_int_t* lddb,
+                                      magma_int_t batchCount, magma_queue_t queue);
+void magmablas_strmm_vbatched(magma_side_t side, magma_uplo_t uplo, magma_trans_t transA, magma_diag_t diag,
+                              magma_int_t* m, magma_int_t* n, float alpha, float** dA_array, magma_int_t* ldda,
+                              float** dB_array, magma_int_t* lddb, magma_int_t batchCount, magma_queue_t queue);
+void magmablas_strmm_vbatched_max_nocheck(magma_side_t side, magma_uplo_t uplo, magma_trans_t transA,
+                                          magma_diag_t diag, magma_int_t* m, magma_int_t* n, float alpha,
+                                          float** dA_array, magma_int_t* ldda, float** dB_array, magma_int_t* lddb,
+                                          magma_int_t batchCount, magma_int_t max_m, magma_int_t max_n,
+                                          magma_queue_t queue);
+void magmablas_strmm_vbatched_max(magma_side_t side, magma_uplo_t uplo, magma_trans_t transA, magma_diag_t diag,
+                                  magma_int_t* m, magma_int_t* n, float alpha, float** dA_array, magma_int_t* ldda,
+                                  float** dB_array, magma_int_t* lddb, magma_int_t batchCount, magma_int_t max_m,
+                                  magma_int_t max_n, magma_queue_t queue);
+void magmablas_strmm_vbatched_nocheck(magma_side_t side, magma_uplo_t uplo, magma_trans_t transA, magma_diag_t diag,
+                                      magma_int_t* m, magma_int_t* n, float alpha, float** dA_array,
+                                      magma_int_t* ldda, float** dB_array, magma_int_t* lddb, magma_int_t batchCount,
+                                      magma_queue_t queue);
+
 #ifdef __cplusplus
 }
 #endif

@@ -13,13 +13,14 @@ from . import _lib
 from .api import (Queue, VarBatch, ptr_array, dgetrf_batched, dgetrs_batched, dgesv_batched, dpotrf_batched,
                   dpotrs_batched, dposv_batched, dposv_vbatched, dsgesv_batched,
                   dgesv_vbatched, dsposv_vbatched, dgetri_outofplace_batched, dgetrf_nopiv_batched,
-                  dgetrs_nopiv_batched, dgesv_nopiv_batched, dgerbt_batched, dgesv_rbt_batched, dgeqrf_batched, gemm_batched,
+                  dgetrs_nopiv_batched, dgesv_nopiv_batched, dgerbt_batched, dgesv_rbt_batched, dgeqrf_batched, gemm_batched, syrk_vbatched,
+                  tri_vbatched,
                   gemm_vbatched)
 
 __all__ = ["Queue", "VarBatch", "ptr_array", "dgetrf_batched", "dgetrs_batched", "dgesv_batched", "dpotrf_batched",
            "dpotrs_batched", "dposv_batched", "dposv_vbatched", "dsgesv_batched", "dgesv_vbatched", "dsposv_vbatched", "dgetri_outofplace_batched",
            "dgetrf_nopiv_batched", "dgetrs_nopiv_batched", "dgesv_nopiv_batched", "dgerbt_batched",
-           "dgesv_rbt_batched", "dgeqrf_batched", "gemm_batched",
+           "dgesv_rbt_batched", "dgeqrf_batched", "gemm_batched", "syrk_vbatched", "tri_vbatched",
            "gemm_vbatched", "load"]
 
 

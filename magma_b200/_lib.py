@@ -105,6 +105,30 @@ SIGNATURES: dict[str, tuple] = {
                                                     _i, _p]),
     "magmablas_sgemm_vbatched_max": (None, [_i, _i, _p, _p, _p, _f, _p, _p, _p, _p, _f, _p, _p, _i, _i, _i, _i, _p]),
     "magmablas_sgemm_vbatched_nocheck": (None, [_i, _i, _p, _p, _p, _f, _p, _p, _p, _p, _f, _p, _p, _i, _p]),
+    "magmablas_dsyrk_vbatched": (None, [_i, _i, _p, _p, _d, _p, _p, _d, _p, _p, _i, _p]),
+    "magmablas_dsyrk_vbatched_max_nocheck": (None, [_i, _i, _p, _p, _d, _p, _p, _d, _p, _p, _i, _i, _i, _p]),
+    "magmablas_dsyrk_vbatched_max": (None, [_i, _i, _p, _p, _d, _p, _p, _d, _p, _p, _i, _i, _i, _p]),
+    "magmablas_dsyrk_vbatched_nocheck": (None, [_i, _i, _p, _p, _d, _p, _p, _d, _p, _p, _i, _p]),
+    "magmablas_ssyrk_vbatched": (None, [_i, _i, _p, _p, _f, _p, _p, _f, _p, _p, _i, _p]),
+    "magmablas_ssyrk_vbatched_max_nocheck": (None, [_i, _i, _p, _p, _f, _p, _p, _f, _p, _p, _i, _i, _i, _p]),
+    "magmablas_ssyrk_vbatched_max": (None, [_i, _i, _p, _p, _f, _p, _p, _f, _p, _p, _i, _i, _i, _p]),
+    "magmablas_ssyrk_vbatched_nocheck": (None, [_i, _i, _p, _p, _f, _p, _p, _f, _p, _p, _i, _p]),
+    "magmablas_dtrsm_vbatched": (None, [_i, _i, _i, _i, _p, _p, _d, _p, _p, _p, _p, _i, _p]),
+    "magmablas_dtrsm_vbatched_max_nocheck": (None, [_i, _i, _i, _i, _p, _p, _d, _p, _p, _p, _p, _i, _i, _i, _p]),
+    "magmablas_dtrsm_vbatched_max": (None, [_i, _i, _i, _i, _p, _p, _d, _p, _p, _p, _p, _i, _i, _i, _p]),
+    "magmablas_dtrsm_vbatched_nocheck": (None, [_i, _i, _i, _i, _p, _p, _d, _p, _p, _p, _p, _i, _p]),
+    "magmablas_strsm_vbatched": (None, [_i, _i, _i, _i, _p, _p, _f, _p, _p, _p, _p, _i, _p]),
+    "magmablas_strsm_vbatched_max_nocheck": (None, [_i, _i, _i, _i, _p, _p, _f, _p, _p, _p, _p, _i, _i, _i, _p]),
+    "magmablas_strsm_vbatched_max": (None, [_i, _i, _i, _i, _p, _p, _f, _p, _p, _p, _p, _i, _i, _i, _p]),
+    "magmablas_strsm_vbatched_nocheck": (None, [_i, _i, _i, _i, _p, _p, _f, _p, _p, _p, _p, _i, _p]),
+    "magmablas_dtrmm_vbatched": (None, [_i, _i, _i, _i, _p, _p, _d, _p, _p, _p, _p, _i, _p]),
+    "magmablas_dtrmm_vbatched_max_nocheck": (None, [_i, _i, _i, _i, _p, _p, _d, _p, _p, _p, _p, _i, _i, _i, _p]),
+    "magmablas_dtrmm_vbatched_max": (None, [_i, _i, _i, _i, _p, _p, _d, _p, _p, _p, _p, _i, _i, _i, _p]),
+    "magmablas_dtrmm_vbatched_nocheck": (None, [_i, _i, _i, _i, _p, _p, _d, _p, _p, _p, _p, _i, _p]),
+    "magmablas_strmm_vbatched": (None, [_i, _i, _i, _i, _p, _p, _f, _p, _p, _p, _p, _i, _p]),
+    "magmablas_strmm_vbatched_max_nocheck": (None, [_i, _i, _i, _i, _p, _p, _f, _p, _p, _p, _p, _i, _i, _i, _p]),
+    "magmablas_strmm_vbatched_max": (None, [_i, _i, _i, _i, _p, _p, _f, _p, _p, _p, _p, _i, _i, _i, _p]),
+    "magmablas_strmm_vbatched_nocheck": (None, [_i, _i, _i, _i, _p, _p, _f, _p, _p, _p, _p, _i, _p]),
     "magma_dsposv_vbatched": (_i, [_i, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _i, _p]),
     "magma_dsposv_vbatched_max_nocheck": (_i, [_i, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _i, _i, _i, _p]),
     # kernel-variant tuning

@@ -14,7 +14,7 @@ import ctypes as C
 import torch
 
 from . import _lib
-from ._lib import MagmaNoTrans, MagmaTrans
+from ._lib import MagmaLeft, MagmaNonUnit, MagmaNoTrans, MagmaRight, MagmaTrans, MagmaUnit
 
 
 class Queue:
@@ -466,3 +466,36 @@ def dgeqrf_batched(A: torch.Tensor, m: int | None = None, queue: Queue | None = 
     _check(q.lib.magma_dgeqrf_batched(m, n, _vp(pA), lda, _vp(pT), _vp(info), batch, q.handle),
            "magma_dgeqrf_batched")
     return tau
+
+
+def syrk_vbatched(A: "VarBatch", C: "VarBatch", n, k, lda, ldc, alpha=1.0, beta=0.0, lower=True, trans=False,
+                  max_sizes=None, checked=True, queue: Queue | None = None) -> None:
+    """Variable-size SYRK through magmablas_{d,s}syrk_vbatched{,_max_nocheck,_nocheck}."""
+    q = queue or default_queue()
+    pre = "d" if C.buf.dtype == torch.float64 else "s"
+    dn, dk, dla, dlc = C.ints(n), C.ints(k), C.ints(lda), C.ints(ldc)
+    args = [MagmaLower if lower else MagmaUpper, _trans(trans), _vp(dn), _vp(dk), alpha, _vp(A.ptrs), _vp(dla),
+            beta, _vp(C.ptrs), _vp(dlc), C.batch]
+    if max_sizes:
+        getattr(q.lib, f"magmablas_{pre}syrk_vbatched_max_nocheck")(*args, *max_sizes, q.handle)
+    elif checked:
+        getattr(q.lib, f"magmablas_{pre}syrk_vbatched")(*args, q.handle)
+    else:
+        getattr(q.lib, f"magmablas_{pre}syrk_vbatched_nocheck")(*args, q.handle)
+
+
+def tri_vbatched(op: str, A: "VarBatch", B: "VarBatch", m, n, lda, ldb, alpha=1.0, left=True, lower=True,
+                 trans=False, unit=False, max_sizes=None, checked=True, queue: Queue | None = None) -> None:
+    """Variable-size TRSM (op "trsm") or TRMM (op "trmm") through magmablas_{d,s}{op}_vbatched*."""
+    q = queue or default_queue()
+    pre = "d" if B.buf.dtype == torch.float64 else "s"
+    dm, dn, dla, dlb = B.ints(m), B.ints(n), B.ints(lda), B.ints(ldb)
+    args = [MagmaLeft if left else MagmaRight, MagmaLower if lower else MagmaUpper, _trans(trans),
+            MagmaUnit if unit else MagmaNonUnit, _vp(dm), _vp(dn), alpha, _vp(A.ptrs), _vp(dla), _vp(B.ptrs),
+            _vp(dlb), B.batch]
+    if max_sizes:
+        getattr(q.lib, f"magmablas_{pre}{op}_vbatched_max_nocheck")(*args, *max_sizes, q.handle)
+    elif checked:
+        getattr(q.lib, f"magmablas_{pre}{op}_vbatched")(*args, q.handle)
+    else:
+        getattr(q.lib, f"magmablas_{pre}{op}_vbatched_nocheck")(*args, q.handle)

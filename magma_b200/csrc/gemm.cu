@@ -13,7 +13,10 @@
 // (instance, tile) pairs along grid.x sized by the bucket's edge; tiles past an
 // instance's own size exit at once.
 // Epilogue as the reference (magmablas/gemm_template_device.cuh:197-227): C is not
-// read when beta == 0.
+// read when beta == 0. SYRK (C = alpha op(A) op(A)^T + beta C on one triangle) is the
+// same kernel with B = A and the other transpose, tiles outside the triangle exiting
+// at once and the epilogue writing only the triangle (the reference's herk template,
+// magmablas/herk_template_kernel_vbatched.cuh, likewise skips those tiles).
 #include "internal.h"
 #include "vbatched.h"
 #include "tuning.h"
@@ -25,6 +28,7 @@ namespace mb200 {
 struct GemmSizes {
     int m, n, k, lda, ldb, ldc;
     const int *m_arr, *n_arr, *k_arr, *lda_arr, *ldb_arr, *ldc_arr;
+    int tri;   // 0: all of C; 1: lower triangle only (i >= j); 2: upper only (syrk)
     __device__ __forceinline__ int M(int i) const { return m_arr ? m_arr[i] : m; }
     __device__ __forceinline__ int N(int i) const { return n_arr ? n_arr[i] : n; }
     __device__ __forceinline__ int K(int i) const { return k_arr ? k_arr[i] : k; }
@@ -65,6 +69,7 @@ gemm_tile_kernel(GemmSizes g, T alpha, const T* const* __restrict__ A_arr, const
     const int i0 = (t / tiles_n) * BM, j0 = (t % tiles_n) * BN;
     const int m = g.M(id), n = g.N(id), k = g.K(id);
     if (i0 >= m || j0 >= n) return;
+    if ((g.tri == 1 && j0 > i0 + BM - 1) || (g.tri == 2 && i0 > j0 + BN - 1)) return;   // tile outside the triangle
     const int lda = g.LDA(id), ldb = g.LDB(id), ldc = g.LDC(id);
     const T* A = A_arr[id];
     const T* B = B_arr[id];
@@ -142,7 +147,7 @@ gemm_tile_kernel(GemmSizes g, T alpha, const T* const* __restrict__ A_arr, const
 #pragma unroll
         for (int i = 0; i < TM; ++i) {
             const int gi = i0 + tx + (BM / TM) * i;
-            if (gi >= m) continue;
+            if (gi >= m || (g.tri == 1 && gj > gi) || (g.tri == 2 && gi > gj)) continue;
             T* c = C + gi + (size_t)gj * ldc;
             *c = (beta == T(0)) ? alpha * acc[i][j] : alpha * acc[i][j] + beta * (*c);
         }
@@ -282,9 +287,89 @@ static int gemm_vbatched_check(magma_trans_t ta, magma_trans_t tb, int* m, int* 
     return 0;
 }
 
+// magmablas/vbatched_check.cu:186-262 (syrk checker): uplo -1, trans -2, n -3, k -4,
+// ldda -7 (ldda < rows of A), lddc -10 (lddc < n), batchCount -11.
+static int syrk_vbatched_check(magma_uplo_t uplo, magma_trans_t trans, int* n, int* k, int* lda, int* ldc,
+                               int batch, magma_queue_t queue, int mx[2]) {
+    if (uplo != MagmaUpper && uplo != MagmaLower) return -1;
+    if (bad_trans(trans)) return -2;
+    if (batch < 0) return -11;
+    mx[0] = mx[1] = 0;
+    if (batch == 0) return 0;
+    int r[6];
+    if (reduce_sizes(n, k, nullptr, batch, queue, r)) return MAGMA_ERR_UNKNOWN;
+    if (r[3] < 0) return -3;
+    if (r[4] < 0) return -4;
+    int sl = 0;
+    if (ld_slack(trans == MagmaNoTrans ? n : k, lda, batch, queue, &sl)) return MAGMA_ERR_UNKNOWN;
+    if (sl < 0) return -7;
+    if (ld_slack(n, ldc, batch, queue, &sl)) return MAGMA_ERR_UNKNOWN;
+    if (sl < 0) return -10;
+    mx[0] = r[0];
+    mx[1] = r[1];
+    return 0;
+}
+
+// magmablas/dsyrk_vbatched_core.cu:102-112: no quick return on k (k = 0 scales the
+// triangle by beta), none on n beyond an empty batch.
+template <typename T>
+static void syrk_vbatched_max_nocheck(magma_uplo_t uplo, magma_trans_t trans, int* n, int* k, T alpha,
+                                      const T* const* A, int* lda, T beta, T** C, int* ldc, int batch, int max_n,
+                                      int max_k, magma_queue_t queue) {
+    (void)max_k;
+    if (max_n <= 0 || batch <= 0) return;
+    GemmSizes g{0, 0, 0, 0, 0, 0, n, n, k, lda, lda, ldc, uplo == MagmaLower ? 1 : 2};
+    const magma_trans_t tb = (trans == MagmaNoTrans) ? MagmaTrans : MagmaNoTrans;
+    gemm_launch_var<T>(trans, tb, g, alpha, A, A, beta, C, batch, max_n, max_n, queue);
+}
+
 }  // namespace mb200
 
 using namespace mb200;
+
+#define MB200_SYRK_API(P, T)                                                                                          \
+    void magmablas_##P##syrk_vbatched_max_nocheck(magma_uplo_t uplo, magma_trans_t trans, magma_int_t* n,             \
+                                                  magma_int_t* k, T alpha, T const* const* dA_array,                  \
+                                                  magma_int_t* ldda, T beta, T** dC_array, magma_int_t* lddc,         \
+                                                  magma_int_t batchCount, magma_int_t max_n, magma_int_t max_k,       \
+                                                  magma_queue_t queue) {                                              \
+        syrk_vbatched_max_nocheck<T>(uplo, trans, n, k, alpha, dA_array, ldda, beta, dC_array, lddc, batchCount,     \
+                                     max_n, max_k, queue);                                                            \
+    }                                                                                                                 \
+    void magmablas_##P##syrk_vbatched_max(magma_uplo_t uplo, magma_trans_t trans, magma_int_t* n, magma_int_t* k,     \
+                                          T alpha, T const* const* dA_array, magma_int_t* ldda, T beta,               \
+                                          T** dC_array, magma_int_t* lddc, magma_int_t batchCount, magma_int_t max_n, \
+                                          magma_int_t max_k, magma_queue_t queue) {                                   \
+        int mx[2];                                                                                                    \
+        const int info = syrk_vbatched_check(uplo, trans, n, k, ldda, lddc, batchCount, queue, mx);                  \
+        if (info != 0) {                                                                                              \
+            magma_xerbla(__func__, -info);                                                                            \
+            return;                                                                                                   \
+        }                                                                                                             \
+        syrk_vbatched_max_nocheck<T>(uplo, trans, n, k, alpha, dA_array, ldda, beta, dC_array, lddc, batchCount,     \
+                                     max_n, max_k, queue);                                                            \
+    }                                                                                                                 \
+    void magmablas_##P##syrk_vbatched_nocheck(magma_uplo_t uplo, magma_trans_t trans, magma_int_t* n, magma_int_t* k, \
+                                              T alpha, T const* const* dA_array, magma_int_t* ldda, T beta,           \
+                                              T** dC_array, magma_int_t* lddc, magma_int_t batchCount,                \
+                                              magma_queue_t queue) {                                                  \
+        int r[6];                                                                                                     \
+        if (batchCount <= 0 || reduce_sizes(n, k, nullptr, batchCount, queue, r)) return;                            \
+        syrk_vbatched_max_nocheck<T>(uplo, trans, n, k, alpha, dA_array, ldda, beta, dC_array, lddc, batchCount,     \
+                                     r[0], r[1], queue);                                                              \
+    }                                                                                                                 \
+    void magmablas_##P##syrk_vbatched(magma_uplo_t uplo, magma_trans_t trans, magma_int_t* n, magma_int_t* k,         \
+                                      T alpha, T const* const* dA_array, magma_int_t* ldda, T beta, T** dC_array,     \
+                                      magma_int_t* lddc, magma_int_t batchCount, magma_queue_t queue) {               \
+        int mx[2];                                                                                                    \
+        const int info = syrk_vbatched_check(uplo, trans, n, k, ldda, lddc, batchCount, queue, mx);                  \
+        if (info != 0) {                                                                                              \
+            magma_xerbla(__func__, -info);                                                                            \
+            return;                                                                                                   \
+        }                                                                                                             \
+        syrk_vbatched_max_nocheck<T>(uplo, trans, n, k, alpha, dA_array, ldda, beta, dC_array, lddc, batchCount,     \
+                                     mx[0], mx[1], queue);                                                            \
+    }
 
 #define MB200_GEMM_API(P, T)                                                                                          \
     void magmablas_##P##gemm_batched(magma_trans_t ta, magma_trans_t tb, magma_int_t m, magma_int_t n, magma_int_t k, \
@@ -349,4 +434,6 @@ using namespace mb200;
 extern "C" {
 MB200_GEMM_API(d, double)
 MB200_GEMM_API(s, float)
+MB200_SYRK_API(d, double)
+MB200_SYRK_API(s, float)
 }

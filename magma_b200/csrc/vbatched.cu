@@ -47,10 +47,10 @@ __global__ void reduce_sizes_kernel(const int* __restrict__ a, const int* __rest
 // min over i of (ld[i] - rows[i]): negative when some leading dimension is too
 // small (the reference's checkers test ld < rows, vbatched_check.cu:38-40, :852)
 __global__ void ld_slack_kernel(const int* __restrict__ rows, const int* __restrict__ ld, int batch,
-                                int* __restrict__ out) {
+                                int* __restrict__ out, int at_least) {
     int mn = INT_MAX;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < batch; i += gridDim.x * blockDim.x)
-        mn = min(mn, ld[i] - rows[i]);
+        mn = min(mn, ld[i] - max(at_least, rows[i]));
     for (int off = 16; off > 0; off >>= 1) mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, off));
     if ((threadIdx.x & 31) == 0) atomicMin(out, mn);
 }
@@ -95,14 +95,23 @@ magma_int_t reduce_sizes(const int* a, const int* b, const int* c, int batch, ma
     return launch_status();
 }
 
-magma_int_t ld_slack(const int* rows, const int* ld, int batch, magma_queue_t queue, int* out) {
+static magma_int_t ld_slack_impl(const int* rows, const int* ld, int batch, magma_queue_t queue, int* out,
+                                 int at_least) {
     int* d = static_cast<int*>(queue_workspace(queue, 64));
     if (!d) return MAGMA_ERR_DEVICE_ALLOC;
     init_ints_kernel<<<1, 32, 0, queue->stream>>>(d, 1, INT_MAX, INT_MAX, 1);
-    ld_slack_kernel<<<min(ceildiv(batch, 256), 148), 256, 0, queue->stream>>>(rows, ld, batch, d);
+    ld_slack_kernel<<<min(ceildiv(batch, 256), 148), 256, 0, queue->stream>>>(rows, ld, batch, d, at_least);
     cudaMemcpyAsync(out, d, sizeof(int), cudaMemcpyDeviceToHost, queue->stream);
     cudaStreamSynchronize(queue->stream);
     return launch_status();
+}
+
+magma_int_t ld_slack(const int* rows, const int* ld, int batch, magma_queue_t queue, int* out) {
+    return ld_slack_impl(rows, ld, batch, queue, out, INT_MIN);
+}
+
+magma_int_t ld_slack1(const int* rows, const int* ld, int batch, magma_queue_t queue, int* out) {
+    return ld_slack_impl(rows, ld, batch, queue, out, 1);
 }
 
 int resident_blocks(const void* kernel, int threads, size_t smem) {

@@ -27,6 +27,8 @@ magma_int_t bucketize2(const int* key, const int* key2, int batch, const int* ed
 magma_int_t reduce_sizes(const int* a, const int* b, const int* c, int batch, magma_queue_t queue, int out[6]);
 // *out = min over i of ld[i] - rows[i]. Synchronises the queue.
 magma_int_t ld_slack(const int* rows, const int* ld, int batch, magma_queue_t queue, int* out);
+// as ld_slack with max(1, rows[i]) in place of rows[i] (the checks written ld < max(1, rows))
+magma_int_t ld_slack1(const int* rows, const int* ld, int batch, magma_queue_t queue, int* out);
 
 // Blocks of `kernel` that fit on the whole GPU at once.
 int resident_blocks(const void* kernel, int threads, size_t smem);

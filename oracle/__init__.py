@@ -123,6 +123,14 @@ def dgeqrf_batched(A: np.ndarray, m: int):
     return tau
 
 
+def dtri(solve: bool, left: bool, lower: bool, trans: bool, unit: bool, m: int, n: int, alpha: float,
+         A: np.ndarray, B: np.ndarray):
+    """trsm (solve) / trmm in the batched kernels' order, in place on one column-major
+    instance: A is (k, lda) with k = m (left) or n (right), B is (n, ldb)."""
+    lib().oracle_dtri(int(solve), int(left), int(lower), int(trans), int(unit), m, n, C.c_double(alpha), _d(A),
+                      A.shape[1], _d(B), B.shape[1])
+
+
 def dgetrs_batched(A: np.ndarray, ipiv: np.ndarray, B: np.ndarray, trans: bool = False):
     """Solve with the factors; B is (batch, nrhs, ldb), overwritten with X."""
     batch, n, lda = A.shape
@@ -240,3 +248,21 @@ def lapack_gemm_vbatched(ta, tb, ms, ns, ks, alpha, As, ldas, Bs, ldbs, beta, Cs
                                      _ptrs(As, C.c_float), _i(la), _ptrs(Bs, C.c_float), _i(lb),
                                      C.c_float(beta), _ptrs(Cs, C.c_float), _i(lc), batch,
                                      nthreads or max_threads())
+
+
+def lapack_dtri_vbatched(solve, left, lower, trans, unit, ms, ns, alpha, As, ldas, Bs, ldbs, nthreads=None):
+    """BLAS dtrsm (solve) / dtrmm per instance, in place on lists of column-major arrays."""
+    batch = len(Bs)
+    _lapack().ref_dtri_vbatched(int(solve), int(left), int(lower), int(trans), int(unit),
+                                _i(np.asarray(ms, np.int32)), _i(np.asarray(ns, np.int32)), C.c_double(alpha),
+                                _ptrs(As, C.c_double), _i(np.asarray(ldas, np.int32)), _ptrs(Bs, C.c_double),
+                                _i(np.asarray(ldbs, np.int32)), batch, nthreads or max_threads())
+
+
+def lapack_dsyrk_vbatched(lower, trans, ns, ks, alpha, As, ldas, beta, Cs, ldcs, nthreads=None):
+    """BLAS dsyrk per instance, in place on lists of column-major arrays."""
+    batch = len(Cs)
+    _lapack().ref_dsyrk_vbatched(int(lower), int(trans), _i(np.asarray(ns, np.int32)), _i(np.asarray(ks, np.int32)),
+                                 C.c_double(alpha), _ptrs(As, C.c_double), _i(np.asarray(ldas, np.int32)),
+                                 C.c_double(beta), _ptrs(Cs, C.c_double), _i(np.asarray(ldcs, np.int32)), batch,
+                                 nthreads or max_threads())

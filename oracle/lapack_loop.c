@@ -32,6 +32,10 @@ typedef void (*dsgesv_t)(const int*, const int*, double*, const int*, int*, cons
                          double*, const int*, double*, float*, int*, int*);
 typedef void (*geqrf_t)(const int*, const int*, double*, const int*, double*, double*, const int*, int*);
 typedef void (*getri_t)(const int*, double*, const int*, const int*, double*, const int*, int*);
+typedef void (*trxm_t)(const char*, const char*, const char*, const char*, const int*, const int*, const double*,
+                       const double*, const int*, double*, const int*, size_t, size_t, size_t, size_t);
+typedef void (*syrk_t)(const char*, const char*, const int*, const int*, const double*, const double*, const int*,
+                       const double*, double*, const int*, size_t, size_t);
 typedef void (*setthreads_t)(int);
 
 static getrf_t p_dgetrf;
@@ -44,6 +48,8 @@ static sgemm_t p_sgemm;
 static dsgesv_t p_dsgesv;
 static geqrf_t p_dgeqrf;
 static getri_t p_dgetri;
+static trxm_t p_dtrsm, p_dtrmm;
+static syrk_t p_dsyrk;
 static setthreads_t p_setthreads;
 
 /* Returns 0 on success, -1 if the library or a symbol is missing. */
@@ -60,9 +66,13 @@ int lapack_loop_init(const char* path) {
     p_dsgesv = (dsgesv_t)dlsym(h, "scipy_dsgesv_");
     p_dgeqrf = (geqrf_t)dlsym(h, "scipy_dgeqrf_");
     p_dgetri = (getri_t)dlsym(h, "scipy_dgetri_");
+    p_dtrsm = (trxm_t)dlsym(h, "scipy_dtrsm_");
+    p_dtrmm = (trxm_t)dlsym(h, "scipy_dtrmm_");
+    p_dsyrk = (syrk_t)dlsym(h, "scipy_dsyrk_");
     p_setthreads = (setthreads_t)dlsym(h, "scipy_openblas_set_num_threads");
     if (!p_dgetrf || !p_dgetrs || !p_dgesv || !p_dpotrf || !p_dpotrs || !p_dgemm || !p_sgemm ||
-        !p_dsgesv || !p_dgeqrf || !p_dgetri || !p_setthreads)
+        !p_dsgesv || !p_dgeqrf || !p_dgetri || !p_dtrsm || !p_dtrmm || !p_dsyrk ||
+        !p_setthreads)
         return -1;
     p_setthreads(1);
     return 0;
@@ -176,5 +186,28 @@ void ref_dgetri_batched(int n, double* A, int lda, long sA, int* ipiv, long sP, 
             int inf2 = 0;
             if (info[i] == 0) p_dgetri(&n, A + (size_t)i * sA, &lda, ipiv + (size_t)i * sP, work, &lwork, &inf2);
         }
+    }
+}
+
+/* dtrsm (solve != 0) or dtrmm per instance (testing_ztrsm_vbatched.cpp, testing_ztrmm_vbatched.cpp). */
+void ref_dtri_vbatched(int solve, int left, int lower, int trans, int unit, const int* m, const int* n, double alpha,
+                       double* const* A, const int* lda, double* const* B, const int* ldb, int batch, int nthreads) {
+    const char sd = left ? 'L' : 'R', ul = lower ? 'L' : 'U', tr = trans ? 'T' : 'N', dg = unit ? 'U' : 'N';
+#pragma omp parallel for schedule(dynamic) num_threads(nthreads)
+    for (int i = 0; i < batch; ++i) {
+        if (m[i] <= 0 || n[i] <= 0) continue;
+        if (solve) p_dtrsm(&sd, &ul, &tr, &dg, &m[i], &n[i], &alpha, A[i], &lda[i], B[i], &ldb[i], 1, 1, 1, 1);
+        else p_dtrmm(&sd, &ul, &tr, &dg, &m[i], &n[i], &alpha, A[i], &lda[i], B[i], &ldb[i], 1, 1, 1, 1);
+    }
+}
+
+/* dsyrk per instance (testing_zsyrk_vbatched.cpp). */
+void ref_dsyrk_vbatched(int lower, int trans, const int* n, const int* k, double alpha, double* const* A,
+                        const int* lda, double beta, double* const* C, const int* ldc, int batch, int nthreads) {
+    const char ul = lower ? 'L' : 'U', tr = trans ? 'T' : 'N';
+#pragma omp parallel for schedule(dynamic) num_threads(nthreads)
+    for (int i = 0; i < batch; ++i) {
+        if (n[i] <= 0) continue;
+        p_dsyrk(&ul, &tr, &n[i], &k[i], &alpha, A[i], &lda[i], &beta, C[i], &ldc[i], 1, 1);
     }
 }

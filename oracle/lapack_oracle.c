@@ -284,3 +284,52 @@ void oracle_dposv_vbatched(int upper, const int* n, const int* nrhs, double* con
         if (do_solve) oracle_dpotrs(upper, n[i], nrhs[i], A[i], lda[i], B[i], ldb[i]);
     }
 }
+
+/* Triangular solve / multiply (BLAS dtrsm / dtrmm semantics) in the batched kernels'
+ * order of operations. The call is seen as a left problem on T (nr x nr) and X
+ * (nr x nc): side Left: T = op(A), X = B; side Right: T = op(A)^T, X = B^T. Rows are
+ * renumbered q (q = i, or nr-1-i) so that T is lower in q for the solve and upper for
+ * the multiply. Per element:
+ *   solve:    s = alpha*b; s = fma(-T(q,q'), x(q'), s) for q' < q ascending; x = s * (1/T(q,q))
+ *             (unit diagonal: the reciprocal is 1);
+ *   multiply: s = 0; s = fma(T(q,q'), b(q'), s) for q' >= q ascending; x = alpha * s.
+ * BLAS itself divides by the diagonal and sums in its own order: the two agree to
+ * rounding. alpha = 0 sets X to zero. */
+void oracle_dtri(int solve, int left, int lowerA, int transA, int unit, int m, int n, double alpha,
+                 const double* A, int lda, double* B, int ldb) {
+    const int nr = left ? m : n, nc = left ? n : m;
+    const int op_lower = (lowerA != 0) != (transA != 0);
+    const int t_lower = left ? op_lower : !op_lower;
+    const int tt = left ? (transA != 0) : !(transA != 0);
+    const int bt = !left;
+    const int flip = solve ? !t_lower : t_lower;
+#define TRI_ROW(q) (flip ? nr - 1 - (q) : (q))
+#define TRI_T(q, qk) (tt ? A[TRI_ROW(qk) + (size_t)TRI_ROW(q) * lda] : A[TRI_ROW(q) + (size_t)TRI_ROW(qk) * lda])
+#define TRI_X(q, c) (*(bt ? &B[(c) + (size_t)TRI_ROW(q) * ldb] : &B[TRI_ROW(q) + (size_t)(c) * ldb]))
+    if (alpha == 0.0) {
+        for (int c = 0; c < nc; ++c)
+            for (int q = 0; q < nr; ++q) TRI_X(q, c) = 0.0;
+        return;
+    }
+    for (int c = 0; c < nc; ++c) {
+        for (int q = 0; q < nr; ++q) {
+            double s;
+            if (solve) {
+                s = alpha * TRI_X(q, c);
+                for (int qk = 0; qk < q; ++qk) s = fma(-TRI_T(q, qk), TRI_X(qk, c), s);
+                const double rcp = unit ? 1.0 : 1.0 / TRI_T(q, q);
+                TRI_X(q, c) = s * rcp;
+            } else {
+                s = 0.0;
+                for (int qk = q; qk < nr; ++qk) {
+                    const double t = (qk == q && unit) ? 1.0 : TRI_T(q, qk);
+                    s = fma(t, TRI_X(qk, c), s);
+                }
+                TRI_X(q, c) = alpha * s;
+            }
+        }
+    }
+#undef TRI_ROW
+#undef TRI_T
+#undef TRI_X
+}

@@ -175,3 +175,37 @@ def test_reference_loop_getri_is_the_inverse():
     assert np.all(info == 0)
     for b in range(50):
         assert np.abs(A[b].T @ X[b].T - np.eye(24)).max() < 1e-10
+
+
+def _tri_case(rng, solve, left, lower, trans, unit, m, n):
+    k = m if left else n
+    A = rng.uniform(-1, 1, (k, k + 3)) + np.eye(k, k + 3) * 4    # column-major (cols, lda)
+    B = rng.uniform(-1, 1, (n, m + 2))
+    return A, B
+
+
+@pytest.mark.parametrize("solve", [True, False])
+def test_oracle_tri_matches_blas(solve):
+    """The restated trsm/trmm (the kernels' order) agrees with OpenBLAS dtrsm/dtrmm to
+    rounding on all 16 side/uplo/trans/diag combinations."""
+    rng = np.random.default_rng(11)
+    for left in (True, False):
+        for lower in (True, False):
+            for trans in (True, False):
+                for unit in (True, False):
+                    m, n = 37, 21
+                    A, B = _tri_case(rng, solve, left, lower, trans, unit, m, n)
+                    B1, B2 = B.copy(), B.copy()
+                    oracle.dtri(solve, left, lower, trans, unit, m, n, 0.75, A, B1)
+                    oracle.lapack_dtri_vbatched(solve, left, lower, trans, unit, [m], [n], 0.75, [A], [A.shape[1]],
+                                                [B2], [B2.shape[1]], nthreads=1)
+                    scale = max(1.0, np.abs(B2).max())
+                    assert np.abs(B1 - B2).max() < 64 * max(m, n) * EPS * scale, (left, lower, trans, unit)
+                    assert np.array_equal(B1[:, m:], B[:, m:])      # padding rows untouched
+
+
+def test_oracle_tri_alpha_zero():
+    A = np.full((5, 5), np.nan)
+    B = np.ones((4, 5))
+    oracle.dtri(True, True, True, False, False, 5, 4, 0.0, A, B)
+    assert np.all(B == 0.0)
