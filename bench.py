@@ -22,6 +22,8 @@ Workloads (the default is the one the metric is quoted on):
   getri  LU + out-of-place inverse (getrf + getri_outofplace) on 10,000 x (32x32) (inverses/s).
   nopiv  gesv_nopiv_batched on 10,000 x (32x32) diagonally dominant, 1 RHS, with
       gesv_rbt_batched on the same inputs beside (solves/s).
+  trsm  trsm_vbatched (left, lower, no-trans, non-unit) on 20,000 instances, M, N ~ U{8..128},
+      with trmm_vbatched on the same operands beside (GFLOP/s).
 
 Timing: W untimed steps, then exactly K steps between a barrier + device
 synchronisation on both sides, measured with CUDA events on the library's
@@ -546,6 +548,147 @@ class C2GemmVbatched:
             f"loop, 1 BLAS thread each"
 
 
+class TrsmVbatched:
+    """magmablas_dtrsm_vbatched (Left, Lower, NoTrans, NonUnit) on 20,000 instances with
+    M, N ~ U{8..128}, beside magmablas_dtrmm_vbatched on the same operands."""
+    unit = "GFLOP/s"
+    dtype = "f64"
+    metric = "trsm_vbatched GFLOP/s (FP64; trmm_vbatched beside)"
+    data = "synthetic: M, N ~ U{8..128} (splitmix64), A = N(0,1)/sqrt(m) + 2 I, B ~ N(0,1) (seeded)"
+    alt_name = "trmm"
+
+    def __init__(self, dev, batch=20000, seed=12):
+        import numpy as np
+        import torch
+
+        from magma_b200 import testing as T
+
+        self.torch, self.dev, self.batch = torch, dev, batch
+        self.name = f"trsm_vbatched_{batch}_MN8-128_left_lower_notrans"
+        M, N, _ = T.gemm_sizes(batch, 8, 128, seed=seed)
+        r8 = lambda v: ((v + 7) // 8) * 8
+        self.M, self.N = M, N
+        self.lda, self.ldb = r8(M), r8(M)
+        m64 = M.astype(np.float64)
+        self.flops = float((m64 * m64 * N).sum())
+        self.bytes64 = float(8 * (m64 * (m64 + 1) / 2 + 2 * m64 * N).sum())
+        rng = np.random.default_rng(seed)
+        sa = self.lda.astype(np.int64) * M
+        sb = self.ldb.astype(np.int64) * N
+        self.offa = np.concatenate([[0], np.cumsum(sa)[:-1]])
+        self.offb = np.concatenate([[0], np.cumsum(sb)[:-1]])
+        fa = rng.standard_normal(int(sa.sum()))
+        for i in range(batch):
+            m, la = int(M[i]), int(self.lda[i])
+            blk = fa[self.offa[i]:self.offa[i] + la * m].reshape(m, la)
+            blk *= 1.0 / np.sqrt(m)
+            blk[np.arange(m), np.arange(m)] += 2.0
+        fb = rng.standard_normal(int(sb.sum()))
+        self.hA, self.hB0 = fa, fb
+        self.A = torch.from_numpy(fa).to(dev)
+        self.B0 = torch.from_numpy(fb).to(dev)
+        self.B = self.B0.clone()
+        self.pA = self.A.data_ptr() + torch.from_numpy(self.offa * 8).to(dev)
+        self.pB = self.B.data_ptr() + torch.from_numpy(self.offb * 8).to(dev)
+        ints = lambda v: torch.from_numpy(np.concatenate([v, [0]]).astype(np.int32)).to(dev)
+        self.dM, self.dN, self.dla, self.dlb = ints(M), ints(N), ints(self.lda), ints(self.ldb)
+        self.l2 = f"A+B {self.bytes64 / 2**30:.2f} GiB (FP64 triangle + B read and written) > L2; B restored between steps"
+
+    def units(self):
+        return self.flops / 1e9
+
+    def config_extra(self):
+        return {"M": "U{8..128}", "N": "U{8..128}", "ld": "roundup(M, 8)", "side": "left", "uplo": "lower",
+                "trans": "no", "diag": "non-unit", "alpha": 1.0, "gflop_per_step": self.flops / 1e9}
+
+    def launches_per_step(self):
+        return 1
+
+    def _call(self, q, fn):
+        fn(141, 122, 111, 131, vp(self.dM), vp(self.dN), 1.0, vp(self.pA), vp(self.dla), vp(self.pB), vp(self.dlb),
+           self.batch, 128, 128, q.handle)
+        return 0
+
+    def restore(self, i):
+        self.B.copy_(self.B0)
+
+    restore_alt = restore
+
+    def step(self, q, i):
+        return self._call(q, q.lib.magmablas_dtrsm_vbatched_max_nocheck)
+
+    def step_alt(self, q, i):
+        return self._call(q, q.lib.magmablas_dtrmm_vbatched_max_nocheck)
+
+    def ratios(self, value, alt_value):
+        return {"trmm_over_trsm": alt_value / value}
+
+    def validate(self, q):
+        import numpy as np
+
+        import oracle
+
+        out = {}
+        for tag, fn in (("trsm", self.step), ("trmm", self.step_alt)):
+            self.restore(0)
+            fn(q, 0)
+            q.sync()
+            got = self.B.cpu().numpy()
+            worst = 0.0
+            for i in range(0, self.batch, max(1, self.batch // 100)):
+                m, n, la, lb = int(self.M[i]), int(self.N[i]), int(self.lda[i]), int(self.ldb[i])
+                A = self.hA[self.offa[i]:self.offa[i] + la * m].reshape(m, la).copy()
+                ref = self.hB0[self.offb[i]:self.offb[i] + lb * n].reshape(n, lb).copy()
+                oracle.dtri(tag == "trsm", True, True, False, False, m, n, 1.0, A, ref)
+                g = got[self.offb[i]:self.offb[i] + lb * n].reshape(n, lb)
+                worst = max(worst, float(np.abs(g - ref).max()))
+            out[f"max_abs_diff_vs_oracle_{tag}"] = worst
+        self.restore(0)
+        return out
+
+    def dominant_kernel(self, q, stream, reps=20):
+        ms = timed_restore(stream, lambda i: self.step(q, i), self.restore, reps) / reps
+        return {"kernel": "tri_panel_kernel<double,solve> (magmablas_dtrsm_vbatched_max_nocheck)", "ms": ms,
+                "alg_bytes": self.bytes64, "tflops": self.flops / ms / 1e9}
+
+    def e2e_setup(self):
+        t = self.torch
+        self.hAp = t.from_numpy(self.hA).pin_memory()
+        self.hBp = t.from_numpy(self.hB0).pin_memory()
+        self.hX = t.empty_like(self.hBp).pin_memory()
+        self.h2d = self.hAp.numel() * 8 + self.hBp.numel() * 8
+        self.d2h = self.hX.numel() * 8
+
+    def e2e_step(self, q, i):
+        self.A.copy_(self.hAp, non_blocking=True)
+        self.B.copy_(self.hBp, non_blocking=True)
+        self.step(q, i)
+        self.hX.copy_(self.B, non_blocking=True)
+
+    def cpu_reference(self, seconds=10.0, nthreads=None, sample=4000):
+        import numpy as np
+
+        import oracle
+
+        As = [self.hA[self.offa[i]:self.offa[i] + int(self.lda[i] * self.M[i])].reshape(int(self.M[i]),
+                                                                                     int(self.lda[i]))
+              for i in range(sample)]
+        fl = float((self.M[:sample].astype(np.float64) ** 2 * self.N[:sample]).sum())
+        done, t_total = 0.0, 0.0
+        while t_total < seconds:
+            Bs = [self.hB0[self.offb[i]:self.offb[i] + int(self.ldb[i] * self.N[i])].reshape(int(self.N[i]),
+                                                                                         int(self.ldb[i])).copy()
+                  for i in range(sample)]
+            t0 = time.perf_counter()
+            oracle.lapack_dtri_vbatched(True, True, True, False, False, self.M[:sample], self.N[:sample], 1.0, As,
+                                        self.lda[:sample], Bs, self.ldb[:sample], nthreads=nthreads)
+            t_total += time.perf_counter() - t0
+            done += fl
+        return done / 1e9 / t_total, done, (nthreads or oracle.max_threads()), \
+            f"{sample}-instance slices of the same inputs, re-run; dtrsm (OpenBLAS 0.3.30, scipy) in an OpenMP " \
+            f"loop, 1 BLAS thread each"
+
+
 class C4CholVbatched:
     """Variable-size Cholesky solve on 50,000 SPD instances, n power-law on [4, 512] (exponent -1.5),
     1-8 RHS: magma_dposv_vbatched_max_nocheck (FP64) replayed as one captured CUDA graph, beside
@@ -1043,8 +1186,8 @@ class NopivBatched:
 
 
 WORKLOADS = {"c3": C3Mixed, "c1": C1DgesvSmall, "c2": C2GemmVbatched, "c4": C4CholVbatched, "qr": QrBatched, "getri": GetriBatched,
-             "nopiv": NopivBatched}
-DEFAULT_STEPS = {"c3": (60, 5), "c1": (20000, 50), "c2": (50, 5), "c4": (20, 3), "c5": (3000, 200), "qr": (200, 5), "getri": (200, 5), "nopiv": (200, 5)}
+             "nopiv": NopivBatched, "trsm": TrsmVbatched}
+DEFAULT_STEPS = {"c3": (60, 5), "c1": (20000, 50), "c2": (50, 5), "c4": (20, 3), "c5": (3000, 200), "qr": (200, 5), "getri": (200, 5), "nopiv": (200, 5), "trsm": (50, 5)}
 
 
 # ---------------------------------------------------------------------- main
