@@ -6,7 +6,8 @@
 // ipiv in reverse order. Here inv(A) = I, then the batched getrs kernels solve
 // A X = I in place with the row interchanges applied to I first: every column of
 // the result is the solve of one unit vector, so the columns are the reference's
-// U^-1 L^-1 e_i, moved to their interchanged positions. info_array receives the
+// U^-1 L^-1 e_i, moved to their interchanged positions (for n <= 32 one fused kernel,
+// getri_small_kernel, does the same operations). info_array receives the
 // 1-based index of the first exactly-zero diagonal entry of U (0 when none), the
 // condition the reference documents for its info.
 #include "internal.h"
@@ -43,6 +44,65 @@ __global__ void getri_setup_kernel(int n, double** dA_array, int ldda, double** 
     }
 }
 
+// n <= 32: one warp per matrix, lane c computes column c of inv(A) with the whole
+// column in registers and the LU factors in shared memory (broadcast reads). The
+// operations are the oracle's dgetrs on B = I, in its order: the row interchanges
+// applied to e_c (tracked as the position of its single 1), then
+//   for k ascending, i > k:   x_i = fma(-x_k, L(i,k), x_i)
+//   for k descending:         x_k = x_k / U(k,k);  i < k: x_i = fma(-x_k, U(i,k), x_i)
+// so the result is bit-identical to the getrs path (and to the oracle). Rows and
+// columns past n are padded with the identity: their terms add -0, which leaves
+// every value unchanged. The columns are staged back through shared memory so the
+// stores coalesce; info = first zero on U's diagonal, from a warp ballot.
+constexpr int kGetriWarps = 4;
+
+__global__ void __launch_bounds__(32 * kGetriWarps)
+getri_small_kernel(int n, double** dA_array, int ldda, int** dipiv_array, double** dinvA_array, int lddia,
+                   int* info_array, int batch) {
+    __shared__ double sLU[kGetriWarps][32][33];   // [warp][column][row]
+    __shared__ int sP[kGetriWarps][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    double (*L)[33] = sLU[w];
+    for (int id = blockIdx.x * kGetriWarps + w; id < batch; id += gridDim.x * kGetriWarps) {
+        const double* A = dA_array[id];
+        for (int j = 0; j < 32; ++j) L[j][lane] = (j < n && lane < n) ? A[lane + (size_t)j * ldda]
+                                                                      : (lane == j ? 1.0 : 0.0);
+        sP[w][lane] = lane < n ? dipiv_array[id][lane] - 1 : lane;
+        __syncwarp();
+        int pos = lane;
+        for (int k = 0; k < n; ++k) {
+            const int p = sP[w][k];
+            pos = (pos == k) ? p : (pos == p ? k : pos);
+        }
+        double x[32];
+#pragma unroll
+        for (int i = 0; i < 32; ++i) x[i] = (i == pos) ? 1.0 : 0.0;
+#pragma unroll
+        for (int k = 0; k < 32; ++k) {
+            const double xk = x[k];
+#pragma unroll
+            for (int i = k + 1; i < 32; ++i) x[i] = fma(-xk, L[k][i], x[i]);
+        }
+#pragma unroll
+        for (int k = 31; k >= 0; --k) {
+            x[k] = x[k] / L[k][k];
+            const double xk = x[k];
+#pragma unroll
+            for (int i = 0; i < k; ++i) x[i] = fma(-xk, L[k][i], x[i]);
+        }
+        const unsigned zero = __ballot_sync(0xffffffffu, lane < n && L[lane][lane] == 0.0);
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < 32; ++i) L[lane][i] = x[i];   // column `lane` of inv(A)
+        __syncwarp();
+        double* W = dinvA_array[id];
+        for (int j = 0; j < n; ++j)
+            if (lane < n) W[lane + (size_t)j * lddia] = L[j][lane];
+        if (info_array && lane == 0) info_array[id] = zero ? __ffs(zero) : 0;
+        __syncwarp();
+    }
+}
+
 }  // namespace mb200
 
 using namespace mb200;
@@ -64,6 +124,12 @@ magma_int_t magma_dgetri_outofplace_batched(magma_int_t n, double** dA_array, ma
     }
     if (n == 0 || batchCount <= 0) return 0;
     if (!small_lu_supported(n, n) && !blocked_lu_supported(n)) return MAGMA_ERR_NOT_SUPPORTED;
+    if (n <= 32) {
+        const int grid = std::min(ceildiv(batchCount, kGetriWarps), 65535);
+        getri_small_kernel<<<grid, 32 * kGetriWarps, 0, queue->stream>>>(n, dA_array, ldda, dipiv_array,
+                                                                        dinvA_array, lddia, info_array, batchCount);
+        return launch_status();
+    }
     getri_setup_kernel<<<std::min(batchCount, 4096), 256, 0, queue->stream>>>(n, dA_array, ldda, dinvA_array,
                                                                                lddia, info_array, batchCount);
     const WorkList wl{nullptr, nullptr, batchCount};

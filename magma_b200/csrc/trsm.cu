@@ -100,24 +100,55 @@ tri_panel_kernel(TriArgs<T> g, int panels, int batch) {
         }
         // chunks: trsm the tiles before this one, trmm this tile and the ones after it
         const int kc_begin = SOLVE ? 0 : tq, kc_end = SOLVE ? tq : ntiles;
-        for (int kc = kc_begin; kc < kc_end; ++kc) {
+        // trmm: the next chunk is fetched into registers while the current one is used;
+        // trsm loads each chunk straight into shared memory (the registers a prefetch
+        // needs cost it occupancy around its serial diagonal solves: measured slower)
+        constexpr bool PREFETCH = !SOLVE;
+        constexpr int EPT = TS * TS / kTriThreads;
+        constexpr int EPR = PREFETCH ? EPT : 1;
+        T rt[EPR], rx[EPR];
+        // element u of this thread's share of chunk kc: its T and X values
+        auto chunk_vals = [&](int kc, int u, T& tv, T& xv) {
             const int k0 = kc * TS, K = min(TS, nr - k0);
-            for (int e = tid; e < TS * TS; e += kTriThreads) {
-                const int r = TT ? e / TS : e % TS, kk = TT ? e % TS : e / TS;
-                T v = T(0);
-                if (r < R && kk < K) {
-                    const int q = q0 + r, qk = k0 + kk;
-                    if (SOLVE) v = tval(q, qk);                          // qk < q0 <= q
-                    else if (qk > q) v = tval(q, qk);
-                    else if (qk == q) v = g.unit ? T(1) : tval(q, qk);
-                }
-                sT[kk][r] = v;
+            const int e = tid + u * kTriThreads;
+            const int r = TT ? e / TS : e % TS, kk = TT ? e % TS : e / TS;
+            T v = T(0);
+            if (r < R && kk < K) {
+                const int q = q0 + r, qk = k0 + kk;
+                if (SOLVE) v = tval(q, qk);                          // qk < q0 <= q
+                else if (qk > q) v = tval(q, qk);
+                else if (qk == q) v = g.unit ? T(1) : tval(q, qk);
             }
-            for (int e = tid; e < TS * TS; e += kTriThreads) {
-                const int kk = BT ? e / TS : e % TS, c = BT ? e % TS : e / TS;
-                sX[kk][c] = (kk < K && c < C) ? *xaddr(k0 + kk, c0 + c) : T(0);
+            tv = v;
+            const int kx = BT ? e / TS : e % TS, c = BT ? e % TS : e / TS;
+            xv = (kx < K && c < C) ? *xaddr(k0 + kx, c0 + c) : T(0);
+        };
+        auto put = [&](int u, T tv, T xv) {
+            const int e = tid + u * kTriThreads;
+            sT[TT ? e % TS : e / TS][TT ? e / TS : e % TS] = tv;
+            sX[BT ? e / TS : e % TS][BT ? e % TS : e / TS] = xv;
+        };
+        if (PREFETCH && kc_begin < kc_end) {
+#pragma unroll
+            for (int u = 0; u < EPR; ++u) chunk_vals(kc_begin, u, rt[u], rx[u]);
+        }
+        for (int kc = kc_begin; kc < kc_end; ++kc) {
+            __syncthreads();   // the previous chunk's readers are done
+            if (PREFETCH) {
+#pragma unroll
+                for (int u = 0; u < EPR; ++u) put(u, rt[u], rx[u]);
+            } else {
+                for (int u = 0; u < EPT; ++u) {
+                    T tv, xv;
+                    chunk_vals(kc, u, tv, xv);
+                    put(u, tv, xv);
+                }
             }
             __syncthreads();
+            if (PREFETCH && kc + 1 < kc_end) {
+#pragma unroll
+                for (int u = 0; u < EPR; ++u) chunk_vals(kc + 1, u, rt[u], rx[u]);
+            }
 #pragma unroll 8
             for (int kk = 0; kk < TS; ++kk) {
                 T ta[4], xb[4];
@@ -131,7 +162,6 @@ tri_panel_kernel(TriArgs<T> g, int panels, int batch) {
                     for (int b = 0; b < 4; ++b) acc[a][b] = SOLVE ? fma(-ta[a], xb[b], acc[a][b])
                                                                   : fma(ta[a], xb[b], acc[a][b]);
             }
-            __syncthreads();
         }
 #pragma unroll
         for (int a = 0; a < 4; ++a)

@@ -17,7 +17,8 @@ def dev(a, cuda):
     return torch.from_numpy(np.ascontiguousarray(a)).to(cuda)
 
 
-@pytest.mark.parametrize("n,batch", [(1, 5), (8, 40), (32, 40), (63, 20), (100, 12), (256, 6), (520, 2)])
+@pytest.mark.parametrize("n,batch", [(1, 5), (3, 30), (8, 40), (17, 50), (31, 40), (32, 300), (33, 20), (63, 20),
+                                     (100, 12), (256, 6), (520, 2)])
 def test_getri_bit_identical(cuda, n, batch):
     import magma_b200 as mb
     A_np, _ = T.lu_uniform(batch, n, 1, seed=300 + n)
@@ -37,9 +38,9 @@ def test_getri_bit_identical(cuda, n, batch):
         assert np.abs(Ar @ X - np.eye(n)).max() <= 1e-9 * max(1.0, np.abs(X).max()) * n
 
 
-def test_getri_reports_zero_pivot(cuda):
+@pytest.mark.parametrize("n", [20, 40])
+def test_getri_reports_zero_pivot(cuda, n):
     import magma_b200 as mb
-    n = 40
     A_np, _ = T.lu_uniform(3, n, 1, seed=9)
     A_np[1, 7, :] = 0.0                      # zero column 7 -> U(8,8) = 0
     A = dev(A_np, cuda)
