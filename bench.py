@@ -1019,7 +1019,7 @@ class GetriBatched:
         return 3 * 8 * n * n + 4 * n + 4        # read A, write LU and inv(A), pivots, info
 
     def launches_per_step(self):
-        return 3                                # getrf, getri set-up, getrs on I
+        return 2                                # getrf, the fused inverse (n <= 32)
 
     def restore(self, i):
         self.A.copy_(self.A0)
@@ -1045,9 +1045,9 @@ class GetriBatched:
     def dominant_kernel(self, q, stream, reps=50):
         ms = timed_restore(stream, lambda i: self.step(q, i), self.restore, reps) / reps
         fl = 2 * self.n ** 3 * self.batch
-        return {"kernel": "getrf+getri (gesv_small_kernel, getri_setup_kernel, getrs_small_kernel)", "ms": ms,
+        return {"kernel": "getrf+getri (getrf_small_kernel, getri_small_kernel)", "ms": ms,
                 "alg_bytes": self.bytes_per_unit() * self.batch, "tflops": fl / (ms * 1e-3) / 1e12,
-                "alg_note": "the whole step (3 launches); 2 n^3 flops per inverse"}
+                "alg_note": "the whole step (2 launches); 2 n^3 flops per inverse"}
 
     def e2e_setup(self):
         t = self.torch
