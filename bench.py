@@ -62,6 +62,19 @@ L2_BYTES = 126 * 2**20
 FP64_NOMINAL_TFLOPS = 37.0   # B200 dense FP64 (CUDA cores / DMMA), nominal
 
 
+def host_cpu() -> dict:
+    """The host's CPU model and logical CPU count (recorded beside every CPU baseline)."""
+    model = "unknown"
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"cpu_model": model, "nproc": os.cpu_count()}
+
+
 def measured_peaks() -> dict:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -368,6 +381,25 @@ class C1DgesvSmall:
         ms = timed(stream, lambda i: self.step(q, i), reps) / reps
         return {"kernel": "gesv_small_kernel<double,32,1,1>", "ms": ms, "alg_bytes": self.bytes_per_unit() * self.batch,
                 "tflops": None}
+
+    def extras(self, q, stream, reps=50):
+        """The same steps replayed from one captured CUDA graph (one launch per ring buffer):
+        launch overhead out of the picture."""
+        t = self.torch
+        try:
+            g = t.cuda.CUDAGraph()
+            with t.cuda.graph(g, stream=stream):
+                for k in range(self.ring):
+                    assert self.step(q, k) == 0
+            g.replay()
+            t.cuda.synchronize()
+            ms = timed(stream, lambda i: g.replay(), reps) / (reps * self.ring)
+            del g
+        except Exception as e:   # reported, not fatal: the eager numbers stand on their own
+            t.cuda.synchronize()
+            return {"graph_replay": {"error": str(e)[:200]}}
+        return {"graph_replay": {"ms_per_step": ms, "solves_per_s": self.batch / (ms * 1e-3),
+                                 "steps_per_graph": self.ring}}
 
     def e2e_setup(self):
         t = self.torch
@@ -843,6 +875,42 @@ class C4CholVbatched:
         return {"kernel": "posv_vbatched (graph: potrf/potrs bucket kernels)", "ms": ms, "alg_bytes": alg,
                 "tflops": self.flops / ms / 1e9}
 
+    def extras(self, q, stream, reps=3):
+        """Per-bucket roofline: each size bucket's instances solved alone (eager calls on a
+        sub-batch of the same pointers), FP64 flops against the nominal FP64 peak and
+        compulsory bytes against the measured copy bandwidth."""
+        import numpy as np
+
+        t = self.torch
+        peaks = measured_peaks()
+        out = []
+        edges = [(4, 32), (33, 64), (65, 128), (129, 256), (257, 512)]
+        ints = lambda v: t.from_numpy(np.concatenate([v, [0]]).astype(np.int32)).to(self.dev)
+        for lo, hi in edges:
+            ids = np.nonzero((self.n >= lo) & (self.n <= hi))[0]
+            if len(ids) == 0:
+                continue
+            sel = t.from_numpy(ids).to(self.dev)
+            pA, pB = self.pA[sel].contiguous(), self.pB[sel].contiguous()
+            dn, dr = ints(self.n[ids]), ints(self.nrhs[ids])
+            info = t.zeros(len(ids) + 1, dtype=t.int32, device=self.dev)
+            mx_n, mx_r = int(self.n[ids].max()), int(self.nrhs[ids].max())
+            call = lambda i: q.lib.magma_dposv_vbatched_max_nocheck(122, vp(dn), vp(dr), vp(pA), vp(dn), vp(pB),
+                                                                    vp(dn), vp(info), len(ids), mx_n, mx_r,
+                                                                    q.handle)
+            self.restore(0)
+            call(0)
+            ms = timed_restore(stream, call, self.restore, reps) / reps
+            nv, rv = self.n[ids].astype(np.float64), self.nrhs[ids]
+            fl = float((nv ** 3 / 3.0 + nv ** 2 / 2.0 + nv / 6.0 + 2.0 * nv * nv * rv).sum())
+            by = float((16.0 * nv ** 2 + 16.0 * nv * rv + 4).sum())
+            tf, gbs = fl / (ms * 1e-3) / 1e12, by / (ms * 1e-3) / 1e9
+            out.append({"n": f"[{lo},{hi}]", "count": int(len(ids)), "ms": ms, "tflops": tf,
+                        "fp64_frac_nominal": tf / FP64_NOMINAL_TFLOPS, "gbs": gbs,
+                        "hbm_frac": gbs / peaks["hbm_gbs"], "flop_per_byte": fl / by})
+        self.restore(0)
+        return {"per_bucket": out}
+
     def e2e_setup(self):
         self.hA = self.A0.cpu().pin_memory()
         self.hB = self.B0.cpu().pin_memory()
@@ -1284,7 +1352,8 @@ def run_reference(args, rank):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype, "data": "synthetic",
         "config": cfg,
         "cpu_baseline": {"value": value, "unit": unit, "cores": nthreads, "kind": "reference",
-                         "sample": desc + " (OpenBLAS 0.3.30, scipy) in an OpenMP loop, 1 BLAS thread each"},
+                         "sample": desc + " (OpenBLAS 0.3.30, scipy) in an OpenMP loop, 1 BLAS thread each",
+                         **host_cpu()},
         "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -1415,6 +1484,7 @@ def main():
             ms_alt = timed_restore(stream, lambda i: W.step_alt(q, i), W.restore_alt, args.steps)
             extra["alt_ms_per_step"] = ms_alt / args.steps
         dom = W.dominant_kernel(q, stream)
+        extras = W.extras(q, stream) if hasattr(W, "extras") else {}
         # end to end (host buffers, copies inside each step)
         W.e2e_setup()
         ke = max(3, min(args.steps, 10 if args.workload == "c3" else 200))
@@ -1443,6 +1513,7 @@ def main():
                        "parallelism": f"replicas x{world}", "l2": W.l2},
         }
         line.update(checks)
+        line.update(extras)
         if ms_alt_total:
             alt_value = units * args.steps / (ms_alt_total * 1e-3)
             line[f"{W.alt_name}_value"] = alt_value
@@ -1476,7 +1547,7 @@ def main():
         if not args.no_cpu_baseline and world == 1:
             v, done, cores, sample = W.cpu_reference()
             line["cpu_baseline"] = {"value": v, "unit": W.unit, "cores": cores, "kind": "reference",
-                                    "sample": sample}
+                                    "sample": sample, **host_cpu()}
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()

@@ -28,7 +28,7 @@ template <typename T, int NC>
 struct CholShared {
     alignas(16) T col[2][NC];   // raw column k (double-buffered)
     alignas(16) T row[2][NC];   // row broadcast for the transposed solve
-    T rhs[2][4];
+    T rhs[2][8];                // one value per right-hand side of a group (R <= 8)
 };
 
 // Factor steps k0 .. k0+nsteps-1 on register columns 0..nsteps-1. `a` holds
@@ -70,6 +70,7 @@ __device__ __forceinline__ int chol_panel_steps(T (&a)[NC], int n, int nsteps, i
 // with row k of L published through shared memory.
 template <typename T, int NC, int NW, int R>
 __device__ __forceinline__ void chol_solve(const T (&a)[NC], int n, int tid, T (&b)[R], CholShared<T, NC>& sh) {
+    static_assert(R <= 8, "CholShared::rhs holds 8 right-hand sides a group");
     static_for<0, NC>([&](auto kc) {
         constexpr int k = decltype(kc)::value;
         if (k >= n) return;

@@ -231,6 +231,7 @@ __device__ __forceinline__ void small_lu_factor(T (&a)[NC], int m, int n, int ti
 template <typename T, int NC, int NW, int R>
 __device__ __forceinline__ void small_lu_solve(const T (&a)[NC], int n, int pos, T (&b)[R],
                                                SmallLuShared<T, NC, NW>& sh) {
+    static_assert(R <= 4, "SmallLuShared::rhs holds 4 right-hand sides a group");
     static_for<0, NC>([&](auto kc) {
         constexpr int k = decltype(kc)::value;
         if (k >= n) return;

@@ -69,6 +69,7 @@ getrf_small_kernel(WorkList wl, LuSizes sz, T** dA_array, int** ipiv_array, int*
 template <typename T, int NC, int NW, int R>
 __global__ void __launch_bounds__(32 * NW * BlockShape<NW>::MPB, MinBlocks<NC, NW>::value)
 gesv_small_kernel(WorkList wl, LuSizes sz, T** dA_array, int** ipiv_array, T** dB_array, int* info_array) {
+    static_assert(R <= 4, "the shared rhs buffer holds 4 right-hand sides a group");
     constexpr int MPB = BlockShape<NW>::MPB;
     __shared__ SmallLuShared<T, NC, NW> shm[MPB];
     const int local = (NW == 1) ? (threadIdx.x >> 5) : 0;
@@ -115,6 +116,7 @@ gesv_small_kernel(WorkList wl, LuSizes sz, T** dA_array, int** ipiv_array, T** d
 template <typename T, int NC, int NW, int R>
 __device__ __forceinline__ void permute_rhs(T (&b)[R], const int* ipiv, int n, int tid,
                                             SmallLuShared<T, NC, NW>& sh, T* xch, bool inverse) {
+    static_assert(R <= 4, "the shared rhs buffer holds 4 right-hand sides a group");
     // idx = where the entry of original row tid sits after LAPACK's DLASWP
     // (forward: k ascending; inverse: k descending). No pivots: nothing moves.
     if (!ipiv) return;
@@ -142,6 +144,7 @@ __device__ __forceinline__ void permute_rhs(T (&b)[R], const int* ipiv, int n, i
 template <typename T, int NC, int NW, int R, bool trans>
 __global__ void __launch_bounds__(32 * NW * BlockShape<NW>::MPB, MinBlocks<NC, NW>::value)
 getrs_small_kernel(WorkList wl, LuSizes sz, T** dA_array, int** ipiv_array, T** dB_array) {
+    static_assert(R <= 4, "the shared rhs buffer holds 4 right-hand sides a group");
     constexpr int MPB = BlockShape<NW>::MPB;
     __shared__ SmallLuShared<T, NC, NW> shm[MPB];
     __shared__ T xch[MPB][32 * NW];
