@@ -17,6 +17,7 @@
 #pragma once
 
 #include "small_lu.cuh"
+#include <type_traits>
 
 namespace mb200 {
 
@@ -33,11 +34,60 @@ struct CholShared {
 
 // Factor steps k0 .. k0+nsteps-1 on register columns 0..nsteps-1. `a` holds
 // this thread's row (entries of columns k0..k0+NC-1); rows are live when
-// k0 <= tid < n. Returns the 1-based failing step or 0; `done` gets the number
-// of completed steps.
+// k0 <= tid < n. Returns the 1-based failing step or 0.
+// The steps run in chunks of CK: a chunk's code is unrolled over the registers
+// from its first column on and looped over its CK steps at run time (the chunk's
+// own columns picked by selects), which keeps the kernel small enough for the
+// instruction cache; each element sees the same operations in the same order.
 template <typename T, int NC, int NW>
 __device__ __forceinline__ int chol_panel_steps(T (&a)[NC], int n, int nsteps, int k0, int tid,
                                                 CholShared<T, NC>& sh) {
+    constexpr int CK = NC < 8 ? NC : 8;
+    static_assert(NC % CK == 0, "chunking");
+    int info = 0;
+    static_for<0, NC / CK>([&](auto cc) {
+        constexpr int c0 = decltype(cc)::value * CK;
+        if (c0 >= nsteps || info != 0) return;
+        const int kend = min(c0 + CK, nsteps);
+#pragma unroll 1
+        for (int k = c0; k < kend; ++k) {
+            const int buf = k & 1;
+            const int g = k0 + k;
+            T ak = a[c0];
+#pragma unroll
+            for (int q = 1; q < CK; ++q) ak = (k == c0 + q) ? a[c0 + q] : ak;
+            if (tid >= g && tid < n && tid < k0 + NC) sh.col[buf][tid - k0] = ak;
+            mat_sync<NW>();
+            const T d = sh.col[buf][k];
+            if (!(d > T(0))) {      // not positive definite (or NaN): stop, A(g,g) keeps d
+                info = g + 1;
+                break;
+            }
+            const T s = sqrt_rn(d);
+            const T r = T(1) / s;
+            const bool live = tid > g && tid < n;
+            const T l = ak * r;
+            const T nk = (tid == g) ? s : (live ? l : ak);
+#pragma unroll
+            for (int q = 0; q < CK; ++q)
+                if (k == c0 + q) a[c0 + q] = nk;
+            if (live) {
+#pragma unroll
+                for (int j = c0; j < c0 + CK; ++j)
+                    if (j > k) a[j] = fma_rn(-l, sh.col[buf][j] * r, a[j]);
+#pragma unroll
+                for (int j = c0 + CK; j < NC; ++j) a[j] = fma_rn(-l, sh.col[buf][j] * r, a[j]);
+            }
+        }
+    });
+    return info;
+}
+
+// The same steps fully unrolled: the blocked factorisation's 32-column panel, whose
+// code is small enough for the instruction cache and which spilled when chunked.
+template <typename T, int NC, int NW>
+__device__ __forceinline__ int chol_panel_steps_unrolled(T (&a)[NC], int n, int nsteps, int k0, int tid,
+                                                         CholShared<T, NC>& sh) {
     int info = 0;
     static_for<0, NC>([&](auto kc) {
         constexpr int k = decltype(kc)::value;
@@ -47,7 +97,7 @@ __device__ __forceinline__ int chol_panel_steps(T (&a)[NC], int n, int nsteps, i
         if (tid >= g && tid < n && tid < k0 + NC) sh.col[buf][tid - k0] = a[k];
         mat_sync<NW>();
         const T d = sh.col[buf][k];
-        if (!(d > T(0))) {          // not positive definite (or NaN): stop, A(g,g) keeps d
+        if (!(d > T(0))) {
             info = g + 1;
             return;
         }
@@ -67,39 +117,60 @@ __device__ __forceinline__ int chol_panel_steps(T (&a)[NC], int n, int nsteps, i
 // Solve L L^T x = b for register-resident rows of L (thread = row, `a` = row).
 // Forward: b(k) /= L(k,k); b(i) = fma(-b(k), L(i,k), b(i)) for i > k.
 // Backward (column sweep of U = L^T): b(k) /= L(k,k); b(i) = fma(-b(k), L(k,i), b(i)) for i < k,
-// with row k of L published through shared memory.
+// with row k of L published through shared memory. Chunked like chol_panel_steps.
 template <typename T, int NC, int NW, int R>
 __device__ __forceinline__ void chol_solve(const T (&a)[NC], int n, int tid, T (&b)[R], CholShared<T, NC>& sh) {
     static_assert(R <= 8, "CholShared::rhs holds 8 right-hand sides a group");
-    static_for<0, NC>([&](auto kc) {
-        constexpr int k = decltype(kc)::value;
-        if (k >= n) return;
-        constexpr int buf = k & 1;
-        if (tid == k) {
+    constexpr int CK = NC < 8 ? NC : 8;
+    auto pick = [&](int k, auto c0c) {
+        constexpr int c0 = decltype(c0c)::value;
+        T ak = a[c0];
 #pragma unroll
-            for (int r = 0; r < R; ++r) { b[r] = b[r] / a[k]; sh.rhs[buf][r] = b[r]; }
-        }
-        mat_sync<NW>();
-        if (tid > k && tid < n) {
+        for (int q = 1; q < CK; ++q) ak = (k == c0 + q) ? a[c0 + q] : ak;
+        return ak;
+    };
+    static_for<0, NC / CK>([&](auto cc) {
+        constexpr int c0 = decltype(cc)::value * CK;
+        if (c0 >= n) return;
+        const int kend = min(c0 + CK, n);
+#pragma unroll 1
+        for (int k = c0; k < kend; ++k) {
+            const int buf = k & 1;
+            const T ak = pick(k, std::integral_constant<int, c0>{});
+            if (tid == k) {
 #pragma unroll
-            for (int r = 0; r < R; ++r) b[r] = fma_rn(-sh.rhs[buf][r], a[k], b[r]);
+                for (int r = 0; r < R; ++r) { b[r] = b[r] / ak; sh.rhs[buf][r] = b[r]; }
+            }
+            mat_sync<NW>();
+            if (tid > k && tid < n) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) b[r] = fma_rn(-sh.rhs[buf][r], ak, b[r]);
+            }
         }
     });
-    static_for<0, NC>([&](auto ic) {
-        constexpr int k = NC - 1 - decltype(ic)::value;
-        if (k >= n) return;
-        constexpr int buf = (k + 1) & 1;
-        if (tid == k) {
+    static_for<0, NC / CK>([&](auto ic) {
+        constexpr int c0 = (NC / CK - 1 - decltype(ic)::value) * CK;
+        if (c0 >= n) return;
+        const int ktop = min(c0 + CK, n) - 1;
+#pragma unroll 1
+        for (int k = ktop; k >= c0; --k) {
+            const int buf = (k + 1) & 1;
+            if (tid == k) {
+                const T ak = pick(k, std::integral_constant<int, c0>{});
 #pragma unroll
-            for (int r = 0; r < R; ++r) { b[r] = b[r] / a[k]; sh.rhs[buf][r] = b[r]; }
+                for (int r = 0; r < R; ++r) { b[r] = b[r] / ak; sh.rhs[buf][r] = b[r]; }
 #pragma unroll
-            for (int j = 0; j < k; ++j) sh.row[buf][j] = a[j];
-        }
-        mat_sync<NW>();
-        if (tid < k) {
-            const T lki = sh.row[buf][tid];
+                for (int j = 0; j < c0; ++j) sh.row[buf][j] = a[j];
 #pragma unroll
-            for (int r = 0; r < R; ++r) b[r] = fma_rn(-sh.rhs[buf][r], lki, b[r]);
+                for (int j = c0; j < c0 + CK; ++j)
+                    if (j < k) sh.row[buf][j] = a[j];
+            }
+            mat_sync<NW>();
+            if (tid < k) {
+                const T lki = sh.row[buf][tid];
+#pragma unroll
+                for (int r = 0; r < R; ++r) b[r] = fma_rn(-sh.rhs[buf][r], lki, b[r]);
+            }
         }
     });
 }
@@ -137,7 +208,7 @@ __device__ int blocked_potrf(T* __restrict__ A, int n, int lda, bool upper, Bloc
 #pragma unroll
         for (int c = 0; c < NB; ++c)
             a[c] = (live && c < nbp && k0 + c <= tid) ? tri(A, lda, upper, tid, k0 + c) : T(0);
-        const int info = chol_panel_steps<T, NB, NW>(a, n, nbp, k0, tid, sh.p);
+        const int info = chol_panel_steps_unrolled<T, NB, NW>(a, n, nbp, k0, tid, sh.p);
         if (live) {
 #pragma unroll
             for (int c = 0; c < NB; ++c)
