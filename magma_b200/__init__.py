@@ -10,18 +10,17 @@ runs in the library's kernels.
 from __future__ import annotations
 
 from . import _lib
-from .api import (Queue, VarBatch, ptr_array, dgetrf_batched, dgetrs_batched, dgesv_batched, dpotrf_batched,
-                  dpotrs_batched, dposv_batched, dposv_vbatched, dsgesv_batched,
-                  dgesv_vbatched, dsposv_vbatched, dgetri_outofplace_batched, dgetrf_nopiv_batched,
-                  dgetrs_nopiv_batched, dgesv_nopiv_batched, dgerbt_batched, dgesv_rbt_batched, dgeqrf_batched, gemm_batched, syrk_vbatched,
-                  tri_vbatched,
-                  gemm_vbatched)
+from .api import (Queue, VarBatch, dgeqrf_batched, dgerbt_batched, dgesv_batched, dgesv_nopiv_batched,
+                  dgesv_rbt_batched, dgesv_vbatched, dgetrf_batched, dgetrf_nopiv_batched, dgetri_outofplace_batched,
+                  dgetrs_batched, dgetrs_nopiv_batched, dposv_batched, dposv_vbatched, dpotrf_batched,
+                  dpotrs_batched, dsgesv_batched, dsposv_vbatched, gemm_batched, gemm_vbatched, ptr_array,
+                  syrk_vbatched, tri_vbatched)
 
 __all__ = ["Queue", "VarBatch", "ptr_array", "dgetrf_batched", "dgetrs_batched", "dgesv_batched", "dpotrf_batched",
-           "dpotrs_batched", "dposv_batched", "dposv_vbatched", "dsgesv_batched", "dgesv_vbatched", "dsposv_vbatched", "dgetri_outofplace_batched",
-           "dgetrf_nopiv_batched", "dgetrs_nopiv_batched", "dgesv_nopiv_batched", "dgerbt_batched",
-           "dgesv_rbt_batched", "dgeqrf_batched", "gemm_batched", "syrk_vbatched", "tri_vbatched",
-           "gemm_vbatched", "load"]
+           "dpotrs_batched", "dposv_batched", "dposv_vbatched", "dsgesv_batched", "dgesv_vbatched", "dsposv_vbatched",
+           "dgetri_outofplace_batched", "dgetrf_nopiv_batched", "dgetrs_nopiv_batched", "dgesv_nopiv_batched",
+           "dgerbt_batched", "dgesv_rbt_batched", "dgeqrf_batched", "gemm_batched", "gemm_vbatched", "syrk_vbatched",
+           "tri_vbatched", "load"]
 
 
 def load():
