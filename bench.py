@@ -1287,11 +1287,12 @@ def run_reference(args, rank):
     from magma_b200 import testing as T
 
     nthreads = oracle.max_threads()
-    if args.workload not in ("c1", "c3", "qr", "getri", "nopiv"):
-        print(json.dumps({"impl": "reference", "unavailable": "the reference arm covers the c1, c3, qr, getri "
-                          "and nopiv workloads; c2/c4 report their CPU LAPACK loop as cpu_baseline"}), flush=True)
+    if args.workload not in ("c1", "c2", "c3", "c4", "qr", "getri", "nopiv", "trsm"):
+        print(json.dumps({"impl": "reference", "unavailable": "no reference arm for this workload (c5 is the "
+                          "request loop; the reference has no serving front end)"}), flush=True)
         return
     metric, unit = METRIC, "solves/s"
+    per_step = None          # units of work per step when they are not instances (GFLOP)
     # each step gets fresh copies of the inputs, made outside the timed call
     if args.workload == "c3":
         sample = 256
@@ -1301,6 +1302,57 @@ def run_reference(args, rank):
         desc = f"{sample} instances per step (256x256, kappa in [1e2,1e6], 4 RHS); LAPACK dsgesv"
         cfg = {"workload": "c3_dsgesv_batched_2048x256_kappa1e2-1e6_nrhs4", "batch": sample, "n": 256, "nrhs": 4}
         dtype = C3Mixed.dtype
+    elif args.workload in ("c2", "trsm"):
+        # a bounded slice of the same size distribution, CPU-generated (same distributions)
+        rng = np.random.default_rng(2)
+        sample = 2000 if args.workload == "c2" else 4000
+        if args.workload == "c2":
+            M, N, K = (v[:sample] for v in T.gemm_sizes(20000, 8, 128, seed=2))
+            r8 = lambda v: ((v + 7) // 8) * 8   # noqa: E731
+            lda, ldb, ldc = r8(M), r8(K), r8(M)
+            As = [rng.standard_normal((int(k), int(la))) for k, la in zip(K, lda)]
+            Bs = [rng.standard_normal((int(nn), int(lb))) for nn, lb in zip(N, ldb)]
+            Cs0 = [rng.standard_normal((int(nn), int(lc))) for nn, lc in zip(N, ldc)]
+            prep = lambda: ([c.copy() for c in Cs0], None)   # noqa: E731
+            fn = lambda cs, _: oracle.lapack_gemm_vbatched(0, 0, M, N, K, 1.0, As, lda, Bs, ldb, 0.5, cs, ldc,   # noqa: E731
+                                                           nthreads=nthreads)
+            per_step = float((2.0 * M.astype(np.float64) * N * K).sum()) / 1e9
+            desc = f"{sample} instances per step (M, N, K ~ U{{8..128}}, alpha 1, beta 0.5); dgemm"
+            cfg = {"workload": "c2_gemm_vbatched_20000_MNK8-128_alpha1_beta0.5", "batch": sample}
+            dtype, metric, unit = C2GemmVbatched.dtype, C2GemmVbatched.metric, C2GemmVbatched.unit
+        else:
+            M, N, _ = (v[:sample] for v in T.gemm_sizes(20000, 8, 128, seed=12))
+            r8 = lambda v: ((v + 7) // 8) * 8   # noqa: E731
+            lda, ldb = r8(M), r8(M)
+            As = []
+            for m, la in zip(M, lda):
+                a = rng.standard_normal((int(m), int(la))) / np.sqrt(float(m))
+                a[np.arange(m), np.arange(m)] += 2.0
+                As.append(a)
+            Bs0 = [rng.standard_normal((int(nn), int(lb))) for nn, lb in zip(N, ldb)]
+            prep = lambda: ([b.copy() for b in Bs0], None)   # noqa: E731
+            fn = lambda bs, _: oracle.lapack_dtri_vbatched(True, True, True, False, False, M, N, 1.0, As, lda, bs,   # noqa: E731
+                                                           ldb, nthreads=nthreads)
+            per_step = float((M.astype(np.float64) ** 2 * N).sum()) / 1e9
+            desc = f"{sample} instances per step (M, N ~ U{{8..128}}, left lower no-trans non-unit); dtrsm"
+            cfg = {"workload": "trsm_vbatched_20000_MN8-128_left_lower_notrans", "batch": sample}
+            dtype, metric, unit = TrsmVbatched.dtype, TrsmVbatched.metric, TrsmVbatched.unit
+    elif args.workload == "c4":
+        rng = np.random.default_rng(4)
+        sample = 5000
+        a_, b_ = 4.0 ** -0.5, 512.0 ** -0.5
+        n = np.rint((a_ - rng.random(sample) * (a_ - b_)) ** -2.0).astype(np.int64).clip(4, 512)
+        nr = rng.integers(1, 9, sample)
+        As0 = []
+        for nv in n:
+            G = rng.standard_normal((int(nv), int(nv)))
+            As0.append(G @ G.T + nv * np.eye(int(nv)))
+        Bs0 = [rng.standard_normal((int(r), int(nv))) for nv, r in zip(n, nr)]
+        prep = lambda: (([a.copy() for a in As0], [b.copy() for b in Bs0]), None)   # noqa: E731
+        fn = lambda ab, _: oracle.lapack_dposv_vbatched(ab[0], ab[1], n, nr, n, n, nthreads=nthreads)   # noqa: E731
+        desc = f"{sample} instances per step (SPD, n power law on [4,512], 1-8 RHS); dpotrf + dpotrs"
+        cfg = {"workload": "c4_posv_vbatched_50000_n4-512_powerlaw1.5_nrhs1-8", "batch": sample}
+        dtype, metric = C4CholVbatched.dtype, C4CholVbatched.metric
     elif args.workload == "getri":
         sample = 10000
         A0, _ = T.lu_uniform(sample, 32, 1, seed=8)
@@ -1344,7 +1396,7 @@ def run_reference(args, rank):
         fn(a, b)
         times.append(time.perf_counter() - t0)
     total = sum(times)
-    value = sample * args.steps / total
+    value = (per_step if per_step is not None else sample) * args.steps / total
     del np
     line = {
         "impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": args.gpus,
