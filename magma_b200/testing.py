@@ -173,7 +173,7 @@ def svd_logrand_torch(batch: int, n: int, kappa_lo: float = 1e2, kappa_hi: float
 
 
 def backward_error_torch(A_cm, X_cm, B_cm):
-    """Normwise backward error per instance and RHS on the GPU (FP64; checker only)."""
+    """Normwise backward error per instance and RHS on the GPU (FP64; used to verify results)."""
     A = A_cm.transpose(1, 2)
     X = X_cm.transpose(1, 2)
     Bm = B_cm.transpose(1, 2)
