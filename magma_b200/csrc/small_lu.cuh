@@ -211,6 +211,85 @@ __device__ __forceinline__ void lu_panel_steps(T (&a)[NC], int m, int nsteps, in
     });
 }
 
+// The steps of lu_panel_steps for wide rows (NC > 32), in chunks of CK = 8: the code
+// of a chunk is unrolled over the registers from the chunk's first column on and
+// looped over its 8 steps at run time (the step's own column picked by selects), so
+// the kernel fits the instruction cache (the fully unrolled 64-column form thrashed
+// it). Every element receives the same operations in the same order.
+template <typename T, int NC, int NW>
+__device__ __forceinline__ void lu_panel_steps_chunked(T (&a)[NC], int m, int nsteps, int tid, int& pos,
+                                                       int& my_ipiv, int& info, SmallLuShared<T, NC, NW>& sh,
+                                                       bool nopiv) {
+    constexpr int CK = 8;
+    static_assert(NC % CK == 0, "chunking");
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    using V2 = typename Vec2<T>::type;
+    static_for<0, NC / CK>([&](auto cc) {
+        constexpr int c0 = decltype(cc)::value * CK;
+        if (c0 >= nsteps) return;
+        const int kend = min(c0 + CK, nsteps);
+#pragma unroll 1
+        for (int k = c0; k < kend; ++k) {
+            const int buf = k & 1;
+            const int g = k;
+            T ak = a[c0];
+#pragma unroll
+            for (int q = 1; q < CK; ++q) ak = (k == c0 + q) ? a[c0 + q] : ak;
+            int p = g, s = g;
+            if (!nopiv) {
+                const bool cand = (pos >= g && tid < m);
+                PivotKey key = pivot_key(ak, cand);
+                p = cand ? pos : INT_MAX;
+                s = warp_argmax(key, p, lane) + warp * 32;
+                if (NW > 1) {
+                    if (lane == 0) {
+                        sh.red_hi[buf][warp] = key.hi; sh.red_lo[buf][warp] = key.lo;
+                        sh.red_p[buf][warp] = p; sh.red_s[buf][warp] = s;
+                    }
+                    __syncthreads();
+                    const bool v = lane < NW;
+                    key = PivotKey{v ? sh.red_hi[buf][lane] : 0u, v ? sh.red_lo[buf][lane] : 0u};
+                    p = v ? sh.red_p[buf][lane] : INT_MAX;
+                    s = sh.red_s[buf][warp_argmax(key, p, lane)];
+                }
+            }
+            // the pivot row publishes columns c0..NC-1 (aligned pairs; consumers read k.. only)
+            if (tid == s) {
+                V2* row2 = reinterpret_cast<V2*>(&sh.row[buf][0]);
+#pragma unroll
+                for (int j = c0; j < NC; j += 2) row2[j / 2] = make_vec2<T>(a[j], a[j + 1]);
+            }
+            mat_sync<NW>();
+            const T piv = sh.row[buf][k];
+            if (tid == g) my_ipiv = p + 1;
+            if (piv != T(0)) {
+                if (pos == g) pos = p;
+                if (tid == s) pos = g;
+            } else if (info == 0) {
+                info = g + 1;
+            }
+            if (pos > g && tid < m) {
+                if (piv != T(0)) {
+                    if (fabs(piv) >= tiny_normal<T>()) ak = ak * (T(1) / piv);
+                    else                               ak = ak / piv;
+                }
+#pragma unroll
+                for (int q = 0; q < CK; ++q)
+                    if (k == c0 + q) a[c0 + q] = ak;
+                const T l = ak;
+                const V2* row2 = reinterpret_cast<const V2*>(&sh.row[buf][0]);
+#pragma unroll
+                for (int j = c0; j < NC; j += 2) {
+                    const V2 u = row2[j / 2];
+                    if (j > k) a[j] = fma_rn(l, -u.x, a[j]);
+                    if (j + 1 > k) a[j + 1] = fma_rn(l, -u.y, a[j + 1]);
+                }
+            }
+        }
+    });
+}
+
 // Whole small matrix (m rows, n <= NC columns): steps 0 .. min(m,n)-1.
 template <typename T, int NC, int NW>
 __device__ __forceinline__ void small_lu_factor(T (&a)[NC], int m, int n, int tid, int& pos,
@@ -219,7 +298,64 @@ __device__ __forceinline__ void small_lu_factor(T (&a)[NC], int m, int n, int ti
     pos = (tid < m) ? tid : INT_MAX / 2;
     info = 0;
     my_ipiv = 0;
-    lu_panel_steps<T, NC, NW>(a, m, min(m, n), n, 0, tid, pos, my_ipiv, info, sh, nopiv);
+    if constexpr (NC > 32) lu_panel_steps_chunked<T, NC, NW>(a, m, min(m, n), tid, pos, my_ipiv, info, sh, nopiv);
+    else lu_panel_steps<T, NC, NW>(a, m, min(m, n), n, 0, tid, pos, my_ipiv, info, sh, nopiv);
+}
+
+// small_lu_solve for wide rows (NC > 32), chunked like lu_panel_steps_chunked.
+template <typename T, int NC, int NW, int R>
+__device__ __forceinline__ void small_lu_solve_chunked(const T (&a)[NC], int n, int pos, T (&b)[R],
+                                                       SmallLuShared<T, NC, NW>& sh) {
+    constexpr int CK = 8;
+    auto pick = [&](int k, auto c0c) {
+        constexpr int c0 = decltype(c0c)::value;
+        T ak = a[c0];
+#pragma unroll
+        for (int q = 1; q < CK; ++q) ak = (k == c0 + q) ? a[c0 + q] : ak;
+        return ak;
+    };
+    static_for<0, NC / CK>([&](auto cc) {
+        constexpr int c0 = decltype(cc)::value * CK;
+        if (c0 >= n) return;
+        const int kend = min(c0 + CK, n);
+#pragma unroll 1
+        for (int k = c0; k < kend; ++k) {
+            const int buf = k & 1;
+            if (pos == k) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) sh.rhs[buf][r] = b[r];
+            }
+            mat_sync<NW>();
+            if (pos > k && pos < n) {
+                const T ak = pick(k, std::integral_constant<int, c0>{});
+#pragma unroll
+                for (int r = 0; r < R; ++r) b[r] = fma_rn(-sh.rhs[buf][r], ak, b[r]);
+            }
+        }
+    });
+    static_for<0, NC / CK>([&](auto ic) {
+        constexpr int c0 = (NC / CK - 1 - decltype(ic)::value) * CK;
+        if (c0 >= n) return;
+        const int ktop = min(c0 + CK, n) - 1;
+#pragma unroll 1
+        for (int kk = ktop; kk >= c0; --kk) {
+            const int buf = (kk + 1) & 1;
+            if (pos == kk) {
+                const T ak = pick(kk, std::integral_constant<int, c0>{});
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    b[r] = b[r] / ak;
+                    sh.rhs[buf][r] = b[r];
+                }
+            }
+            mat_sync<NW>();
+            if (pos < kk) {
+                const T ak = pick(kk, std::integral_constant<int, c0>{});
+#pragma unroll
+                for (int r = 0; r < R; ++r) b[r] = fma_rn(-sh.rhs[buf][r], ak, b[r]);
+            }
+        }
+    });
 }
 
 // Solve with the factors held in registers. Each thread holds its LU row at
@@ -232,6 +368,10 @@ template <typename T, int NC, int NW, int R>
 __device__ __forceinline__ void small_lu_solve(const T (&a)[NC], int n, int pos, T (&b)[R],
                                                SmallLuShared<T, NC, NW>& sh) {
     static_assert(R <= 4, "SmallLuShared::rhs holds 4 right-hand sides a group");
+    if constexpr (NC > 32) {
+        small_lu_solve_chunked<T, NC, NW, R>(a, n, pos, b, sh);
+        return;
+    }
     static_for<0, NC>([&](auto kc) {
         constexpr int k = decltype(kc)::value;
         if (k >= n) return;
