@@ -30,7 +30,11 @@ enum { MAGMA_B200_SOLVE_LU = 0, MAGMA_B200_SOLVE_CHOLESKY = 1 };
 
 /* Creates a server on `device` with a device arena of budget_bytes (one
  * cudaMalloc, here), `streams` CUDA streams (batches in flight) and at most
- * max_batch requests per micro-batch. Returns MAGMA_SUCCESS or a MAGMA error. */
+ * max_batch requests per micro-batch. Before returning it runs one small batch of
+ * every kernel family and size bucket, so that no request pays a kernel's first-use
+ * load. Each stream carries 4 auxiliary streams: the process should have
+ * CUDA_DEVICE_MAX_CONNECTIONS >= 5 * streams (the library requests 32 at load time
+ * unless it is already set). Returns MAGMA_SUCCESS or a MAGMA error. */
 magma_int_t magma_b200_server_create(magma_int_t device, size_t budget_bytes, magma_int_t streams,
                                      magma_int_t max_batch, magma_b200_server_t* server);
 

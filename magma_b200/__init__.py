@@ -9,8 +9,14 @@ runs in the library's kernels.
 """
 from __future__ import annotations
 
-from . import _lib
-from .api import (Queue, VarBatch, dgeqrf_batched, dgerbt_batched, dgesv_batched, dgesv_nopiv_batched,
+import os
+
+# The library's queues use more streams than the driver's default 8 hardware work
+# queues; ask for 32 before any CUDA context exists (a value already set is kept).
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
+from . import _lib  # noqa: E402
+from .api import (Queue, VarBatch, dgeqrf_batched, dgerbt_batched, dgesv_batched, dgesv_nopiv_batched,  # noqa: E402
                   dgesv_rbt_batched, dgesv_vbatched, dgetrf_batched, dgetrf_nopiv_batched, dgetri_outofplace_batched,
                   dgetrs_batched, dgetrs_nopiv_batched, dposv_batched, dposv_vbatched, dpotrf_batched,
                   dpotrs_batched, dsgesv_batched, dsposv_vbatched, gemm_batched, gemm_vbatched, ptr_array,

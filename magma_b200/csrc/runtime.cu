@@ -252,6 +252,18 @@ void magma_iset_pointer(magma_int_t** out, magma_int_t* in, magma_int_t lda, mag
 }
 }  // extern "C"
 
+// Every queue owns a stream and 4 auxiliary streams, so a process with a few queues
+// (the request loop runs 4: 20 streams) exceeds the driver's default of 8 hardware
+// work queues, and streams that share one are serialised: a small request's kernel
+// waited behind another class's 18 ms factorisation (measured: small-request p50
+// 3-7 ms instead of 0.1-0.5 ms under mixed load). When the library is loaded before
+// the process creates its CUDA context (any program linked against it), this asks the
+// driver for 32 hardware queues; a value the caller already set is kept, and a context
+// that already exists is not affected.
+__attribute__((constructor)) static void mb200_request_hw_queues() {
+    setenv("CUDA_DEVICE_MAX_CONNECTIONS", "32", 0);
+}
+
 namespace mb200 {
 magma_int_t queue_fork(magma_queue_t queue) {
     if (!queue->aux_ready) {
