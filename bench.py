@@ -1258,7 +1258,7 @@ class NopivBatched:
 
 WORKLOADS = {"c3": C3Mixed, "c1": C1DgesvSmall, "c2": C2GemmVbatched, "c4": C4CholVbatched, "qr": QrBatched, "getri": GetriBatched,
              "nopiv": NopivBatched, "trsm": TrsmVbatched}
-DEFAULT_STEPS = {"c3": (60, 5), "c1": (20000, 50), "c2": (50, 5), "c4": (20, 3), "c5": (3000, 200), "qr": (200, 5), "getri": (200, 5), "nopiv": (200, 5), "trsm": (50, 5)}
+DEFAULT_STEPS = {"c3": (60, 5), "c1": (20000, 50), "c2": (50, 5), "c4": (20, 3), "c5": (10000, 200), "qr": (200, 5), "getri": (200, 5), "nopiv": (200, 5), "trsm": (50, 5)}
 
 
 # ---------------------------------------------------------------------- main
@@ -1432,7 +1432,7 @@ def run_serving(args, rank, world):
     stated = 1e4
     sweep = []
     clocks = ClockSampler("GPU-" + str(torch.cuda.get_device_properties(dev).uuid))
-    with serve.Server(40 << 30, streams=4, max_batch=256) as sv:
+    with serve.Server(40 << 30, streams=6, max_batch=256) as sv:
         serve.run_load(sv, warm, rate=1e4, seed=1)
         clocks.start()
         for r in rates:
@@ -1457,7 +1457,7 @@ def run_serving(args, rank, world):
             "ms_per_step": 1e3 / at["throughput"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": serve.__doc__.split("\n")[3].strip() + " (seeded)",
             "config": {"workload": f"c5_serving_{args.steps}req_lu70_chol30_n8-1024_nrhs1-16",
-                       "offered_rate": stated, "hbm_budget_bytes": 40 << 30, "streams": 4, "max_batch": 256,
+                       "offered_rate": stated, "hbm_budget_bytes": 40 << 30, "streams": 6, "max_batch": 256,
                        "parallelism": f"replicas x{world}", "l2": "per-request copies from pinned host memory"},
             "p50_ms": at["p50_ms"], "p99_ms": at["p99_ms"], "sweep": sweep, "bwd_err_max": be,
             "peak_device_bytes": stats["peak_bytes"], "micro_batches": stats["batches"],
