@@ -539,6 +539,37 @@ void magmablas_strmm_vbatched_nocheck(magma_side_t side, magma_uplo_t uplo, magm
                                       magma_int_t* ldda, float** dB_array, magma_int_t* lddb, magma_int_t batchCount,
                                       magma_queue_t queue);
 
+
+/* Fixed-size forms (include/magma_zbatched.h:132-157,202-208,271-277): SYRK checks as
+ * magmablas/zherk_batched_core.cu:233-258 (uplo -1, trans -2, n -3, k -4, ldda -7, lddc -10;
+ * nothing done when n or k is 0); trsm/trmm as magmablas/ztrsm_batched.cpp:196-229 and
+ * magmablas/ztrmm_batched_core.cu:811-832 (side -1, uplo -2, transA -3, diag -4, m -5, n -6,
+ * ldda -9, lddb -11). The same kernels as the variable-size forms. */
+void magmablas_dsyrk_batched(magma_uplo_t uplo, magma_trans_t trans, magma_int_t n, magma_int_t k, double alpha,
+                             double const* const* dA_array, magma_int_t ldda, double beta, double** dC_array,
+                             magma_int_t lddc, magma_int_t batchCount, magma_queue_t queue);
+void magma_dsyrk_batched(magma_uplo_t uplo, magma_trans_t trans, magma_int_t n, magma_int_t k, double alpha,
+                         double const* const* dA_array, magma_int_t ldda, double beta, double** dC_array,
+                         magma_int_t lddc, magma_int_t batchCount, magma_queue_t queue);
+void magmablas_dtrsm_batched(magma_side_t side, magma_uplo_t uplo, magma_trans_t transA, magma_diag_t diag,
+                             magma_int_t m, magma_int_t n, double alpha, double** dA_array, magma_int_t ldda,
+                             double** dB_array, magma_int_t lddb, magma_int_t batchCount, magma_queue_t queue);
+void magmablas_dtrmm_batched(magma_side_t side, magma_uplo_t uplo, magma_trans_t transA, magma_diag_t diag,
+                             magma_int_t m, magma_int_t n, double alpha, double** dA_array, magma_int_t ldda,
+                             double** dB_array, magma_int_t lddb, magma_int_t batchCount, magma_queue_t queue);
+void magmablas_ssyrk_batched(magma_uplo_t uplo, magma_trans_t trans, magma_int_t n, magma_int_t k, float alpha,
+                             float const* const* dA_array, magma_int_t ldda, float beta, float** dC_array,
+                             magma_int_t lddc, magma_int_t batchCount, magma_queue_t queue);
+void magma_ssyrk_batched(magma_uplo_t uplo, magma_trans_t trans, magma_int_t n, magma_int_t k, float alpha,
+                         float const* const* dA_array, magma_int_t ldda, float beta, float** dC_array,
+                         magma_int_t lddc, magma_int_t batchCount, magma_queue_t queue);
+void magmablas_strsm_batched(magma_side_t side, magma_uplo_t uplo, magma_trans_t transA, magma_diag_t diag,
+                             magma_int_t m, magma_int_t n, float alpha, float** dA_array, magma_int_t ldda,
+                             float** dB_array, magma_int_t lddb, magma_int_t batchCount, magma_queue_t queue);
+void magmablas_strmm_batched(magma_side_t side, magma_uplo_t uplo, magma_trans_t transA, magma_diag_t diag,
+                             magma_int_t m, magma_int_t n, float alpha, float** dA_array, magma_int_t ldda,
+                             float** dB_array, magma_int_t lddb, magma_int_t batchCount, magma_queue_t queue);
+
 #ifdef __cplusplus
 }
 #endif

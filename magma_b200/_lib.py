@@ -105,6 +105,14 @@ SIGNATURES: dict[str, tuple] = {
                                                     _i, _p]),
     "magmablas_sgemm_vbatched_max": (None, [_i, _i, _p, _p, _p, _f, _p, _p, _p, _p, _f, _p, _p, _i, _i, _i, _i, _p]),
     "magmablas_sgemm_vbatched_nocheck": (None, [_i, _i, _p, _p, _p, _f, _p, _p, _p, _p, _f, _p, _p, _i, _p]),
+    "magmablas_dsyrk_batched": (None, [_i, _i, _i, _i, _d, _p, _i, _d, _p, _i, _i, _p]),
+    "magma_dsyrk_batched": (None, [_i, _i, _i, _i, _d, _p, _i, _d, _p, _i, _i, _p]),
+    "magmablas_dtrsm_batched": (None, [_i, _i, _i, _i, _i, _i, _d, _p, _i, _p, _i, _i, _p]),
+    "magmablas_dtrmm_batched": (None, [_i, _i, _i, _i, _i, _i, _d, _p, _i, _p, _i, _i, _p]),
+    "magmablas_ssyrk_batched": (None, [_i, _i, _i, _i, _f, _p, _i, _f, _p, _i, _i, _p]),
+    "magma_ssyrk_batched": (None, [_i, _i, _i, _i, _f, _p, _i, _f, _p, _i, _i, _p]),
+    "magmablas_strsm_batched": (None, [_i, _i, _i, _i, _i, _i, _f, _p, _i, _p, _i, _i, _p]),
+    "magmablas_strmm_batched": (None, [_i, _i, _i, _i, _i, _i, _f, _p, _i, _p, _i, _i, _p]),
     "magmablas_dsyrk_vbatched": (None, [_i, _i, _p, _p, _d, _p, _p, _d, _p, _p, _i, _p]),
     "magmablas_dsyrk_vbatched_max_nocheck": (None, [_i, _i, _p, _p, _d, _p, _p, _d, _p, _p, _i, _i, _i, _p]),
     "magmablas_dsyrk_vbatched_max": (None, [_i, _i, _p, _p, _d, _p, _p, _d, _p, _p, _i, _i, _i, _p]),

@@ -310,6 +310,30 @@ static int syrk_vbatched_check(magma_uplo_t uplo, magma_trans_t trans, int* n, i
     return 0;
 }
 
+// Fixed size (magmablas/zherk_batched_core.cu:233-258): uplo -1, trans -2 (NoTrans or Trans),
+// n -3, k -4, ldda < (trans == NoTrans ? n : k) -7, lddc < n -10; quick return when n or
+// k is 0 (C is then left as it is, unlike the variable-size form).
+template <typename T>
+static void syrk_batched(const char* name, magma_uplo_t uplo, magma_trans_t trans, int n, int k, T alpha,
+                         const T* const* A, int lda, T beta, T** C, int ldc, int batch, magma_queue_t queue) {
+    int info = 0;
+    if (uplo != MagmaUpper && uplo != MagmaLower) info = -1;
+    else if (trans != MagmaNoTrans && trans != MagmaTrans) info = -2;
+    else if (n < 0) info = -3;
+    else if (k < 0) info = -4;
+    else if (trans == MagmaNoTrans ? lda < n : lda < k) info = -7;
+    else if (ldc < n) info = -10;
+    if (info != 0) {
+        magma_xerbla(name, -info);
+        return;
+    }
+    if (n <= 0 || k <= 0 || batch <= 0) return;
+    GemmSizes g{n, n, k, lda, lda, ldc, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                uplo == MagmaLower ? 1 : 2};
+    const magma_trans_t tb = (trans == MagmaNoTrans) ? MagmaTrans : MagmaNoTrans;
+    gemm_launch<T>(trans, tb, g, alpha, A, A, beta, C, batch, n, n, queue->stream);
+}
+
 // magmablas/dsyrk_vbatched_core.cu:102-112: no quick return on k (k = 0 scales the
 // triangle by beta), none on n beyond an empty batch.
 template <typename T>
@@ -326,6 +350,18 @@ static void syrk_vbatched_max_nocheck(magma_uplo_t uplo, magma_trans_t trans, in
 }  // namespace mb200
 
 using namespace mb200;
+
+#define MB200_SYRK_FIXED_API(P, T)                                                                                    \
+    void magmablas_##P##syrk_batched(magma_uplo_t uplo, magma_trans_t trans, magma_int_t n, magma_int_t k, T alpha,  \
+                                     T const* const* dA_array, magma_int_t ldda, T beta, T** dC_array,               \
+                                     magma_int_t lddc, magma_int_t batchCount, magma_queue_t queue) {                \
+        syrk_batched<T>(__func__, uplo, trans, n, k, alpha, dA_array, ldda, beta, dC_array, lddc, batchCount, queue); \
+    }                                                                                                                 \
+    void magma_##P##syrk_batched(magma_uplo_t uplo, magma_trans_t trans, magma_int_t n, magma_int_t k, T alpha,      \
+                                 T const* const* dA_array, magma_int_t ldda, T beta, T** dC_array, magma_int_t lddc, \
+                                 magma_int_t batchCount, magma_queue_t queue) {                                       \
+        syrk_batched<T>(__func__, uplo, trans, n, k, alpha, dA_array, ldda, beta, dC_array, lddc, batchCount, queue); \
+    }
 
 #define MB200_SYRK_API(P, T)                                                                                          \
     void magmablas_##P##syrk_vbatched_max_nocheck(magma_uplo_t uplo, magma_trans_t trans, magma_int_t* n,             \
@@ -436,4 +472,6 @@ MB200_GEMM_API(d, double)
 MB200_GEMM_API(s, float)
 MB200_SYRK_API(d, double)
 MB200_SYRK_API(s, float)
+MB200_SYRK_FIXED_API(d, double)
+MB200_SYRK_FIXED_API(s, float)
 }

@@ -31,7 +31,8 @@ template <typename T>
 struct TriArgs {
     const T* const* A;
     T** B;
-    const int *m, *n, *lda, *ldb;
+    const int *m, *n, *lda, *ldb;   // per-instance sizes (variable size), or null:
+    int m0, n0, lda0, ldb0;         // the sizes shared by every instance (fixed size)
     T alpha;
     bool left, unit;
 };
@@ -50,12 +51,12 @@ tri_panel_kernel(TriArgs<T> g, int panels, int batch) {
     __shared__ T rcp[TS];
     const int id = blockIdx.x / panels, panel = blockIdx.x - id * panels;
     if (id >= batch) return;
-    const int m = g.m[id], n = g.n[id];
+    const int m = g.m ? g.m[id] : g.m0, n = g.n ? g.n[id] : g.n0;
     const int nr = g.left ? m : n, nc = g.left ? n : m;
     const int c0 = panel * TS;
     if (nr <= 0 || c0 >= nc) return;
     const int C = min(TS, nc - c0);
-    const int lda = g.lda[id], ldb = g.ldb[id];
+    const int lda = g.lda ? g.lda[id] : g.lda0, ldb = g.ldb ? g.ldb[id] : g.ldb0;
     const T* A = g.A[id];
     T* B = g.B[id];
     const int tid = threadIdx.x, tx = tid % 8, ty = tid / 8;
@@ -231,8 +232,46 @@ static void tri_vbatched(bool solve, magma_side_t side, magma_uplo_t uplo, magma
         magma_xerbla(solve ? "magmablas_trsm_vbatched" : "magmablas_trmm_vbatched", 12);
         return;
     }
-    const TriArgs<T> g{A, B, m, n, lda, ldb, alpha, left, diag == MagmaUnit};
+    const TriArgs<T> g{A, B, m, n, lda, ldb, 0, 0, 0, 0, alpha, left, diag == MagmaUnit};
     const int code = (solve ? 8 : 0) | (flip ? 4 : 0) | (tt ? 2 : 0) | (bt ? 1 : 0);
+    tri_dispatch<T>(code, g, panels, batch, (unsigned)blocks, queue->stream);
+}
+
+// Fixed size (magmablas/ztrsm_batched.cpp:196-229, magmablas/ztrmm_batched_core.cu:811-832):
+// side -1, uplo -2, transA -3, diag -4, m -5, n -6, ldda < max(1, rows of A) -9,
+// lddb < max(1, m) -11; quick return when m or n is 0.
+template <typename T>
+static void tri_batched(bool solve, const char* name, magma_side_t side, magma_uplo_t uplo, magma_trans_t transA,
+                        magma_diag_t diag, int m, int n, T alpha, T* const* A, int lda, T** B, int ldb, int batch,
+                        magma_queue_t queue) {
+    int info = 0;
+    const int nrow_a = side == MagmaLeft ? m : n;
+    if (side != MagmaLeft && side != MagmaRight) info = -1;
+    else if (uplo != MagmaUpper && uplo != MagmaLower) info = -2;
+    else if (transA != MagmaNoTrans && transA != MagmaTrans && transA != MagmaConjTrans) info = -3;
+    else if (diag != MagmaUnit && diag != MagmaNonUnit) info = -4;
+    else if (m < 0) info = -5;
+    else if (n < 0) info = -6;
+    else if (lda < std::max(1, nrow_a)) info = -9;
+    else if (ldb < std::max(1, m)) info = -11;
+    if (info != 0) {
+        magma_xerbla(name, -info);
+        return;
+    }
+    if (m == 0 || n == 0 || batch <= 0) return;
+    const bool left = side == MagmaLeft, opt = transA != MagmaNoTrans;
+    const bool op_lower = (uplo == MagmaLower) != opt;
+    const bool t_lower = left ? op_lower : !op_lower;
+    const bool tt = left ? opt : !opt;
+    const bool flip = solve ? !t_lower : t_lower;
+    const int panels = ceildiv(left ? n : m, kTriTile);
+    const long blocks = (long)batch * panels;
+    if (blocks > 0x7fffffffL) {
+        magma_xerbla(name, 12);
+        return;
+    }
+    const TriArgs<T> g{A, B, nullptr, nullptr, nullptr, nullptr, m, n, lda, ldb, alpha, left, diag == MagmaUnit};
+    const int code = (solve ? 8 : 0) | (flip ? 4 : 0) | (tt ? 2 : 0) | (!left ? 1 : 0);
     tri_dispatch<T>(code, g, panels, batch, (unsigned)blocks, queue->stream);
 }
 
@@ -310,7 +349,19 @@ using namespace mb200;
                         mx[0], mx[1], queue);                                                                         \
     }
 
+#define MB200_TRI_FIXED_API(P, T, OP, SOLVE)                                                                          \
+    void magmablas_##P##OP##_batched(magma_side_t side, magma_uplo_t uplo, magma_trans_t transA, magma_diag_t diag,   \
+                                     magma_int_t m, magma_int_t n, T alpha, T** dA_array, magma_int_t ldda,          \
+                                     T** dB_array, magma_int_t lddb, magma_int_t batchCount, magma_queue_t queue) {  \
+        tri_batched<T>(SOLVE, __func__, side, uplo, transA, diag, m, n, alpha, dA_array, ldda, dB_array, lddb,       \
+                       batchCount, queue);                                                                            \
+    }
+
 extern "C" {
+MB200_TRI_FIXED_API(d, double, trsm, true)
+MB200_TRI_FIXED_API(s, float, trsm, true)
+MB200_TRI_FIXED_API(d, double, trmm, false)
+MB200_TRI_FIXED_API(s, float, trmm, false)
 MB200_TRI_API(d, double, trsm, true)
 MB200_TRI_API(s, float, trsm, true)
 MB200_TRI_API(d, double, trmm, false)

@@ -1,5 +1,5 @@
-"""GPU tests of the variable-size batched BLAS-3 routines beside GEMM:
-magmablas_{d,s}trsm_vbatched*, magmablas_{d,s}trmm_vbatched* and magmablas_{d,s}syrk_vbatched*.
+"""GPU tests of the batched BLAS-3 routines beside GEMM: magmablas_{d,s}trsm_vbatched*,
+magmablas_{d,s}trmm_vbatched*, magmablas_{d,s}syrk_vbatched* and their fixed-size forms.
 
 trsm / trmm (FP64) are BIT-IDENTICAL to the oracle, which restates the kernels' order of
 operations (and is itself pinned to OpenBLAS dtrsm/dtrmm to rounding). FP32 and syrk use
@@ -12,6 +12,8 @@ import oracle
 from magma_b200 import testing as T
 
 pytestmark = pytest.mark.gpu
+
+EPS = np.finfo(np.float64).eps
 
 COMBOS = [(left, lower, trans, unit) for left in (True, False) for lower in (True, False)
           for trans in (False, True) for unit in (False, True)]
@@ -199,3 +201,87 @@ def test_syrk_vbatched_argument_errors(cuda, capfd):
     assert "parameter 7" in capfd.readouterr().err
     mb.syrk_vbatched(A, C, [4], [4], [4], [3])
     assert "parameter 10" in capfd.readouterr().err
+
+
+# ------------------------------------------------------------------ fixed-size forms
+@pytest.mark.parametrize("op", ["trsm", "trmm"])
+@pytest.mark.parametrize("left,lower,trans,unit", COMBOS[::5] + [(True, True, False, False)])
+def test_tri_batched_fixed_bit_identical(cuda, op, left, lower, trans, unit):
+    """magmablas_dtrsm_batched / magmablas_dtrmm_batched (one size for all instances) give
+    the oracle's bits, like the variable-size forms."""
+    import torch
+
+    from magma_b200.api import _vp, default_queue, ptr_array
+    q = default_queue()
+    rng = np.random.default_rng(31)
+    m, n, batch = 70, 45, 30
+    k = m if left else n
+    lda, ldb = k + 2, m + 3
+    A = rng.uniform(-1, 1, (batch, k, lda))
+    idx = np.arange(k)
+    A[:, idx, idx] += 2.0 * np.sign(A[:, idx, idx] + 1e-300) + 1.0
+    B = rng.uniform(-1, 1, (batch, n, ldb))
+    gA = torch.from_numpy(A).to(cuda)
+    gB = torch.from_numpy(B).to(cuda)
+    from magma_b200 import _lib
+    f = getattr(q.lib, f"magmablas_d{op}_batched")
+    pA, pB = ptr_array(gA), ptr_array(gB)          # kept alive until the call has run
+    f(_lib.MagmaLeft if left else _lib.MagmaRight, _lib.MagmaLower if lower else _lib.MagmaUpper,
+      _lib.MagmaTrans if trans else _lib.MagmaNoTrans, _lib.MagmaUnit if unit else _lib.MagmaNonUnit,
+      m, n, 0.625, _vp(pA), lda, _vp(pB), ldb, batch, q.handle)
+    out = gB.cpu().numpy()
+    for b in range(batch):
+        ref = B[b].copy()
+        oracle.dtri(op == "trsm", left, lower, trans, unit, m, n, 0.625, A[b].copy(), ref)
+        assert np.array_equal(out[b], ref), b
+
+
+@pytest.mark.parametrize("lower,trans", [(True, False), (False, True)])
+def test_syrk_batched_fixed(cuda, lower, trans):
+    import torch
+
+    from magma_b200 import _lib
+    from magma_b200.api import _vp, default_queue, ptr_array
+    q = default_queue()
+    rng = np.random.default_rng(41)
+    n, k, batch = 60, 37, 25
+    rows, cols = (k, n) if trans else (n, k)
+    lda, ldc = rows + 1, n + 2
+    A = rng.standard_normal((batch, cols, lda))
+    C0 = rng.standard_normal((batch, n, ldc))
+    gA, gC = torch.from_numpy(A).to(cuda), torch.from_numpy(C0.copy()).to(cuda)
+    pA, pC = ptr_array(gA), ptr_array(gC)          # kept alive until the call has run
+    q.lib.magmablas_dsyrk_batched(_lib.MagmaLower if lower else _lib.MagmaUpper,
+                                  _lib.MagmaTrans if trans else _lib.MagmaNoTrans, n, k, 0.7,
+                                  _vp(pA), lda, -0.4, _vp(pC), ldc, batch, q.handle)
+    out = gC.cpu().numpy()
+    mask = np.tril(np.ones((n, n), bool)) if lower else np.triu(np.ones((n, n), bool))
+    for b in range(batch):
+        a = A[b][:cols, :rows].T
+        op = a if not trans else a.T
+        c0 = C0[b][:, :n].T
+        ref = 0.7 * op @ op.T - 0.4 * c0
+        got = out[b][:, :n].T
+        assert syrk_err(np.where(mask, got, 0), np.where(mask, ref, 0), op, c0, k, 0.7, -0.4) < 30 * EPS
+        assert np.array_equal(got[~mask], c0[~mask])
+        assert np.array_equal(out[b][:, n:], C0[b][:, n:])
+
+
+def test_fixed_forms_argument_errors(cuda, capfd):
+    import torch
+
+    from magma_b200 import _lib
+    from magma_b200.api import _vp, default_queue, ptr_array
+    q = default_queue()
+    A = torch.zeros((1, 4, 4), dtype=torch.float64, device=cuda)
+    pA = ptr_array(A)
+    L, N, NU = _lib.MagmaLeft, _lib.MagmaNoTrans, _lib.MagmaNonUnit
+    q.lib.magmablas_dtrsm_batched(L, _lib.MagmaLower, N, NU, 4, 4, 1.0, _vp(pA), 3, _vp(pA), 4, 1, q.handle)
+    assert "parameter 9" in capfd.readouterr().err
+    q.lib.magmablas_dtrmm_batched(L, _lib.MagmaLower, N, NU, 4, 4, 1.0, _vp(pA), 4, _vp(pA), 3, 1, q.handle)
+    assert "parameter 11" in capfd.readouterr().err
+    q.lib.magmablas_dsyrk_batched(_lib.MagmaLower, _lib.MagmaConjTrans, 4, 4, 1.0, _vp(pA), 4, 0.0, _vp(pA), 4, 1,
+                                  q.handle)
+    assert "parameter 2" in capfd.readouterr().err
+    q.lib.magma_dsyrk_batched(_lib.MagmaLower, N, 4, 4, 1.0, _vp(pA), 3, 0.0, _vp(pA), 4, 1, q.handle)
+    assert "parameter 7" in capfd.readouterr().err
