@@ -115,13 +115,20 @@ __device__ __forceinline__ int chol_panel_steps_unrolled(T (&a)[NC], int n, int 
 }
 
 // Solve L L^T x = b for register-resident rows of L (thread = row, `a` = row).
-// Forward: b(k) /= L(k,k); b(i) = fma(-b(k), L(i,k), b(i)) for i > k.
-// Backward (column sweep of U = L^T): b(k) /= L(k,k); b(i) = fma(-b(k), L(k,i), b(i)) for i < k,
+// Forward: b(k) *= 1/L(k,k); b(i) = fma(-b(k), L(i,k), b(i)) for i > k.
+// Backward (column sweep of U = L^T): b(k) *= 1/L(k,k); b(i) = fma(-b(k), L(k,i), b(i)) for i < k,
 // with row k of L published through shared memory. Chunked like chol_panel_steps.
+// The diagonal enters as its correctly rounded reciprocal, formed by each thread for its
+// own row before the sweeps, so no division sits on the step-to-step chain (an IEEE
+// division is ~127 cycles of it on B200); the oracle's dpotrs is restated the same way.
 template <typename T, int NC, int NW, int R>
 __device__ __forceinline__ void chol_solve(const T (&a)[NC], int n, int tid, T (&b)[R], CholShared<T, NC>& sh) {
     static_assert(R <= 8, "CholShared::rhs holds 8 right-hand sides a group");
     constexpr int CK = NC < 8 ? NC : 8;
+    T dk = T(1);
+#pragma unroll
+    for (int j = 0; j < NC; ++j) dk = (j == tid) ? a[j] : dk;
+    const T rk = T(1) / dk;   // this row's 1/L(tid,tid)
     auto pick = [&](int k, auto c0c) {
         constexpr int c0 = decltype(c0c)::value;
         T ak = a[c0];
@@ -139,7 +146,7 @@ __device__ __forceinline__ void chol_solve(const T (&a)[NC], int n, int tid, T (
             const T ak = pick(k, std::integral_constant<int, c0>{});
             if (tid == k) {
 #pragma unroll
-                for (int r = 0; r < R; ++r) { b[r] = b[r] / ak; sh.rhs[buf][r] = b[r]; }
+                for (int r = 0; r < R; ++r) { b[r] = b[r] * rk; sh.rhs[buf][r] = b[r]; }
             }
             mat_sync<NW>();
             if (tid > k && tid < n) {
@@ -156,9 +163,8 @@ __device__ __forceinline__ void chol_solve(const T (&a)[NC], int n, int tid, T (
         for (int k = ktop; k >= c0; --k) {
             const int buf = (k + 1) & 1;
             if (tid == k) {
-                const T ak = pick(k, std::integral_constant<int, c0>{});
 #pragma unroll
-                for (int r = 0; r < R; ++r) { b[r] = b[r] / ak; sh.rhs[buf][r] = b[r]; }
+                for (int r = 0; r < R; ++r) { b[r] = b[r] * rk; sh.rhs[buf][r] = b[r]; }
 #pragma unroll
                 for (int j = 0; j < c0; ++j) sh.row[buf][j] = a[j];
 #pragma unroll
@@ -267,6 +273,7 @@ template <typename T, int NT, int R>
 struct BlockedCholRsShared {
     T sb[32][R];
     T D[32][33];
+    T rD[32];   // 1 / D(i,i) of the current diagonal block
 };
 
 template <typename T, int NT, int R>
@@ -287,11 +294,12 @@ __device__ void blocked_potrs(const T* __restrict__ A, int n, int lda, bool uppe
 #pragma unroll
                 for (int c = 0; c < 32; ++c)
                     if (j0 + c < j1 && j0 + lane < j1 && c <= lane) sh.D[lane][c] = L(j0 + lane, j0 + c);
+                if (j0 + lane < j1) sh.rD[lane] = T(1) / L(j0 + lane, j0 + lane);
                 __syncwarp();
                 for (int k = j0; k < j1; ++k) {
                     if (t == k) {
 #pragma unroll
-                        for (int r = 0; r < R; ++r) { b[r] = b[r] / sh.D[k - j0][k - j0]; sh.sb[k - j0][r] = b[r]; }
+                        for (int r = 0; r < R; ++r) { b[r] = b[r] * sh.rD[k - j0]; sh.sb[k - j0][r] = b[r]; }
                     }
                     __syncwarp();
                     if (t > k && t < j1) {
@@ -313,11 +321,12 @@ __device__ void blocked_potrs(const T* __restrict__ A, int n, int lda, bool uppe
 #pragma unroll
                 for (int c = 0; c < 32; ++c)
                     if (j0 + c < j1 && j0 + lane < j1 && c <= lane) sh.D[lane][c] = L(j0 + lane, j0 + c);
+                if (j0 + lane < j1) sh.rD[lane] = T(1) / L(j0 + lane, j0 + lane);
                 __syncwarp();
                 for (int k = j1 - 1; k >= j0; --k) {
                     if (t == k) {
 #pragma unroll
-                        for (int r = 0; r < R; ++r) { b[r] = b[r] / sh.D[k - j0][k - j0]; sh.sb[k - j0][r] = b[r]; }
+                        for (int r = 0; r < R; ++r) { b[r] = b[r] * sh.rD[k - j0]; sh.sb[k - j0][r] = b[r]; }
                     }
                     __syncwarp();
                     if (t >= j0 && t < k) {

@@ -259,16 +259,18 @@ void oracle_dpotrf(int upper, int n, double* a, int lda, int* info) {
 
 /* LAPACK dpotrs: L y = b (column sweep, reference DTRSM Left Lower NoTrans
  * NonUnit), then L^T x = y by the column sweep of the upper-triangular solve
- * with U = L^T (reference DTRSM Left Upper NoTrans NonUnit loop order). */
+ * with U = L^T (reference DTRSM Left Upper NoTrans NonUnit loop order), except
+ * that b(k) is multiplied by the correctly rounded 1/L(k,k) where DTRSM divides
+ * (the batched kernels' form: no division on the sweep's dependency chain). */
 void oracle_dpotrs(int upper, int n, int nrhs, const double* a, int lda, double* b, int ldb) {
 #define LL(i, j) (*(upper ? &A_(j, i) : &A_(i, j)))
     for (int c = 0; c < nrhs; ++c) {
         for (int k = 0; k < n; ++k) {
-            B_(k, c) = B_(k, c) / LL(k, k);
+            B_(k, c) = B_(k, c) * (1.0 / LL(k, k));
             for (int i = k + 1; i < n; ++i) B_(i, c) = fma(-B_(k, c), LL(i, k), B_(i, c));
         }
         for (int k = n - 1; k >= 0; --k) {
-            B_(k, c) = B_(k, c) / LL(k, k);
+            B_(k, c) = B_(k, c) * (1.0 / LL(k, k));
             for (int i = 0; i < k; ++i) B_(i, c) = fma(-B_(k, c), LL(k, i), B_(i, c));
         }
     }
