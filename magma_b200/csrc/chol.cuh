@@ -276,6 +276,25 @@ struct BlockedCholRsShared {
     T rD[32];   // 1 / D(i,i) of the current diagonal block
 };
 
+// The warp that owns diagonal block [j0, j0+cnt) loads it into shared memory (rows past
+// cnt: zero) with its reciprocals: the loads go out unconditionally, clamped inside the
+// matrix, 8 at a time, so they overlap instead of completing one by one.
+template <typename T, int NT, int R, typename F>
+__device__ __forceinline__ void load_diag_block(BlockedCholRsShared<T, NT, R>& sh, int cnt, int lane, F&& Lb) {
+    const int li = min(lane, cnt - 1);
+#pragma unroll
+    for (int c0 = 0; c0 < 32; c0 += 8) {
+        T v[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) v[c] = Lb(li, min(c0 + c, cnt - 1));
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+            if (c0 + c <= lane && lane < cnt) sh.D[lane][c0 + c] = v[c];
+    }
+    if (lane < cnt) sh.rD[lane] = T(1) / Lb(lane, lane);
+    __syncwarp();
+}
+
 template <typename T, int NT, int R>
 __device__ void blocked_potrs(const T* __restrict__ A, int n, int lda, bool upper, T* __restrict__ B, int nrhs,
                               int ldb, BlockedCholRsShared<T, NT, R>& sh) {
@@ -288,57 +307,54 @@ __device__ void blocked_potrs(const T* __restrict__ A, int n, int lda, bool uppe
         for (int r = 0; r < R; ++r) b[r] = (t < n && c0 + r < nrhs) ? B[t + (size_t)(c0 + r) * ldb] : T(0);
         // forward: L y = b, blocks ascending
         for (int J = 0; J < nblk; ++J) {
-            const int j0 = J * 32, j1 = min(n, j0 + 32);
+            const int j0 = J * 32, j1 = min(n, j0 + 32), cnt = j1 - j0;
             __syncthreads();
             if ((t >> 5) == J) {
+                load_diag_block(sh, cnt, lane, [&](int i, int j) { return L(j0 + i, j0 + j); });
+                // steps unrolled over the block (no loop or branch overhead on the chain)
+                static_for<0, 32>([&](auto kc) {
+                    constexpr int k = decltype(kc)::value;
+                    if (k >= cnt) return;
+                    if (lane == k) {
 #pragma unroll
-                for (int c = 0; c < 32; ++c)
-                    if (j0 + c < j1 && j0 + lane < j1 && c <= lane) sh.D[lane][c] = L(j0 + lane, j0 + c);
-                if (j0 + lane < j1) sh.rD[lane] = T(1) / L(j0 + lane, j0 + lane);
-                __syncwarp();
-                for (int k = j0; k < j1; ++k) {
-                    if (t == k) {
-#pragma unroll
-                        for (int r = 0; r < R; ++r) { b[r] = b[r] * sh.rD[k - j0]; sh.sb[k - j0][r] = b[r]; }
+                        for (int r = 0; r < R; ++r) { b[r] = b[r] * sh.rD[k]; sh.sb[k][r] = b[r]; }
                     }
                     __syncwarp();
-                    if (t > k && t < j1) {
-                        const T l = sh.D[t - j0][k - j0];
+                    if (lane > k && lane < cnt) {
+                        const T l = sh.D[lane][k];
 #pragma unroll
-                        for (int r = 0; r < R; ++r) b[r] = fma_rn(-sh.sb[k - j0][r], l, b[r]);
+                        for (int r = 0; r < R; ++r) b[r] = fma_rn(-sh.sb[k][r], l, b[r]);
                     }
-                }
+                });
             }
             __syncthreads();
             if (t >= j1 && t < n)
-                block_update<T, R, false>(b, sh.sb, j1 - j0, [&](int q) { return L(t, j0 + q); });
+                block_update<T, R, false>(b, sh.sb, cnt, [&](int q) { return L(t, j0 + q); });
         }
         // backward: L^T x = y, blocks descending (column sweep of U = L^T)
         for (int J = nblk - 1; J >= 0; --J) {
-            const int j0 = J * 32, j1 = min(n, j0 + 32);
+            const int j0 = J * 32, j1 = min(n, j0 + 32), cnt = j1 - j0;
             __syncthreads();
             if ((t >> 5) == J) {
+                load_diag_block(sh, cnt, lane, [&](int i, int j) { return L(j0 + i, j0 + j); });
+                static_for<0, 32>([&](auto kc) {
+                    constexpr int k = 31 - decltype(kc)::value;
+                    if (k >= cnt) return;
+                    if (lane == k) {
 #pragma unroll
-                for (int c = 0; c < 32; ++c)
-                    if (j0 + c < j1 && j0 + lane < j1 && c <= lane) sh.D[lane][c] = L(j0 + lane, j0 + c);
-                if (j0 + lane < j1) sh.rD[lane] = T(1) / L(j0 + lane, j0 + lane);
-                __syncwarp();
-                for (int k = j1 - 1; k >= j0; --k) {
-                    if (t == k) {
-#pragma unroll
-                        for (int r = 0; r < R; ++r) { b[r] = b[r] * sh.rD[k - j0]; sh.sb[k - j0][r] = b[r]; }
+                        for (int r = 0; r < R; ++r) { b[r] = b[r] * sh.rD[k]; sh.sb[k][r] = b[r]; }
                     }
                     __syncwarp();
-                    if (t >= j0 && t < k) {
-                        const T u = sh.D[k - j0][t - j0];   // U(t, k) = L(k, t)
+                    if (lane < k) {
+                        const T u = sh.D[k][lane];   // U(t, k) = L(k, t)
 #pragma unroll
-                        for (int r = 0; r < R; ++r) b[r] = fma_rn(-sh.sb[k - j0][r], u, b[r]);
+                        for (int r = 0; r < R; ++r) b[r] = fma_rn(-sh.sb[k][r], u, b[r]);
                     }
-                }
+                });
             }
             __syncthreads();
             if (t < j0)
-                block_update<T, R, true>(b, sh.sb, j1 - j0, [&](int q) { return L(j0 + q, t); });
+                block_update<T, R, true>(b, sh.sb, cnt, [&](int q) { return L(j0 + q, t); });
         }
         if (t < n) {
 #pragma unroll
