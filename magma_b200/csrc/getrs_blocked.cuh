@@ -56,14 +56,22 @@ __device__ __forceinline__ void permute_rows(T (&b)[R], int n, int t, int idx, B
 }
 
 
-// Warp `J` stages the diagonal block A[j0:j1, j0:j1] into shared memory.
+// Warp `J` stages the diagonal block A[j0:j1, j0:j1] into shared memory. The loads go
+// out unconditionally (clamped inside the block), 8 at a time, so they overlap.
 template <typename T, int NT, int R>
 __device__ __forceinline__ void stage_diag(const T* __restrict__ A, int lda, int j0, int j1, int t,
                                            BlockedRsShared<T, NT, R>& sh) {
-    const int lane = t & 31;
+    const int lane = t & 31, cnt = j1 - j0;
+    const int li = j0 + min(lane, cnt - 1);
 #pragma unroll
-    for (int c = 0; c < 32; ++c)
-        if (j0 + c < j1 && j0 + lane < j1) sh.D[lane][c] = A[j0 + lane + (size_t)(j0 + c) * lda];
+    for (int c0 = 0; c0 < 32; c0 += 8) {
+        T v[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) v[c] = A[li + (size_t)(j0 + min(c0 + c, cnt - 1)) * lda];
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+            if (c0 + c < cnt && lane < cnt) sh.D[lane][c0 + c] = v[c];
+    }
     __syncwarp();
 }
 
@@ -89,18 +97,21 @@ __device__ void blocked_getrs(bool trans, const T* __restrict__ A, int n, int ld
                 __syncthreads();
                 if ((t >> 5) == J) {   // the warp that owns rows j0..j1-1 solves the diagonal block
                     stage_diag<T, NT, R>(A, lda, j0, j1, t, sh);
-                    for (int k = j0; k < j1; ++k) {
-                        if (t == k) {
+                    const int lane = t & 31, cnt = j1 - j0;
+                    static_for<0, 32>([&](auto kc) {   // steps unrolled: no loop overhead on the chain
+                        constexpr int k = decltype(kc)::value;
+                        if (k >= cnt) return;
+                        if (lane == k) {
 #pragma unroll
-                            for (int r = 0; r < R; ++r) sh.sb[k - j0][r] = b[r];
+                            for (int r = 0; r < R; ++r) sh.sb[k][r] = b[r];
                         }
                         __syncwarp();
-                        if (t > k && t < j1) {
-                            const T l = sh.D[t - j0][k - j0];
+                        if (lane > k && lane < cnt) {
+                            const T l = sh.D[lane][k];
 #pragma unroll
-                            for (int r = 0; r < R; ++r) b[r] = fma_rn(-sh.sb[k - j0][r], l, b[r]);
+                            for (int r = 0; r < R; ++r) b[r] = fma_rn(-sh.sb[k][r], l, b[r]);
                         }
-                    }
+                    });
                 }
                 __syncthreads();
                 if (t >= j1 && t < n) {
@@ -120,22 +131,25 @@ __device__ void blocked_getrs(bool trans, const T* __restrict__ A, int n, int ld
                 __syncthreads();
                 if ((t >> 5) == J) {
                     stage_diag<T, NT, R>(A, lda, j0, j1, t, sh);
-                    for (int k = j1 - 1; k >= j0; --k) {
-                        if (t == k) {
-                            const T d = sh.D[k - j0][k - j0];
+                    const int lane = t & 31, cnt = j1 - j0;
+                    static_for<0, 32>([&](auto kc) {
+                        constexpr int k = 31 - decltype(kc)::value;
+                        if (k >= cnt) return;
+                        if (lane == k) {
+                            const T d = sh.D[k][k];
 #pragma unroll
                             for (int r = 0; r < R; ++r) {
                                 b[r] = b[r] / d;
-                                sh.sb[k - j0][r] = b[r];
+                                sh.sb[k][r] = b[r];
                             }
                         }
                         __syncwarp();
-                        if (t >= j0 && t < k) {
-                            const T u = sh.D[t - j0][k - j0];
+                        if (lane < k) {
+                            const T u = sh.D[lane][k];
 #pragma unroll
-                            for (int r = 0; r < R; ++r) b[r] = fma_rn(-sh.sb[k - j0][r], u, b[r]);
+                            for (int r = 0; r < R; ++r) b[r] = fma_rn(-sh.sb[k][r], u, b[r]);
                         }
-                    }
+                    });
                 }
                 __syncthreads();
                 if (t < j0) {
@@ -156,22 +170,25 @@ __device__ void blocked_getrs(bool trans, const T* __restrict__ A, int n, int ld
                 __syncthreads();
                 if ((t >> 5) == J) {
                     stage_diag<T, NT, R>(A, lda, j0, j1, t, sh);
-                    for (int k = j0; k < j1; ++k) {
-                        if (t == k) {
-                            const T d = sh.D[k - j0][k - j0];
+                    const int lane = t & 31, cnt = j1 - j0;
+                    static_for<0, 32>([&](auto kc) {
+                        constexpr int k = decltype(kc)::value;
+                        if (k >= cnt) return;
+                        if (lane == k) {
+                            const T d = sh.D[k][k];
 #pragma unroll
                             for (int r = 0; r < R; ++r) {
                                 b[r] = b[r] / d;
-                                sh.sb[k - j0][r] = b[r];
+                                sh.sb[k][r] = b[r];
                             }
                         }
                         __syncwarp();
-                        if (t > k && t < j1) {
-                            const T u = sh.D[k - j0][t - j0];
+                        if (lane > k && lane < cnt) {
+                            const T u = sh.D[k][lane];
 #pragma unroll
-                            for (int r = 0; r < R; ++r) b[r] = fma_rn(-u, sh.sb[k - j0][r], b[r]);
+                            for (int r = 0; r < R; ++r) b[r] = fma_rn(-u, sh.sb[k][r], b[r]);
                         }
-                    }
+                    });
                 }
                 __syncthreads();
                 if (t >= j1 && t < n) {
@@ -191,18 +208,21 @@ __device__ void blocked_getrs(bool trans, const T* __restrict__ A, int n, int ld
                 __syncthreads();
                 if ((t >> 5) == J) {
                     stage_diag<T, NT, R>(A, lda, j0, j1, t, sh);
-                    for (int k = j1 - 1; k >= j0; --k) {
-                        if (t == k) {
+                    const int lane = t & 31, cnt = j1 - j0;
+                    static_for<0, 32>([&](auto kc) {
+                        constexpr int k = 31 - decltype(kc)::value;
+                        if (k >= cnt) return;
+                        if (lane == k) {
 #pragma unroll
-                            for (int r = 0; r < R; ++r) sh.sb[k - j0][r] = b[r];
+                            for (int r = 0; r < R; ++r) sh.sb[k][r] = b[r];
                         }
                         __syncwarp();
-                        if (t >= j0 && t < k) {
-                            const T l = sh.D[k - j0][t - j0];
+                        if (lane < k) {
+                            const T l = sh.D[k][lane];
 #pragma unroll
-                            for (int r = 0; r < R; ++r) b[r] = fma_rn(-l, sh.sb[k - j0][r], b[r]);
+                            for (int r = 0; r < R; ++r) b[r] = fma_rn(-l, sh.sb[k][r], b[r]);
                         }
-                    }
+                    });
                 }
                 __syncthreads();
                 if (t < j0) {
