@@ -152,6 +152,8 @@ dsgesv_refine_kernel(int n, int nrhs, double** dA_array, int lda, int** ipiv_arr
         int iiter = 0, stalls = 0;
         double prev_ratio = 1e300;
         for (;;) {
+            // column t of A to L2 while the solve below runs, for this pass's residual
+            if (t < n) prefetch_l2(A + (size_t)t * lda, (unsigned)n * 8u);
             // C = SA^-1 res in single precision (res = B on the first pass)
             bool ovf = false;
             float f[R];

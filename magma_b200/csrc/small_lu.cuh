@@ -51,6 +51,21 @@ template <> __device__ __forceinline__ float tiny_normal<float>() { return FLT_M
 __device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
 __device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 
+// Asks L2 to fetch [p, p + bytes) ahead of use, without waiting and without
+// registers: a bulk prefetch through the copy engine when p is 16-byte aligned
+// (the size rounded down to whole 16-byte units), else one line at a time.
+// Every byte of the range must lie inside the caller's allocation.
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
+    const unsigned long long a = reinterpret_cast<unsigned long long>(p);
+    if ((a & 15) == 0) {
+        const unsigned sz = bytes & ~15u;
+        if (sz) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(sz) : "memory");
+    } else {
+        for (unsigned off = 0; off < bytes; off += 128)
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const char*>(p) + off));
+    }
+}
+
 // Barrier over the threads that share one matrix.
 template <int NW>
 __device__ __forceinline__ void mat_sync() {
