@@ -183,7 +183,7 @@ dsgesv_refine_kernel(int n, int nrhs, double** dA_array, int lda, int** ipiv_arr
 #pragma unroll
             for (int r = 0; r < R; ++r) res[r] = b[r];
             if (t < n) {
-#pragma unroll 16
+#pragma unroll(NT >= 256 ? 32 : 16)
                 for (int j = 0; j < n; ++j) {
                     const double a = A[t + (size_t)j * lda];
 #pragma unroll

@@ -74,6 +74,13 @@ __device__ __forceinline__ void refine_solve(const float* __restrict__ SA, int n
                                              RefineSmem<NT, R>& sh) {
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
     const int nblk = (n + 31) / 32;
+    // L2 prefetch of the panel a later block step reads: columns of block J2, the rows
+    // below the block (forward sweep) or above it (backward sweep); lane k takes column k.
+    auto prefetch_panel = [&](int J2, bool below) {
+        const int col = J2 * 32 + lane;
+        const int r0 = below ? (J2 + 1) * 32 : 0, r1 = below ? n : J2 * 32;
+        if (col < n && r1 > r0) prefetch_l2(SA + (size_t)col * n + r0, (unsigned)(r1 - r0) * 4u);
+    };
     // block step of the warp that owns block J: f_J <- inv * f_J, published in sx[buf]
     auto diag_step = [&](int J, int which, int buf) {
 #pragma unroll
@@ -97,6 +104,10 @@ __device__ __forceinline__ void refine_solve(const float* __restrict__ SA, int n
     // forward: unit lower L, blocks ascending; rows below the block apply its update
     for (int J = 0; J < nblk; ++J) {
         const int j0 = J * 32, buf = J & 1;
+        if (w == (J == 0 ? 1 : 0)) {   // a warp that is idle in this step prefetches the next one's panel
+            if (J + 1 < nblk) prefetch_panel(J + 1, true);
+            else prefetch_panel(J, false);
+        }
         float lv[32];
         const bool below = (w > J && t < n);
         if (below) {
@@ -116,6 +127,7 @@ __device__ __forceinline__ void refine_solve(const float* __restrict__ SA, int n
     // backward: U, blocks descending; rows above the block apply its update
     for (int J = nblk - 1; J >= 0; --J) {
         const int j0 = J * 32, buf = (2 * nblk - 1 - J) & 1;
+        if (J > 0 && w == (J == nblk - 1 ? 0 : nblk - 1)) prefetch_panel(J - 1, false);
         float uv[32];
         const bool above = (w < J);
         if (above) {
