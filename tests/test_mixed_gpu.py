@@ -112,3 +112,34 @@ def test_dsgesv_tensor_core_lu_fallbacks(cuda):
     assert list(info[[1, 3]]) == list(oinf) and oinf[1] == 11
     be = T.backward_error(A_np[[0, 1, 4]], X.cpu().numpy()[[0, 1, 4]], B_np[[0, 1, 4]], n)
     assert be.max() <= 1e-14
+
+
+@pytest.mark.parametrize("n,nrhs,batch,chunks", [(96, 3, 37, 8), (40, 2, 9, 4), (256, 4, 20, 3)])
+def test_dsgesv_host_pipelined_matches_device_call(cuda, n, nrhs, batch, chunks):
+    """HostDsgesv (pinned host buffers, uploads/solves/read-backs overlapped chunk by chunk)
+    gives the same X, iter and info, bit for bit, as one magma_dsgesv_batched call over the
+    whole batch on device-resident data; one instance takes the FP64 fallback."""
+    import torch
+    import magma_b200 as mb
+    from magma_b200.api import HostDsgesv, default_queue
+    A_np, B_np, kap = T.svd_logrand(batch, n, 1e2, 1e6, nrhs=nrhs, seed=3 * n + batch)
+    A_np[1, 2, 3] = 1e39                                      # overflows FP32 -> FP64 fallback
+    X_d, ipiv_d, it_d, info_d = mb.dsgesv_batched(dev(A_np, cuda), dev(B_np, cuda))
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    hA, hB = pin(A_np), pin(B_np)
+    hX = torch.full((batch, nrhs, n), np.nan, dtype=torch.float64).pin_memory()
+    hI = torch.full((batch,), 99, dtype=torch.int32).pin_memory()
+    hF = torch.full((batch,), 99, dtype=torch.int32).pin_memory()
+    solver = HostDsgesv(batch, n, nrhs, chunks=chunks)
+    assert solver.bounds[0][0] == 0 and solver.bounds[-1][1] == batch and len(solver.bounds) <= chunks
+    for _ in range(2):                                        # the staging buffers are reused
+        hX.fill_(np.nan)
+        solver(hA, hB, hX, hI, hF)
+        default_queue().stream.synchronize()
+        assert np.array_equal(hX.numpy(), X_d.cpu().numpy())
+        assert np.array_equal(hI.numpy(), it_d.cpu().numpy())
+        assert np.array_equal(hF.numpy(), info_d.cpu().numpy())
+    assert hI.numpy()[1] == -2
+    assert T.backward_error(A_np, hX.numpy(), B_np, n).max() <= 1e-14
+    with pytest.raises(ValueError):
+        solver(hA.clone(), hB, hX, hI, hF)                    # not pinned
