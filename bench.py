@@ -415,14 +415,14 @@ class C1DgesvSmall:
         self.h2d = self.hA.numel() * 8 + self.hB.numel() * 8
         self.d2h = self.hX.numel() * 8 + self.hP.numel() * 4 + self.hI.numel() * 4
 
+    e2e_api = "magma_b200.api.HostDgesv, 4 chunks: uploads, solves and read-backs overlapped"
+
     def e2e_step(self, q, i):
-        k = i % self.ring
-        self.A[k].copy_(self.hA, non_blocking=True)
-        self.B[k].copy_(self.hB, non_blocking=True)
-        self.step(q, i)
-        self.hX.copy_(self.B[k], non_blocking=True)
-        self.hP.copy_(self.ipiv, non_blocking=True)
-        self.hI.copy_(self.info, non_blocking=True)
+        if getattr(self, "pipe", None) is None:
+            from magma_b200.api import HostDgesv
+
+            self.pipe = HostDgesv(self.batch, self.n, self.nrhs, chunks=4, queue=q)
+        self.pipe(self.hA, self.hB, self.hX, self.hP, self.hI)
 
     def cpu_reference(self, seconds=10.0, nthreads=None):
         import oracle

@@ -16,13 +16,13 @@ import os
 os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 from . import _lib  # noqa: E402
-from .api import (HostDsgesv, Queue, VarBatch, dgeqrf_batched, dgerbt_batched, dgesv_batched, dgesv_nopiv_batched,  # noqa: E402
+from .api import (HostDgesv, HostDsgesv, Queue, VarBatch, dgeqrf_batched, dgerbt_batched, dgesv_batched, dgesv_nopiv_batched,  # noqa: E402
                   dgesv_rbt_batched, dgesv_vbatched, dgetrf_batched, dgetrf_nopiv_batched, dgetri_outofplace_batched,
                   dgetrs_batched, dgetrs_nopiv_batched, dposv_batched, dposv_vbatched, dpotrf_batched,
                   dpotrs_batched, dsgesv_batched, dsposv_vbatched, gemm_batched, gemm_vbatched, ptr_array,
                   syrk_vbatched, tri_vbatched)
 
-__all__ = ["HostDsgesv", "Queue", "VarBatch", "ptr_array", "dgetrf_batched", "dgetrs_batched", "dgesv_batched", "dpotrf_batched",
+__all__ = ["HostDgesv", "HostDsgesv", "Queue", "VarBatch", "ptr_array", "dgetrf_batched", "dgetrs_batched", "dgesv_batched", "dpotrf_batched",
            "dpotrs_batched", "dposv_batched", "dposv_vbatched", "dsgesv_batched", "dgesv_vbatched", "dsposv_vbatched",
            "dgetri_outofplace_batched", "dgetrf_nopiv_batched", "dgetrs_nopiv_batched", "dgesv_nopiv_batched",
            "dgerbt_batched", "dgesv_rbt_batched", "dgeqrf_batched", "gemm_batched", "gemm_vbatched", "syrk_vbatched",

@@ -261,24 +261,23 @@ def dsgesv_batched(A: torch.Tensor, B: torch.Tensor, queue: Queue | None = None)
     return X, ipiv, it, info
 
 
-class HostDsgesv:
-    """Mixed-precision batched solve of systems that live in pinned host memory, with the
-    transfers pipelined against the solves.
+class _HostPipeline:
+    """Batched solve of systems that live in pinned host memory, with the transfers
+    pipelined against the solves.
 
-    The batch is cut into `chunks` slices. All slices' uploads (A and B) are queued on one
-    copy stream, back to back, so the host-to-device link never idles; slice c is solved
-    by magma_dsgesv_batched on the queue's stream as soon as its upload has landed, and its
-    X, iter and info go back to the host on a second copy stream while later slices are
-    still uploading or solving. Results per instance are those of one magma_dsgesv_batched
-    call over the whole batch (every kernel works instance by instance).
+    The batch is cut into `chunks` slices. All slices' uploads are queued on one copy
+    stream, back to back, so the host-to-device link never idles; slice c is solved on the
+    queue's stream as soon as its upload has landed, and its results go back to the host on
+    a second copy stream while later slices are still uploading or solving. Every kernel
+    works instance by instance, so the results equal those of one call over the whole batch.
 
     A call is asynchronous: it returns once everything is queued, and the queue's stream
     waits for the last read-back, so a stream synchronize (or an event recorded on that
     stream) covers the whole transfer-solve-transfer sequence. Device staging buffers,
     streams and pointer arrays are allocated once, at construction."""
 
-    def __init__(self, batch: int, n: int, nrhs: int, chunks: int = 8, queue: Queue | None = None,
-                 lda: int | None = None, ldb: int | None = None):
+    def __init__(self, batch: int, n: int, nrhs: int, chunks: int, queue: Queue | None, lda: int | None,
+                 ldb: int | None):
         if batch < 1 or n < 1 or nrhs < 1 or chunks < 1:
             raise ValueError("batch, n, nrhs and chunks must be positive")
         self.q = queue or default_queue()
@@ -286,28 +285,28 @@ class HostDsgesv:
         self.lda, self.ldb = lda or n, ldb or n
         if self.lda < n or self.ldb < n:
             raise ValueError("lda and ldb must be at least n")
-        dev = torch.device("cuda", torch.cuda.current_device())
-        f64 = dict(dtype=torch.float64, device=dev)
+        self.dev = torch.device("cuda", torch.cuda.current_device())
+        f64 = dict(dtype=torch.float64, device=self.dev)
         self.A = torch.empty((batch, n, self.lda), **f64)
         self.B = torch.empty((batch, nrhs, self.ldb), **f64)
-        self.X = torch.empty((batch, nrhs, n), **f64)
-        self.ipiv = torch.zeros((batch, n), dtype=torch.int32, device=dev)
-        self.iter = torch.zeros(batch, dtype=torch.int32, device=dev)
-        self.info = torch.zeros(batch, dtype=torch.int32, device=dev)
-        self.pA, self.pB, self.pX, self.pP = ptr_array(self.A), ptr_array(self.B), ptr_array(self.X), ptr_array(self.ipiv)
+        self.ipiv = torch.zeros((batch, n), dtype=torch.int32, device=self.dev)
+        self.info = torch.zeros(batch, dtype=torch.int32, device=self.dev)
+        self.pA, self.pB, self.pP = ptr_array(self.A), ptr_array(self.B), ptr_array(self.ipiv)
         per = -(-batch // chunks)
         self.bounds = [(c0, min(batch, c0 + per)) for c0 in range(0, batch, per)]
-        self.up, self.down = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+        self.up, self.down = torch.cuda.Stream(self.dev), torch.cuda.Stream(self.dev)
 
-    def __call__(self, hA: torch.Tensor, hB: torch.Tensor, hX: torch.Tensor, hIter: torch.Tensor,
-                 hInfo: torch.Tensor) -> None:
-        """hA (batch, n, lda) and hB (batch, nrhs, ldb) in, hX (batch, nrhs, n), hIter and
-        hInfo (batch, int32) out; all pinned host tensors."""
-        for t in (hA, hB, hX, hIter, hInfo):
+    def _run(self, hA, hB, reads, solve) -> None:
+        """Uploads hA/hB, calls solve(c0, c1) per slice on the queue's stream and copies
+        each (host, device) pair of `reads` back slice by slice."""
+        for t in (hA, hB, *(h for h, _ in reads)):
             if t.is_cuda or not t.is_pinned():
-                raise ValueError("HostDsgesv takes pinned host tensors")
+                raise ValueError(f"{type(self).__name__} takes pinned host tensors")
         if tuple(hA.shape) != tuple(self.A.shape) or tuple(hB.shape) != tuple(self.B.shape):
             raise ValueError("hA/hB shapes differ from the ones the solver was built for")
+        for h, d in reads:
+            if tuple(h.shape) != tuple(d.shape) or h.dtype != d.dtype:
+                raise ValueError(f"output of shape {tuple(h.shape)} ({h.dtype}) expected {tuple(d.shape)} ({d.dtype})")
         ws = self.q.stream
         self.up.wait_stream(ws)       # earlier work on the staging buffers is ordered first
         self.down.wait_stream(ws)
@@ -317,20 +316,63 @@ class HostDsgesv:
                 self.A[c0:c1].copy_(hA[c0:c1], non_blocking=True)
                 self.B[c0:c1].copy_(hB[c0:c1], non_blocking=True)
                 landed.append(self.up.record_event())
-        L = self.q.lib
         for (c0, c1), ev in zip(self.bounds, landed):
             ws.wait_event(ev)
+            solve(c0, c1)
+            solved = ws.record_event()
+            self.down.wait_event(solved)
+            with torch.cuda.stream(self.down):
+                for h, d in reads:
+                    h[c0:c1].copy_(d[c0:c1], non_blocking=True)
+        ws.wait_stream(self.down)
+
+
+class HostDsgesv(_HostPipeline):
+    """magma_dsgesv_batched (FP32 LU, FP64 refinement, FP64 fallback) on systems in pinned
+    host memory, uploads and read-backs overlapped with the solves chunk by chunk."""
+
+    def __init__(self, batch: int, n: int, nrhs: int, chunks: int = 8, queue: Queue | None = None,
+                 lda: int | None = None, ldb: int | None = None):
+        super().__init__(batch, n, nrhs, chunks, queue, lda, ldb)
+        self.X = torch.empty((batch, nrhs, n), dtype=torch.float64, device=self.dev)
+        self.iter = torch.zeros(batch, dtype=torch.int32, device=self.dev)
+        self.pX = ptr_array(self.X)
+
+    def __call__(self, hA: torch.Tensor, hB: torch.Tensor, hX: torch.Tensor, hIter: torch.Tensor,
+                 hInfo: torch.Tensor) -> None:
+        """hA (batch, n, lda) and hB (batch, nrhs, ldb) in, hX (batch, nrhs, n), hIter and
+        hInfo (batch, int32) out; all pinned host tensors."""
+        L = self.q.lib
+
+        def solve(c0, c1):
             _check(L.magma_dsgesv_batched(self.n, self.nrhs, _vp(self.pA[c0:]), self.lda, _vp(self.pP[c0:]),
                                           _vp(self.pB[c0:]), self.ldb, _vp(self.pX[c0:]), self.n,
                                           _vp(self.iter[c0:]), _vp(self.info[c0:]), c1 - c0, self.q.handle),
                    "magma_dsgesv_batched")
-            solved = ws.record_event()
-            self.down.wait_event(solved)
-            with torch.cuda.stream(self.down):
-                hX[c0:c1].copy_(self.X[c0:c1], non_blocking=True)
-                hIter[c0:c1].copy_(self.iter[c0:c1], non_blocking=True)
-                hInfo[c0:c1].copy_(self.info[c0:c1], non_blocking=True)
-        ws.wait_stream(self.down)
+
+        self._run(hA, hB, [(hX, self.X), (hIter, self.iter), (hInfo, self.info)], solve)
+
+
+class HostDgesv(_HostPipeline):
+    """magma_dgesv_batched (FP64 LU with partial pivoting + solve) on systems in pinned host
+    memory, uploads and read-backs overlapped with the solves chunk by chunk."""
+
+    def __init__(self, batch: int, n: int, nrhs: int, chunks: int = 4, queue: Queue | None = None,
+                 lda: int | None = None, ldb: int | None = None):
+        super().__init__(batch, n, nrhs, chunks, queue, lda, ldb)
+
+    def __call__(self, hA: torch.Tensor, hB: torch.Tensor, hX: torch.Tensor, hIpiv: torch.Tensor,
+                 hInfo: torch.Tensor) -> None:
+        """hA (batch, n, lda) and hB (batch, nrhs, ldb) in; hX (batch, nrhs, ldb) = the
+        solutions, hIpiv (batch, n) and hInfo (batch,) int32 out; all pinned host tensors."""
+        L = self.q.lib
+
+        def solve(c0, c1):
+            _check(L.magma_dgesv_batched(self.n, self.nrhs, _vp(self.pA[c0:]), self.lda, _vp(self.pP[c0:]),
+                                         _vp(self.pB[c0:]), self.ldb, _vp(self.info[c0:]), c1 - c0, self.q.handle),
+                   "magma_dgesv_batched")
+
+        self._run(hA, hB, [(hX, self.B), (hIpiv, self.ipiv), (hInfo, self.info)], solve)
 
 
 # ------------------------------------------------------------------------------- GEMM

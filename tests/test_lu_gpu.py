@@ -215,3 +215,31 @@ def test_blocked_singular(cuda):
     assert info[1] == 78 and info[2] == 1
     assert np.array_equal(info, oinf) and np.array_equal(ipiv, oip)
     assert np.array_equal(np.nan_to_num(LU), np.nan_to_num(O))
+
+
+@pytest.mark.parametrize("n,nrhs,batch,chunks", [(32, 1, 1001, 4), (20, 3, 5, 8), (100, 2, 33, 3)])
+def test_gesv_host_pipelined_matches_oracle(cuda, n, nrhs, batch, chunks):
+    """HostDgesv (pinned host buffers, uploads/solves/read-backs overlapped chunk by chunk)
+    returns the oracle's X, ipiv and info bit for bit; one instance is singular."""
+    import torch
+    from magma_b200.api import HostDgesv, default_queue
+    A_np, B_np = T.lu_uniform(batch, n, nrhs, seed=5 * n + batch)
+    A_np[2, 4, :] = 0.0                                      # column 5 zero -> info = 5
+    OA, OB = A_np.copy(), B_np.copy()
+    oip, oinf = oracle.dgesv_batched(OA, OB)
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    hA, hB = pin(A_np), pin(B_np)
+    hX = torch.full(B_np.shape, np.nan, dtype=torch.float64).pin_memory()
+    hP = torch.zeros((batch, n), dtype=torch.int32).pin_memory()
+    hI = torch.full((batch,), 99, dtype=torch.int32).pin_memory()
+    solver = HostDgesv(batch, n, nrhs, chunks=chunks)
+    for _ in range(2):                                       # the staging buffers are reused
+        hX.fill_(np.nan)
+        solver(hA, hB, hX, hP, hI)
+        default_queue().stream.synchronize()
+        assert np.array_equal(hP.numpy(), oip)
+        assert np.array_equal(hI.numpy(), oinf) and oinf[2] == 5
+        ok = oinf == 0
+        assert np.array_equal(hX.numpy()[ok], OB[ok])
+    with pytest.raises(ValueError):
+        solver(hA, hB, hX, hP[:, :1].clone().pin_memory(), hI)   # wrong output shape
