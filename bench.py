@@ -1263,6 +1263,18 @@ DEFAULT_STEPS = {"c3": (60, 5), "c1": (20000, 50), "c2": (50, 5), "c4": (20, 3),
 
 
 # ---------------------------------------------------------------------- main
+def max_over_ranks(vals, dist, device=None):
+    """Element-wise maximum of per-rank timings over all ranks (every rank receives the
+    result); the job's time is its slowest replica's. `dist` None: one rank, unchanged."""
+    if dist is None:
+        return [float(v) for v in vals]
+    import torch
+
+    t = torch.tensor([float(v) for v in vals], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
 def dist_setup(args):
     import torch
 
@@ -1550,11 +1562,7 @@ def main():
         if dist:
             dist.barrier()
         ms_e2e = timed(stream, lambda i: W.e2e_step(q, i), ke)
-    vals = [ms_total, ms_e2e, extra.get("alt_ms_per_step", 0.0) * args.steps]
-    if dist:
-        t = torch.tensor(vals, device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        vals = [float(v) for v in t.tolist()]
+    vals = max_over_ranks([ms_total, ms_e2e, extra.get("alt_ms_per_step", 0.0) * args.steps], dist, dev)
     ms_total, ms_e2e, ms_alt_total = vals
     units = W.units() * world
     value = units * args.steps / (ms_total * 1e-3)
