@@ -9,7 +9,6 @@ import numpy as np
 import pytest
 
 import oracle
-from magma_b200 import testing as T
 
 pytestmark = pytest.mark.gpu
 
