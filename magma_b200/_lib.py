@@ -24,6 +24,7 @@ MagmaNoTrans, MagmaTrans, MagmaConjTrans = 111, 112, 113
 MagmaUpper, MagmaLower, MagmaFull = 121, 122, 123
 MagmaNonUnit, MagmaUnit = 131, 132
 MagmaLeft, MagmaRight = 141, 142
+MagmaFalse, MagmaTrue = 0, 1
 
 MAGMA_SUCCESS = 0
 MAGMA_ERR_NOT_SUPPORTED = -103

@@ -93,3 +93,57 @@ def test_server_submit_argument_errors():
     assert lib.magma_b200_server_submit(None, 0, 4, 1, p, 3, p, 4, p, 4, 0) == -5
     assert lib.magma_b200_server_submit(None, 0, 4, 1, p, 4, p, 4, p, 2, 0) == -9
     assert lib.magma_b200_server_submit(None, 0, 2000, 1, p, 2000, p, 2000, p, 2000, 0) == _lib.MAGMA_ERR_NOT_SUPPORTED
+
+
+def test_cholesky_argument_errors(q):
+    lib = _lib.load()
+    L, U = _lib.MagmaLower, _lib.MagmaUpper
+    # potrf: uplo -1, n -2, ldda -4; batchCount 0 keeps the info reset off the device
+    assert lib.magma_dpotrf_batched(7, 4, None, 4, None, 0, q) == -1
+    assert lib.magma_dpotrf_batched(L, -1, None, 4, None, 0, q) == -2
+    assert lib.magma_dpotrf_batched(U, 4, None, 3, None, 0, q) == -4
+    assert lib.magma_dpotrf_batched(L, 0, None, 1, None, 0, q) == 0
+    # potrs / posv test every argument in turn and report the last failure,
+    # as src/zpotrs_batched.cpp:79-88 and src/zposv_batched.cpp:99-108 do
+    for f, tail in ((lib.magma_dpotrs_batched, (1, q)), (lib.magma_dposv_batched, (None, 1, q))):
+        assert f(7, 4, 1, None, 4, None, 4, *tail) == -1
+        assert f(L, -1, 1, None, 4, None, 4, *tail) == -2
+        assert f(L, 4, -1, None, 4, None, 4, *tail) == -3
+        assert f(U, 4, 1, None, 3, None, 4, *tail) == -5
+        assert f(L, 4, 1, None, 4, None, 3, *tail) == -7
+        assert f(7, 4, 1, None, 3, None, 3, *tail) == -7
+        assert f(L, 0, 1, None, 1, None, 1, *tail) == 0
+
+
+def test_mixed_inverse_nopiv_rbt_argument_errors(q):
+    lib = _lib.load()
+    # magma_dsgesv_batched: n -1, nrhs -2, ldda -4, lddb -7, lddx -9
+    f = lib.magma_dsgesv_batched
+    assert f(-1, 1, None, 4, None, None, 4, None, 4, None, None, 1, q) == -1
+    assert f(4, -1, None, 4, None, None, 4, None, 4, None, None, 1, q) == -2
+    assert f(4, 1, None, 3, None, None, 4, None, 4, None, None, 1, q) == -4
+    assert f(4, 1, None, 4, None, None, 3, None, 4, None, None, 1, q) == -7
+    assert f(4, 1, None, 4, None, None, 4, None, 3, None, None, 1, q) == -9
+    assert f(0, 1, None, 1, None, None, 1, None, 1, None, None, 1, q) == 0
+    # magma_dgetri_outofplace_batched: n -1, ldda -3, lddia -6
+    g = lib.magma_dgetri_outofplace_batched
+    assert g(-1, None, 4, None, None, 4, None, 1, q) == -1
+    assert g(4, None, 3, None, None, 4, None, 1, q) == -3
+    assert g(4, None, 4, None, None, 3, None, 1, q) == -6
+    assert g(0, None, 1, None, None, 1, None, 1, q) == 0
+    # magma_dgesv_nopiv_batched: n -1, nrhs -2, ldda -4, lddb -6
+    h = lib.magma_dgesv_nopiv_batched
+    assert h(-1, 1, None, 4, None, 4, None, 1, q) == -1
+    assert h(4, -1, None, 4, None, 4, None, 1, q) == -2
+    assert h(4, 1, None, 3, None, 4, None, 1, q) == -4
+    assert h(4, 1, None, 4, None, 3, None, 1, q) == -6
+    # magma_dgerbt_batched: gen -1, n -2, nrhs -3, ldda -5, lddb -7, also written to the
+    # host info argument (src/zgerbt_batched.cpp:129-142)
+    info = C.c_int(123)
+    r = lib.magma_dgerbt_batched
+    assert r(5, 4, 1, None, 4, None, 4, None, None, C.byref(info), 1, q) == -1 and info.value == -1
+    assert r(_lib.MagmaTrue, -4, 1, None, 4, None, 4, None, None, C.byref(info), 1, q) == -2 and info.value == -2
+    assert r(_lib.MagmaFalse, 4, -1, None, 4, None, 4, None, None, C.byref(info), 1, q) == -3
+    assert r(_lib.MagmaFalse, 4, 1, None, 3, None, 4, None, None, C.byref(info), 1, q) == -5
+    assert r(_lib.MagmaFalse, 4, 1, None, 4, None, 3, None, None, C.byref(info), 1, q) == -7 and info.value == -7
+    assert r(_lib.MagmaFalse, 0, 1, None, 1, None, 1, None, None, C.byref(info), 1, q) == 0 and info.value == 0
