@@ -346,8 +346,8 @@ magma_int_t magma_dposv_vbatched_max_nocheck(magma_uplo_t uplo, magma_int_t* n, 
 
 /* ------------------------------------------------------------------------
  * Kernel-variant tuning (no reference counterpart; takes the role of the
- * reference's static tables control/batched_kernel_param.h and
- * magmablas/gemm_config/*.h). The table holds 9 values: the GEMM tile variant
+ * reference's static tables control/batched_kernel_param.h and the headers
+ * under magmablas/gemm_config/). The table holds 9 values: the GEMM tile variant
  * (0: 64x64, 1: 32x32, 2: 16x16) for max(M,N) <= 16, <= 32, <= 64 and larger,
  * first for FP64 then FP32, and 1/0 for the tensor-core LU in
  * magma_dsgesv_batched (n = 96..256, step 32). Defaults are built in;

@@ -49,7 +49,6 @@ struct GemmTile {
 using GemmTile0 = GemmTile<64, 64, 4, 4, 2, 3>;     // 256 threads
 using GemmTile1 = GemmTile<32, 32, 4, 4, 10, 16>;   // 64 threads
 using GemmTile2 = GemmTile<16, 16, 2, 2, 16, 16>;   // 64 threads
-constexpr int kGemmVariants = 3;
 
 template <typename T, bool TA, bool TB, typename S>
 __global__ void __launch_bounds__(S::NT, (sizeof(T) == 8 ? S::MINB_D : S::MINB_F))
@@ -248,7 +247,7 @@ static void gemm_batched(const char* name, magma_trans_t ta, magma_trans_t tb, i
         return;
     }
     if (m <= 0 || n <= 0 || k <= 0 || batch <= 0) return;
-    GemmSizes g{m, n, k, lda, ldb, ldc, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    GemmSizes g{m, n, k, lda, ldb, ldc, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0};
     gemm_launch<T>(ta, tb, g, alpha, A, B, beta, C, batch, m, n, queue->stream);
 }
 
@@ -258,7 +257,7 @@ static void gemm_vbatched_max_nocheck(magma_trans_t ta, magma_trans_t tb, int* m
                                       const T* const* A, int* lda, const T* const* B, int* ldb, T beta, T** C,
                                       int* ldc, int batch, int max_m, int max_n, int max_k, magma_queue_t queue) {
     if (max_m <= 0 || max_n <= 0 || max_k <= 0 || batch <= 0) return;
-    GemmSizes g{0, 0, 0, 0, 0, 0, m, n, k, lda, ldb, ldc};
+    GemmSizes g{0, 0, 0, 0, 0, 0, m, n, k, lda, ldb, ldc, 0};
     gemm_launch_var<T>(ta, tb, g, alpha, A, B, beta, C, batch, max_m, max_n, queue);
 }
 
