@@ -189,7 +189,7 @@ void ref_dgetri_batched(int n, double* A, int lda, long sA, int* ipiv, long sP, 
     }
 }
 
-/* dtrsm (solve != 0) or dtrmm per instance (testing_ztrsm_vbatched.cpp, testing_ztrmm_vbatched.cpp). */
+/* dtrsm (solve != 0) or dtrmm per instance (testing_ztrsm_vbatched.cpp:327, testing_ztrmm_vbatched.cpp:238). */
 void ref_dtri_vbatched(int solve, int left, int lower, int trans, int unit, const int* m, const int* n, double alpha,
                        double* const* A, const int* lda, double* const* B, const int* ldb, int batch, int nthreads) {
     const char sd = left ? 'L' : 'R', ul = lower ? 'L' : 'U', tr = trans ? 'T' : 'N', dg = unit ? 'U' : 'N';
@@ -201,7 +201,7 @@ void ref_dtri_vbatched(int solve, int left, int lower, int trans, int unit, cons
     }
 }
 
-/* dsyrk per instance (testing_zsyrk_vbatched.cpp). */
+/* dsyrk per instance (testing_zsyrk_vbatched.cpp:244). */
 void ref_dsyrk_vbatched(int lower, int trans, const int* n, const int* k, double alpha, double* const* A,
                         const int* lda, double beta, double* const* C, const int* ldc, int batch, int nthreads) {
     const char ul = lower ? 'L' : 'U', tr = trans ? 'T' : 'N';

@@ -93,7 +93,9 @@ void oracle_dgetrf_nopiv_batched(int m, int n, double* A, int lda, long strideA,
         oracle_dgetf2_nopiv(m, n, A + (size_t)i * strideA, lda, ipiv + (size_t)i * strideP, info + i);
 }
 
-/* LAPACK 3.x dgeqr2 (Householder QR: dlarfg, then dlarf on the trailing columns), with
+/* The reference's QR tester checks magma_zgeqrf_batched against host LAPACK zgeqrf, one
+ * instance at a time (testing/testing_zgeqrf_batched.cpp:224).
+ * LAPACK 3.x dgeqr2 (Householder QR: dlarfg, then dlarf on the trailing columns), with
  * the summation order of the batched path written out: the rows of a column are dealt
  * to P lanes (row r to lane r mod P, P = 1, 2, 4, 8 for m <= 16, 32, 64, 256); each
  * lane sums its rows in ascending order with fma, and the P partial sums are added as
@@ -287,7 +289,10 @@ void oracle_dposv_vbatched(int upper, const int* n, const int* nrhs, double* con
     }
 }
 
-/* Triangular solve / multiply (BLAS dtrsm / dtrmm semantics) in the batched kernels'
+/* The reference's testers check the batched triangular routines against host BLAS:
+ * ztrsm (testing/testing_ztrsm_vbatched.cpp:327) and ztrmm
+ * (testing/testing_ztrmm_vbatched.cpp:238), one instance at a time.
+ * Triangular solve / multiply (BLAS dtrsm / dtrmm semantics) in the batched kernels'
  * order of operations. The call is seen as a left problem on T (nr x nr) and X
  * (nr x nc): side Left: T = op(A), X = B; side Right: T = op(A)^T, X = B^T. Rows are
  * renumbered q (q = i, or nr-1-i) so that T is lower in q for the solve and upper for
