@@ -36,3 +36,13 @@ def test_reference_arm_runs_on_rank_0_only():
     r = run_bench(ARGS, WORLD_SIZE="2", RANK="1", LOCAL_RANK="1")
     assert r.returncode == 0, r.stderr[-2000:]
     assert r.stdout.strip() == ""
+
+
+def test_reference_arm_without_a_counterpart_says_unavailable():
+    """The request loop (c5) has no reference implementation: one `unavailable` line, exit 0."""
+    r = run_bench(["--impl", "reference", "--workload", "c5", "--steps", "1", "--warmup", "3"])
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["unavailable"]
