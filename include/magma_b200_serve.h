@@ -50,8 +50,10 @@ magma_int_t magma_b200_server_submit(magma_b200_server_t server, magma_int_t kin
                                      const double* A, magma_int_t lda, const double* B, magma_int_t ldb, double* X,
                                      magma_int_t ldx, long long tag);
 
-/* Reports up to `max` completed requests (each once): tag, LAPACK info,
- * submit and completion times (steady clock, ns). Returns the count. */
+/* Reports up to `max` completed requests (each once): tag, info, submit and
+ * completion times (steady clock, ns). info is LAPACK's (0, or > 0 for the first
+ * zero pivot / non-positive minor), or a negative MAGMA error code when the solver
+ * call of the request's batch failed. Returns the count. */
 magma_int_t magma_b200_server_poll(magma_b200_server_t server, long long* tags, magma_int_t* infos,
                                    long long* t_submit_ns, long long* t_done_ns, magma_int_t max);
 

@@ -183,6 +183,7 @@ struct Slot {
     std::vector<Request*> reqs;
     bool busy = false;
     int cls = 0;              // size class this slot serves
+    int rc[2] = {0, 0};       // return code of the batch's LU / Cholesky solver call
 };
 
 constexpr int kClasses = 2;
@@ -244,17 +245,18 @@ void magma_b200_server::launch(Slot& s) {
         }
     }
     cudaMemcpyAsync(s.d_meta, s.h_meta, 2 * meta.bytes, cudaMemcpyHostToDevice, s.stream);
+    s.rc[0] = s.rc[1] = 0;
     for (int f = 0; f < 2; ++f) {
         if (!cnt[f]) continue;
         char* d = s.d_meta + f * meta.bytes;
         auto I = [&](size_t o) { return reinterpret_cast<int*>(d + o); };
         auto P = [&](size_t o) { return reinterpret_cast<double**>(d + o); };
         if (f == MAGMA_B200_SOLVE_LU)
-            magma_dgesv_vbatched_max_nocheck(I(meta.n), I(meta.nrhs), P(meta.pa), I(meta.lda),
+            s.rc[f] = magma_dgesv_vbatched_max_nocheck(I(meta.n), I(meta.nrhs), P(meta.pa), I(meta.lda),
                                              reinterpret_cast<int**>(d + meta.pp), P(meta.pb), I(meta.ldb),
                                              I(meta.info), cnt[f], maxn[f], maxr[f], s.queue);
         else
-            magma_dposv_vbatched_max_nocheck(MagmaLower, I(meta.n), I(meta.nrhs), P(meta.pa), I(meta.lda),
+            s.rc[f] = magma_dposv_vbatched_max_nocheck(MagmaLower, I(meta.n), I(meta.nrhs), P(meta.pa), I(meta.lda),
                                              P(meta.pb), I(meta.ldb), I(meta.info), cnt[f], maxn[f], maxr[f],
                                              s.queue);
     }
@@ -332,7 +334,9 @@ void magma_b200_server::complete_loop(int cls) {
         int idx[2] = {0, 0};
         for (Request* r : s->reqs) {
             const int* info = reinterpret_cast<const int*>(s->h_meta + r->kind * meta.bytes + meta.info);
-            r->info = info[idx[r->kind]++];
+            const int k = idx[r->kind]++;
+            // a failed solver call leaves no info behind: report its MAGMA error code instead
+            r->info = s->rc[r->kind] != 0 ? s->rc[r->kind] : info[k];
             r->t_done = t;
             arena.release(r->off, r->bytes);
             finished.push_back(r);
