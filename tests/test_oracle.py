@@ -209,3 +209,26 @@ def test_oracle_tri_alpha_zero():
     B = np.ones((4, 5))
     oracle.dtri(True, True, True, False, False, 5, 4, 0.0, A, B)
     assert np.all(B == 0.0)
+
+
+@pytest.mark.parametrize("m,n", [(32, 32), (40, 24), (17, 30), (64, 64)])
+def test_oracle_nopiv_is_the_pivoted_lu_when_the_diagonal_wins(m, n):
+    """On column-wise diagonally dominant instances partial pivoting keeps every diagonal
+    pivot, so the no-pivoting LU (the oracle of magma_dgetrf_nopiv_batched) must equal the
+    pivoted getf2 restatement bit for bit -- that one is pinned to LAPACK on the golden
+    vectors -- and LAPACK's own dgetrf to rounding, with LAPACK's identity pivots."""
+    rng = np.random.default_rng(100 * m + n)
+    batch, k = 20, min(m, n)
+    A = rng.uniform(-1, 1, (batch, n, m))                   # column-major (batch, n, lda = m)
+    for i in range(k):
+        A[:, i, i] += max(m, n)
+    P, Q, L = A.copy(), A.copy(), A.copy()
+    ip_n, inf_n = oracle.dgetrf_nopiv_batched(P, m)
+    ip_p, inf_p = oracle.dgetrf_batched(Q, m)
+    ident = np.tile(np.arange(1, k + 1, dtype=np.int32), (batch, 1))
+    assert np.array_equal(ip_p[:, :k], ident)                # no interchange happened
+    assert np.array_equal(P, Q)
+    assert not inf_n.any() and not inf_p.any()
+    ip_l, inf_l = oracle.lapack_dgetrf_batched(L, m)
+    assert np.array_equal(ip_l[:, :k], ident) and not inf_l.any()
+    assert np.abs(P - L).max() <= 8 * max(m, n) * EPS * np.abs(A).max()
