@@ -66,7 +66,8 @@ def default_queue() -> Queue:
 
 def ptr_array(t: torch.Tensor) -> torch.Tensor:
     """Device array (int64) of per-instance base pointers of a batched tensor."""
-    assert t.is_cuda
+    if not t.is_cuda:
+        raise ValueError("ptr_array needs a CUDA tensor (the library takes device pointer arrays)")
     n = t.shape[0]
     step = t.stride(0) * t.element_size()
     return t.data_ptr() + torch.arange(n, device=t.device, dtype=torch.int64) * step

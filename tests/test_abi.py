@@ -147,3 +147,13 @@ def test_mixed_inverse_nopiv_rbt_argument_errors(q):
     assert r(_lib.MagmaFalse, 4, 1, None, 3, None, 4, None, None, C.byref(info), 1, q) == -5
     assert r(_lib.MagmaFalse, 4, 1, None, 4, None, 3, None, None, C.byref(info), 1, q) == -7 and info.value == -7
     assert r(_lib.MagmaFalse, 0, 1, None, 1, None, 1, None, None, C.byref(info), 1, q) == 0 and info.value == 0
+
+
+def test_ptr_array_rejects_host_tensors():
+    """The Python binding builds MAGMA's device pointer arrays; a host tensor is an error."""
+    import torch
+
+    from magma_b200.api import ptr_array
+
+    with pytest.raises(ValueError):
+        ptr_array(torch.zeros((2, 3, 3), dtype=torch.float64))
