@@ -30,7 +30,11 @@ synchronisation on both sides, measured with CUDA events on the library's
 stream, max over ranks. The c3 inputs (1 GiB of A) exceed the 126 MB L2; c3
 re-creates its overwritten inputs on the device between steps, outside the
 per-step event brackets (the FP64 form overwrites A with its factors); c1
-cycles through a ring of input buffers larger than L2. N > 1 runs one replica
+cycles through a ring of input buffers larger than L2 (each slot reset to the
+original inputs after use, outside the brackets). Every workload whose metric is
+"solves/s at bwd err <= 1e-14" checks the outputs of its last timed step (and of
+its second arm's) against that bar on every instance, with info == 0; a miss
+exits non-zero with no JSON line. N > 1 runs one replica
 per GPU on its own batch (instances are independent; no collective on the
 data path; scaling "weak").
 
@@ -63,6 +67,18 @@ os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 METRIC = "solves/s at bwd err ≤1e-14: mixed-prec vs FP64 on 1 B200; p50/p99 latency"
 L2_BYTES = 126 * 2**20
 FP64_NOMINAL_TFLOPS = 37.0   # B200 dense FP64 (CUDA cores / DMMA), nominal
+BWD_BAR = 1e-14              # the metric's accuracy bar: normwise backward error per instance
+
+
+def accuracy_gate(tag, be, info):
+    """The metric's bar on one step's outputs: every instance's normwise backward error
+    <= BWD_BAR and info == 0 (the inputs are well-posed). `be` and `info` are tensors over
+    the instances. Returns ({tag_bwd_err_max, tag_info_nonzero, tag_ok}, ok)."""
+    worst = float(be.max().item()) if be.numel() else 0.0
+    bad_be = int((~(be <= BWD_BAR)).sum().item())          # NaN counts as a miss
+    nz = int((info != 0).sum().item())
+    ok = bad_be == 0 and nz == 0
+    return {f"{tag}_bwd_err_max": worst, f"{tag}_over_bar": bad_be, f"{tag}_info_nonzero": nz}, ok
 
 
 def host_cpu() -> dict:
@@ -260,6 +276,22 @@ class C3Mixed:
         self.A.copy_(self.A0)
         return {"bwd_err_max_mixed": be_mixed, "bwd_err_max_fp64": be_64, "iter_hist": hist}
 
+    def check_last(self, q):
+        """The bar on the last timed mixed step's outputs (X, info) for every instance."""
+        from magma_b200.testing import backward_error_torch
+
+        q.sync()
+        return accuracy_gate("last_step_mixed", backward_error_torch(self.A0, self.X, self.B0).amax(dim=1),
+                             self.info)
+
+    def check_last_alt(self, q):
+        """The bar on the last timed FP64 step's outputs (B overwritten by X, info)."""
+        from magma_b200.testing import backward_error_torch
+
+        q.sync()
+        return accuracy_gate("last_step_fp64", backward_error_torch(self.A0, self.B64, self.B0).amax(dim=1),
+                             self.info)
+
     def dominant_kernel(self, q, stream, reps=5):
         """Per-stage device times of the mixed step (queue stage timing: CUDA events the
         library records on its stream between the LU, refinement and fallback stages);
@@ -344,14 +376,17 @@ class C1DgesvSmall:
         self.A_np, self.B_np = T.lu_uniform(batch, n, nrhs, seed=seed)
         step_bytes = 8 * batch * (n * n + n * nrhs)
         self.ring = max(2, -(-3 * L2_BYTES // step_bytes))
-        self.A = [torch.from_numpy(self.A_np).to(dev) for _ in range(self.ring)]
-        self.B = [torch.from_numpy(self.B_np).to(dev) for _ in range(self.ring)]
+        self.A0 = torch.from_numpy(self.A_np).to(dev)
+        self.B0 = torch.from_numpy(self.B_np).to(dev)
+        self.A = [self.A0.clone() for _ in range(self.ring)]
+        self.B = [self.B0.clone() for _ in range(self.ring)]
         self.ipiv = torch.zeros((batch, n), dtype=torch.int32, device=dev)
         self.info = torch.zeros(batch, dtype=torch.int32, device=dev)
         self.pA = [ptr_array(a) for a in self.A]
         self.pB = [ptr_array(b) for b in self.B]
         self.pP = ptr_array(self.ipiv)
-        self.l2 = f"ring of {self.ring} distinct input buffers ({step_bytes / 2**20:.0f} MiB each) > L2"
+        self.l2 = (f"ring of {self.ring} distinct input buffers ({step_bytes / 2**20:.0f} MiB each) > L2, each reset "
+                   f"to the original inputs after use, outside the per-step event brackets")
 
     def units(self):
         return self.batch
@@ -366,10 +401,29 @@ class C1DgesvSmall:
     def launches_per_step(self):
         return 1
 
+    def restore(self, i):
+        """Step i reads ring slot i % ring. restore(0) resets every slot to the original
+        inputs; restore(i) resets the slot step i-1 used, which is next read ring-1 steps
+        later (more than twice L2 of traffic in between), so every step solves the original
+        systems from HBM."""
+        slots = range(self.ring) if i == 0 else [(i - 1) % self.ring]
+        for k in slots:
+            self.A[k].copy_(self.A0)
+            self.B[k].copy_(self.B0)
+
     def step(self, q, i):
         k = i % self.ring
+        self.last = k
         return q.lib.magma_dgesv_batched(self.n, self.nrhs, vp(self.pA[k]), self.n, vp(self.pP), vp(self.pB[k]),
                                          self.n, vp(self.info), self.batch, q.handle)
+
+    def check_last(self, q):
+        """The bar on the last timed step's outputs (its ring slot's X, info) for every instance."""
+        from magma_b200.testing import backward_error_torch
+
+        q.sync()
+        return accuracy_gate("last_step_fp64", backward_error_torch(self.A0, self.B[self.last], self.B0).amax(dim=1),
+                             self.info)
 
     def validate(self, q):
         from magma_b200 import testing as T
@@ -873,6 +927,21 @@ class C4CholVbatched:
         return {"bwd_err_max_fp64": be64, "bwd_err_max_mixed": bem, "iter_hist_mixed": hist, "info_nonzero": nz64,
                 "bwd_err_sample": len(sample)}
 
+    def _bwd_all(self, X):
+        from magma_b200.testing import backward_error_vbatched_torch
+
+        return backward_error_vbatched_torch(self.A0, X, self.B0, self.n, self.nrhs, self.offA, self.offB)
+
+    def check_last(self, q):
+        """The bar on the last timed FP64 step's outputs (B overwritten by X, info), every instance."""
+        q.sync()
+        return accuracy_gate("last_step_fp64", self._bwd_all(self.B), self.info[:self.batch])
+
+    def check_last_alt(self, q):
+        """The bar on the last timed mixed step's outputs (X, info), every instance."""
+        q.sync()
+        return accuracy_gate("last_step_mixed", self._bwd_all(self.X), self.info[:self.batch])
+
     def dominant_kernel(self, q, stream, reps=5):
         ms = timed_restore(stream, lambda i: self.step(q, i), self.restore, reps) / reps
         alg = float((16.0 * self.n ** 2 + 16.0 * self.n * self.nrhs + 4).sum())
@@ -1209,6 +1278,16 @@ class NopivBatched:
     def ratios(self, value, alt_value):
         return {"rbt_over_nopiv": alt_value / value}
 
+    def check_last(self, q, tag="last_step_nopiv"):
+        """The bar on the last timed step's outputs (B overwritten by X, info), every instance."""
+        from magma_b200.testing import backward_error_torch
+
+        q.sync()
+        return accuracy_gate(tag, backward_error_torch(self.A0, self.B, self.B0).amax(dim=1), self.info)
+
+    def check_last_alt(self, q):
+        return self.check_last(q, "last_step_rbt")
+
     def validate(self, q):
         from magma_b200 import testing as T
 
@@ -1543,6 +1622,12 @@ def main():
             dist.barrier()
         clk = clocks.stop()
         assert all(rc == 0 for rc in rcs), f"library returned {set(rcs)}"
+        gate = {}
+        gate_ok = all(v <= BWD_BAR for k, v in checks.items() if k.startswith("bwd_err_max"))
+        if hasattr(W, "check_last"):
+            g, ok = W.check_last(q)
+            gate.update(g)
+            gate_ok &= ok
         extra = {}
         if hasattr(W, "step_alt"):
             for i in range(3):
@@ -1551,6 +1636,10 @@ def main():
             torch.cuda.synchronize(dev)
             ms_alt = timed_restore(stream, lambda i: W.step_alt(q, i), W.restore_alt, args.steps)
             extra["alt_ms_per_step"] = ms_alt / args.steps
+            if hasattr(W, "check_last_alt"):
+                g, ok = W.check_last_alt(q)
+                gate.update(g)
+                gate_ok &= ok
         dom = W.dominant_kernel(q, stream)
         extras = W.extras(q, stream) if hasattr(W, "extras") else {}
         # end to end (host buffers, copies inside each step)
@@ -1562,8 +1651,16 @@ def main():
         if dist:
             dist.barrier()
         ms_e2e = timed(stream, lambda i: W.e2e_step(q, i), ke)
-    vals = max_over_ranks([ms_total, ms_e2e, extra.get("alt_ms_per_step", 0.0) * args.steps], dist, dev)
-    ms_total, ms_e2e, ms_alt_total = vals
+    vals = max_over_ranks([ms_total, ms_e2e, extra.get("alt_ms_per_step", 0.0) * args.steps,
+                           0.0 if gate_ok else 1.0], dist, dev)
+    ms_total, ms_e2e, ms_alt_total, gate_failed = vals
+    if gate_failed:
+        # a step that missed the metric's accuracy bar has no throughput to report
+        sys.stderr.write(f"bench: accuracy bar (backward error <= {BWD_BAR:g}, info == 0) missed on the last "
+                         f"timed step: {json.dumps(gate)}\n")
+        if dist:
+            dist.destroy_process_group()
+        sys.exit(3)
     units = W.units() * world
     value = units * args.steps / (ms_total * 1e-3)
     if rank == 0:
@@ -1577,6 +1674,9 @@ def main():
                        "parallelism": f"replicas x{world}", "l2": W.l2},
         }
         line.update(checks)
+        line.update(gate)
+        if gate:
+            line["accuracy_gate"] = f"passed: every instance of the last timed step(s) at backward error <= {BWD_BAR:g}, info 0"
         line.update(extras)
         if ms_alt_total:
             alt_value = units * args.steps / (ms_alt_total * 1e-3)

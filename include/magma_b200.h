@@ -73,6 +73,14 @@ cudaStream_t magma_queue_get_cuda_stream(magma_queue_t queue);
  * it before capturing batched calls into a CUDA graph. */
 magma_int_t  magma_queue_reserve_workspace(magma_queue_t queue, size_t bytes);
 
+/* No reference counterpart. Caps the queue's device workspace at `bytes` (a
+ * workspace already larger is freed after the queue's stream drains). A call that
+ * would need more returns MAGMA_ERR_DEVICE_ALLOC before enqueueing any work, as
+ * the reference does when its per-call cudaMalloc fails (src/zgetrf_batched.cpp:
+ * 172-194, src/zpotrf_vbatched.cpp:99,124). For callers with a fixed device-memory
+ * budget. Returns MAGMA_SUCCESS, or -1 for a null queue. */
+magma_int_t  magma_b200_queue_set_workspace_limit(magma_queue_t queue, size_t bytes);
+
 /* No reference counterpart (the reference's timers are host wall clocks around
  * whole calls). With stage timing on, multi-kernel routines record CUDA events
  * on the queue's stream at their stage boundaries -- magma_dgesv_batched
@@ -81,6 +89,14 @@ magma_int_t  magma_queue_reserve_workspace(magma_queue_t queue, size_t bytes);
  * (waits for its last event; returns the number of stages written, <= max). */
 magma_int_t  magma_b200_stage_timing(magma_queue_t queue, magma_int_t enable);
 magma_int_t  magma_b200_stage_times(magma_queue_t queue, float* ms, magma_int_t max);
+
+/* No reference counterpart; a test hook. With cycles > 0, the tensor-core LU of
+ * magma_dsgesv_batched issues no tensor-core work and bounds each completion wait
+ * at `cycles` clock cycles, so the first wait runs out with nothing in flight: the
+ * kernel raises its error flag, releases its tensor memory and hands its instances
+ * to the FP64 fallback (iter -3), the path a real time-out takes. 0 restores normal
+ * operation. Process-wide; for tests only. */
+void magma_b200_debug_tc_wait_limit(long long cycles);
 
 #define magma_queue_create(device, queue_ptr) \
         magma_queue_create_internal(device, queue_ptr, __func__, __FILE__, __LINE__)
@@ -392,7 +408,14 @@ void magma_sgemm_batched(magma_trans_t transA, magma_trans_t transB, magma_int_t
 /* Variable-size GEMM, m/n/k/ldda/lddb/lddc device arrays of batchCount+1 entries.
  * magmablas/zgemm_vbatched.cpp:235-271 (checked; one host synchronisation for the
  * checker and the maxima), :19-29 (_max_nocheck), :33 (_max), :81 (_nocheck);
- * checks as magmablas/vbatched_check.cu:78-99 (batchCount -14). */
+ * checks as magmablas/vbatched_check.cu:78-99 (batchCount -14).
+ * Argument order of _max_nocheck and _max: (..., lddc, batchCount, max_m, max_n, max_k,
+ * queue), as the reference DEFINES them (magmablas/zgemm_vbatched.cpp:19-29, 46-56) and as
+ * every caller inside the reference passes them (magmablas/ztrsm_vbatched_core.cu:235-236,
+ * zgemm_vbatched.cpp:99-106, testing/testing_zgemm_vbatched.cpp:244-251). The reference's
+ * public header declares (max_m, max_n, max_k, batchCount) instead
+ * (include/magma_zvbatched.h:90-112); the four are all magma_int_t, so the reference reads
+ * them in definition order whatever a caller compiled against, and so does this library. */
 void magmablas_dgemm_vbatched(magma_trans_t transA, magma_trans_t transB, magma_int_t* m, magma_int_t* n,
                               magma_int_t* k, double alpha, double const* const* dA_array, magma_int_t* ldda,
                               double const* const* dB_array, magma_int_t* lddb, double beta, double** dC_array,

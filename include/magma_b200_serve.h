@@ -57,6 +57,14 @@ magma_int_t magma_b200_server_submit(magma_b200_server_t server, magma_int_t kin
 magma_int_t magma_b200_server_poll(magma_b200_server_t server, long long* tags, magma_int_t* infos,
                                    long long* t_submit_ns, long long* t_done_ns, magma_int_t max);
 
+/* Caps the device workspace of each of the server's stream queues at `bytes`
+ * (magma_b200_queue_set_workspace_limit; the workspace reserved at creation is
+ * released when larger). Waits until no batch is in flight first. A micro-batch
+ * whose solver call then needs more workspace fails with MAGMA_ERR_DEVICE_ALLOC,
+ * and every request of that batch reports the code as its info. Returns
+ * MAGMA_SUCCESS. */
+magma_int_t magma_b200_server_set_workspace_limit(magma_b200_server_t server, size_t bytes);
+
 /* Blocks until every submitted request has completed. */
 magma_int_t magma_b200_server_drain(magma_b200_server_t server);
 

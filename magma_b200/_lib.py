@@ -50,8 +50,10 @@ SIGNATURES: dict[str, tuple] = {
     "magma_queue_get_device": (_i, [_p]),
     "magma_queue_get_cuda_stream": (_p, [_p]),
     "magma_queue_reserve_workspace": (_i, [_p, _sz]),
+    "magma_b200_queue_set_workspace_limit": (_i, [_p, _sz]),
     "magma_b200_stage_timing": (_i, [_p, _i]),
     "magma_b200_stage_times": (_i, [_p, _p, _i]),
+    "magma_b200_debug_tc_wait_limit": (None, [C.c_longlong]),
     "magma_setvector_internal": (None, [_i, _i, _p, _i, _p, _i, _p, _s, _s, _i]),
     "magma_getvector_internal": (None, [_i, _i, _p, _i, _p, _i, _p, _s, _s, _i]),
     "magma_setvector_async_internal": (None, [_i, _i, _p, _i, _p, _i, _p, _s, _s, _i]),
@@ -151,6 +153,7 @@ SIGNATURES: dict[str, tuple] = {
     "magma_b200_server_submit": (_i, [_p, _i, _i, _i, _p, _i, _p, _i, _p, _i, C.c_longlong]),
     "magma_b200_server_poll": (_i, [_p, _p, _p, _p, _p, _i]),
     "magma_b200_server_drain": (_i, [_p]),
+    "magma_b200_server_set_workspace_limit": (_i, [_p, _sz]),
     "magma_b200_server_stats": (None, [_p, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                                        C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "magma_b200_server_destroy": (_i, [_p]),

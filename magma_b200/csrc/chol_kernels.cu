@@ -164,7 +164,7 @@ static void launch_potrf_blocked(const WorkList& wl, int bound, bool persistent,
                                  T** A, int* info, cudaStream_t s) {
     auto k = potrf_blocked_kernel<T, NB, NT, CW, CB>;
     const int smem = (int)sizeof(BlockedCholShared<T, NB, NT, CW>);
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    ensure_dynamic_smem((const void*)k, smem);
     k<<<grid_for(k, NT, bound, persistent, smem), NT, smem, s>>>(wl, sz, upper, A, info);
 }
 

@@ -18,7 +18,13 @@
 // stream capture. Every call reuses the same array, and its bucket counters
 // are cleared at the start of each call; two calls whose work overlaps on the
 // GPU (different streams, no ordering between them) would race on it, so
-// callers must order them (for example by using one stream).
+// callers must order them (for example by using one stream). The cached
+// address belongs to the device's current context: after cudaDeviceReset (or
+// anything else that destroys and recreates the primary context) the module is
+// loaded again, possibly elsewhere, so a process that resets a device must not
+// call this entry point on it afterwards. The size buckets run one after another
+// on the queue's stream (the allocating entry point spreads them over auxiliary
+// streams), so a batch of mixed sizes takes somewhat longer here.
 #include "internal.h"
 #include "chol_launch.h"
 #include "vbatched.h"
@@ -39,14 +45,24 @@ static std::mutex g_scratch_mutex;
 // Device address of g_chol_noalloc_scratch on `device` (looked up once, with
 // that device current); nullptr if the lookup fails.
 static int* noalloc_scratch(int device) {
-    if (device < 0 || device >= kNoAllocMaxDevices) return nullptr;
+    if (device < 0 || device >= kNoAllocMaxDevices) {
+        std::fprintf(stderr, "magma_dpotrf_vbatched_max_nocheck_noalloc: device %d is outside the %d devices "
+                     "this entry point serves\n", device, kNoAllocMaxDevices);
+        return nullptr;
+    }
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
     if (!g_scratch_addr[device]) {
         int prev = -1;
-        if (cudaGetDevice(&prev) != cudaSuccess) return nullptr;
-        if (prev != device && cudaSetDevice(device) != cudaSuccess) return nullptr;
+        cudaError_t e = cudaGetDevice(&prev);
+        if (e == cudaSuccess && prev != device) e = cudaSetDevice(device);
+        if (e != cudaSuccess) {
+            std::fprintf(stderr, "magma_dpotrf_vbatched_max_nocheck_noalloc: cannot make device %d current: %s\n",
+                         device, cudaGetErrorString(e));
+            cudaGetLastError();
+            return nullptr;
+        }
         int* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void**>(&p), g_chol_noalloc_scratch);
+        e = cudaGetSymbolAddress(reinterpret_cast<void**>(&p), g_chol_noalloc_scratch);
         if (prev != device) cudaSetDevice(prev);
         if (e != cudaSuccess) {
             std::fprintf(stderr, "libmagma_b200: cudaGetSymbolAddress(g_chol_noalloc_scratch) failed: %s\n",

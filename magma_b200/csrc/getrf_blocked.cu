@@ -59,7 +59,7 @@ static void launch_getrf_blocked(const WorkList& wl, int bound, bool persistent,
                                  int* info, cudaStream_t s) {
     auto k = getrf_blocked_kernel<T, NB, NT, CW, CB>;
     const int smem = (int)sizeof(BlockedLuShared<T, NB, NT, CW>);
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    ensure_dynamic_smem((const void*)k, smem);
     k<<<blocked_grid(k, NT, bound, persistent, smem), NT, smem, s>>>(wl, sz, A, ipiv, info);
 }
 

@@ -23,13 +23,7 @@ static int small_grid(int nw, int bound, bool persistent) {
     const int mpb = (nw == 1) ? 4 : 1;
     const int items = ceildiv(bound, mpb);
     if (!persistent) return items;
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    }
-    return std::max(1, std::min(items, sms * (nw == 1 ? 3 : 4)));
+    return std::max(1, std::min(items, device_sm_count() * (nw == 1 ? 3 : 4)));
 }
 
 // Dispatch on the column bound (8, 16, 32, 64) and warps per matrix (rows / 32).

@@ -17,9 +17,10 @@ struct magma_queue {
     int          device;
     cudaStream_t stream;
     bool         own_stream;
-    // grow-only workspace owned by the queue
+    // grow-only workspace owned by the queue, never larger than ws_limit
     void*        ws;
     size_t       ws_bytes;
+    size_t       ws_limit;
     // host-pinned staging word used by routines that must read one value back
     int*         h_flag;
     // auxiliary streams for independent work (size buckets), created on first use
@@ -38,7 +39,9 @@ namespace mb200 {
 // Returns a device workspace of at least `bytes` on `queue`, growing it when
 // needed. Growing synchronises the queue's stream (the old buffer may still be
 // in use by enqueued work) -- callers that capture CUDA graphs reserve the
-// workspace once before capture with magma_queue_reserve_workspace().
+// workspace once before capture with magma_queue_reserve_workspace(). Returns
+// nullptr when the allocation fails or `bytes` exceeds the queue's limit
+// (magma_b200_queue_set_workspace_limit); callers report MAGMA_ERR_DEVICE_ALLOC.
 void* queue_workspace(magma_queue_t queue, size_t bytes);
 
 // Fork/join of the queue's auxiliary streams: queue_fork makes every auxiliary
@@ -69,5 +72,12 @@ inline magma_int_t launch_status() {
 }
 
 inline int ceildiv(long a, long b) { return (int)((a + b - 1) / b); }
+
+// SM count of the current device (looked up once per device).
+int device_sm_count();
+
+// Raises `kernel`'s dynamic shared-memory limit on the current device to at least
+// `bytes`, calling cudaFuncSetAttribute only the first time per (kernel, device, size).
+void ensure_dynamic_smem(const void* kernel, int bytes);
 
 }  // namespace mb200

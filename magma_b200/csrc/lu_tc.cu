@@ -27,6 +27,7 @@
 #include "tc_ptx.cuh"
 #include "lu_tc.h"
 #include <cfloat>
+#include <atomic>
 #include <climits>
 
 namespace mb200 {
@@ -218,7 +219,7 @@ lu_tf32x3_kernel(TcLuArgs g) {
             tc::fence_proxy_async_smem();
             tc::fence_before_sync();
             __syncthreads();
-            if (t == 0) {
+            if (t == 0 && g.issue_mma) {
                 tc::fence_after_sync();
                 const uint32_t idesc = tc::idesc_tf32(128, ncols, true);   // D += (-L21) U12
                 const int halves = (n + 127) / 128;
@@ -237,10 +238,10 @@ lu_tf32x3_kernel(TcLuArgs g) {
                 }
                 tc::commit(mbar);
             }
-            // bounded wait for the update (about 4 s)
+            // bounded wait for the update (about 4 s unless the test hook shortens it)
             bool done = false;
             const long long t0 = clock64();
-            while (!(done = tc::mbar_try_wait(mbar, phase)) && clock64() - t0 < (1ll << 33)) {
+            while (!(done = tc::mbar_try_wait(mbar, phase)) && clock64() - t0 < g.wait_limit) {
             }
             phase ^= 1u;
             if (__syncthreads_or(!done)) {
@@ -271,15 +272,23 @@ size_t lu_tc_smem_bytes() { return sizeof(TcLuSmem) + 1024; }
 // Two blocks of this kernel must never share an SM: each allocates all 512 TMEM columns.
 static_assert(2 * (sizeof(TcLuSmem) + 1024) > 228 * 1024, "one tensor-core LU block per SM");
 
-magma_int_t lu_tc_launch(const TcLuArgs& args, cudaStream_t s) {
+// Test hook state: > 0 replaces the completion-wait bound and suppresses the MMAs.
+static std::atomic<long long> g_test_wait_limit{0};
+
+magma_int_t lu_tc_launch(const TcLuArgs& in, cudaStream_t s) {
+    TcLuArgs args = in;
+    const long long hook = g_test_wait_limit.load(std::memory_order_relaxed);
+    args.wait_limit = hook > 0 ? hook : (1ll << 33);
+    args.issue_mma = hook > 0 ? 0 : 1;
     const int smem = (int)lu_tc_smem_bytes();
-    cudaFuncSetAttribute(lu_tf32x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    int sms = 0, dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int grid = std::max(1, std::min(args.batch, sms));
+    ensure_dynamic_smem((const void*)lu_tf32x3_kernel, smem);
+    const int grid = std::max(1, std::min(args.batch, device_sm_count()));
     lu_tf32x3_kernel<<<grid, kTcNT, smem, s>>>(args);
     return launch_status();
 }
 
 }  // namespace mb200
+
+extern "C" void magma_b200_debug_tc_wait_limit(long long cycles) {
+    mb200::g_test_wait_limit.store(cycles > 0 ? cycles : 0, std::memory_order_relaxed);
+}

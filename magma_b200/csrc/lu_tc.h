@@ -15,6 +15,8 @@ struct TcLuArgs {
     int* fail_count;   // instances for the FP64 fallback
     int* fail_list;
     int* err;          // set to 1 when a tensor-core wait timed out
+    long long wait_limit;   // clock cycles a tensor-core completion wait may take
+    int issue_mma;          // 0 only under the time-out test hook: no tensor-core work is issued
 };
 
 bool lu_tc_supported(int n);

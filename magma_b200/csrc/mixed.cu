@@ -246,7 +246,7 @@ static void launch_refine(int n, int nrhs, double** A, int lda, int** ipiv, doub
                           const MixedWs& w, int* iter, int batch, cudaStream_t s) {
     auto k = dsgesv_refine_kernel<NT, R>;
     const int smem = (int)sizeof(RefineSmem<NT, R>);
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    ensure_dynamic_smem((const void*)k, smem);
     k<<<batch, NT, smem, s>>>(n, nrhs, A, lda, ipiv, B, ldb, X, ldx, w, iter);
 }
 
@@ -273,7 +273,8 @@ magma_int_t dsgesv_batched(int n, int nrhs, double** dA, int lda, int** ipiv, do
     if (use_tensor_core_lu(n)) {
         // 1+2. conversion, norm and an FP32-accurate LU on the tensor cores, TMEM-resident
         cudaMemsetAsync(w.err, 0, sizeof(int), s);
-        const TcLuArgs args{n, batch, lda, dA, w.SA, ipiv, w.sinfo, w.anrm, iter, w.fail_count, w.fail_list, w.err};
+        const TcLuArgs args{n, batch, lda, dA, w.SA, ipiv, w.sinfo, w.anrm, iter, w.fail_count, w.fail_list, w.err,
+                            0, 1};   // wait bound and MMA issue are set by lu_tc_launch
         if ((rc = lu_tc_launch(args, s))) return rc;
     } else {
         // 1. conversion + norm

@@ -345,7 +345,7 @@ static void launch_bucket_stage(int stage, const WorkList& wl, int batch, const 
     } else {
         auto k = dsposv_refine_vkernel<NT, R>;
         const int smem = (int)sizeof(CholRefineSmem<NT, R>);
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        ensure_dynamic_smem((const void*)k, smem);
         k<<<persistent_grid(k, NT, smem, batch), NT, smem, s>>>(wl, n, nrhs, A, lda, B, ldb, X, ldx, S, ws, iter);
     }
 }

@@ -8,6 +8,7 @@
 #include <algorithm>
 
 #include <atomic>
+#include <cstdint>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -117,6 +118,7 @@ void magma_queue_create_internal(magma_device_t device, magma_queue_t* queue_ptr
     q->own_stream = true;
     q->ws = nullptr;
     q->ws_bytes = 0;
+    q->ws_limit = SIZE_MAX;
     q->h_flag = nullptr;
     q->aux_ready = false;
     q->stage_on = false;
@@ -138,6 +140,7 @@ void magma_queue_create_from_cuda_internal(magma_device_t device, cudaStream_t s
     q->stream = stream;
     q->ws = nullptr;
     q->ws_bytes = 0;
+    q->ws_limit = SIZE_MAX;
     q->h_flag = nullptr;
     q->aux_ready = false;
     q->stage_on = false;
@@ -302,8 +305,10 @@ void queue_join(magma_queue_t queue) {
 
 void* queue_workspace(magma_queue_t queue, size_t bytes) {
     if (bytes <= queue->ws_bytes) return queue->ws;
-    // round up to 2 MiB so that small growth steps do not reallocate
+    if (bytes > queue->ws_limit) return nullptr;
+    // round up to 2 MiB so that small growth steps do not reallocate (within the limit)
     size_t want = (bytes + (size_t(2) << 20) - 1) & ~((size_t(2) << 20) - 1);
+    want = std::min(want, queue->ws_limit);
     if (queue->ws) {
         cudaStreamSynchronize(queue->stream);
         cudaFree(queue->ws);
@@ -322,6 +327,18 @@ void* queue_workspace(magma_queue_t queue, size_t bytes) {
 }  // namespace mb200
 
 extern "C" {
+
+magma_int_t magma_b200_queue_set_workspace_limit(magma_queue_t queue, size_t bytes) {
+    if (!queue) return -1;
+    queue->ws_limit = bytes;
+    if (queue->ws_bytes > bytes) {   // the queue holds no more than its limit from here on
+        cudaStreamSynchronize(queue->stream);
+        cudaFree(queue->ws);
+        queue->ws = nullptr;
+        queue->ws_bytes = 0;
+    }
+    return MAGMA_SUCCESS;
+}
 
 magma_int_t magma_b200_stage_timing(magma_queue_t queue, magma_int_t enable) {
     if (!queue) return -1;

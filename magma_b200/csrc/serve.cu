@@ -443,6 +443,19 @@ magma_int_t magma_b200_server_drain(magma_b200_server_t sv) {
     return MAGMA_SUCCESS;
 }
 
+magma_int_t magma_b200_server_set_workspace_limit(magma_b200_server_t sv, size_t bytes) {
+    std::unique_lock<std::mutex> lk(sv->mu);
+    // no batch in flight: the dispatcher marks a slot busy under this lock before launching
+    sv->cv_drain.wait(lk, [&] {
+        for (const Slot& s : sv->slots)
+            if (s.busy) return false;
+        return true;
+    });
+    cudaSetDevice(sv->device);
+    for (Slot& s : sv->slots) magma_b200_queue_set_workspace_limit(s.queue, bytes);
+    return MAGMA_SUCCESS;
+}
+
 void magma_b200_server_stats(magma_b200_server_t sv, long long* submitted, long long* completed, long long* batches,
                              long long* peak_bytes) {
     std::lock_guard<std::mutex> lk(sv->mu);

@@ -9,6 +9,9 @@
 // its own list.
 #include "internal.h"
 #include "vbatched.h"
+#include <mutex>
+#include <map>
+#include <atomic>
 
 namespace mb200 {
 
@@ -114,16 +117,41 @@ magma_int_t ld_slack1(const int* rows, const int* ld, int batch, magma_queue_t q
     return ld_slack_impl(rows, ld, batch, queue, out, 1);
 }
 
-int resident_blocks(const void* kernel, int threads, size_t smem) {
-    static int sms = 0;
-    if (sms == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+int device_sm_count() {
+    constexpr int kMaxDev = 64;
+    static std::atomic<int> sms[kMaxDev] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= kMaxDev) {
+        int v = 0;
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        return max(1, v);
     }
+    int v = sms[dev].load(std::memory_order_relaxed);
+    if (v == 0) {
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        v = max(1, v);
+        sms[dev].store(v, std::memory_order_relaxed);
+    }
+    return v;
+}
+
+void ensure_dynamic_smem(const void* kernel, int bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, int> done;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(mu);
+    int& have = done[{kernel, dev}];
+    if (have >= bytes) return;
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess) have = bytes;
+    else cudaGetLastError();   // the launch that follows reports the failure
+}
+
+int resident_blocks(const void* kernel, int threads, size_t smem) {
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
-    return max(1, per_sm) * sms;
+    return max(1, per_sm) * device_sm_count();
 }
 
 }  // namespace mb200

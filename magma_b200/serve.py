@@ -53,6 +53,10 @@ class Server:
     def drain(self) -> None:
         self.lib.magma_b200_server_drain(self.h)
 
+    def set_workspace_limit(self, nbytes: int) -> None:
+        """Caps each stream queue's device workspace (magma_b200_server_set_workspace_limit)."""
+        self.lib.magma_b200_server_set_workspace_limit(self.h, nbytes)
+
     def stats(self) -> dict:
         v = [C.c_longlong() for _ in range(4)]
         self.lib.magma_b200_server_stats(self.h, *[C.byref(x) for x in v])

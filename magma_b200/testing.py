@@ -180,3 +180,59 @@ def backward_error_torch(A_cm, X_cm, B_cm):
     R = Bm - A @ X
     anorm = A.abs().sum(dim=2).amax(dim=1)
     return R.abs().amax(dim=1) / (anorm[:, None] * X.abs().amax(dim=1) + Bm.abs().amax(dim=1))
+
+
+def backward_error_vbatched_torch(A_flat, X_flat, B_flat, ns, nrhss, offA, offB):
+    """Per-instance normwise backward error (max over RHS) of a variable-size batch on the GPU.
+
+    A_flat, X_flat, B_flat are flat FP64 CUDA tensors; instance i is the n_i x n_i
+    column-major block at offA[i] (lda = n_i) and its n_i x nrhs_i right-hand sides
+    and solutions at offB[i] (ldb = n_i). Instances are grouped by order; RHS columns
+    past an instance's own count are masked out. Returns a (batch,) FP64 tensor."""
+    import torch
+
+    ns, nrhss = np.asarray(ns), np.asarray(nrhss)
+    dev = A_flat.device
+    out = torch.zeros(len(ns), dtype=torch.float64, device=dev)
+    for n in np.unique(ns):
+        n = int(n)
+        ids = np.nonzero(ns == n)[0]
+        if n == 0:
+            continue
+        rmax = int(nrhss[ids].max())
+        ia = torch.from_numpy(np.asarray(offA)[ids]).to(dev)[:, None] + torch.arange(n * n, device=dev)[None, :]
+        A = A_flat[ia].reshape(len(ids), n, n).transpose(1, 2)                 # row-major view
+        r = torch.arange(rmax, device=dev)
+        live = r[None, :] < torch.from_numpy(nrhss[ids]).to(dev)[:, None]       # (k, rmax)
+        ib = (torch.from_numpy(np.asarray(offB)[ids]).to(dev)[:, None, None] + (r * n)[None, :, None]
+              + torch.arange(n, device=dev)[None, None, :])
+        ib = torch.where(live[:, :, None], ib, torch.zeros_like(ib))
+        X = torch.where(live[:, :, None], X_flat[ib], 0.0).transpose(1, 2)     # (k, n, rmax)
+        B = torch.where(live[:, :, None], B_flat[ib], 0.0).transpose(1, 2)
+        R = B - A @ X
+        anorm = A.abs().sum(dim=2).amax(dim=1)
+        be = R.abs().amax(dim=1) / (anorm[:, None] * X.abs().amax(dim=1) + B.abs().amax(dim=1))
+        be = torch.where(live, be, torch.zeros_like(be))
+        out[torch.from_numpy(ids).to(dev)] = be.amax(dim=1)
+    return out
+
+
+def lu_residual_torch(A0_cm, LU_cm, ipiv):
+    """MAGMA's getrf check ||P A - L U||_F / (||A||_F n) per instance on the GPU, for square
+    column-major (batch, n, n) tensors and 1-based LAPACK pivots (batch, n)."""
+    import torch
+
+    batch, n, _ = A0_cm.shape
+    piv = np.asarray(ipiv.cpu() if hasattr(ipiv, "cpu") else ipiv).astype(np.int64) - 1
+    perm = np.tile(np.arange(n), (batch, 1))
+    rows = np.arange(batch)
+    for j in range(n):                                   # LAPACK's sequential interchanges
+        p = piv[:, j]
+        pj, pp = perm[rows, j].copy(), perm[rows, p].copy()
+        perm[rows, j], perm[rows, p] = pp, pj
+    A = A0_cm.transpose(1, 2)                            # row-major views
+    LU = LU_cm.transpose(1, 2)
+    PA = torch.gather(A, 1, torch.from_numpy(perm).to(A.device)[:, :, None].expand(batch, n, n))
+    eye = torch.eye(n, dtype=LU.dtype, device=LU.device)
+    R = PA - (torch.tril(LU, -1) + eye) @ torch.triu(LU)
+    return torch.linalg.norm(R, dim=(1, 2)) / (torch.linalg.norm(A, dim=(1, 2)) * n)

@@ -117,3 +117,42 @@ def test_gemm_vbatched_argument_errors(cuda, capfd):
     assert "parameter 8" in capfd.readouterr().err
     mb.gemm_vbatched(A, A, A, [4], [4], [4], [4], [4], [2])
     assert "parameter 13" in capfd.readouterr().err
+
+
+@pytest.mark.parametrize("variant", ["max_nocheck", "max"])
+def test_gemm_vbatched_max_argument_order(cuda, variant):
+    """The _max_nocheck and _max forms take (..., lddc, batchCount, max_m, max_n, max_k, queue):
+    the order of the reference's definitions (magmablas/zgemm_vbatched.cpp:19-29, 46-56)
+    and of every call inside the reference (magmablas/ztrsm_vbatched_core.cu:235-236,
+    zgemm_vbatched.cpp:99-106, testing/testing_zgemm_vbatched.cpp:244-251), which its
+    public header declares as (max_m, max_n, max_k, batchCount). Called here with
+    batchCount 5 and distinct maxima 16, 24, 40 over 40 allocated instances: the five
+    products must be right and instances 5..39 untouched."""
+    import ctypes as C
+
+    import torch
+
+    from magma_b200.api import VarBatch, default_queue
+    q = default_queue()
+    total, live = 40, 5
+    M = np.full(total, 8, np.int32)
+    N = np.full(total, 8, np.int32)
+    K = np.full(total, 8, np.int32)
+    M[:live], N[:live], K[:live] = [16, 3, 9, 16, 1], [24, 5, 24, 2, 7], [40, 11, 3, 40, 8]
+    As = [T.normal(21, 3 * i, int(K[i] * M[i])).reshape(K[i], M[i]) for i in range(total)]
+    Bs = [T.normal(21, 3 * i + 1, int(N[i] * K[i])).reshape(N[i], K[i]) for i in range(total)]
+    Cs = [T.normal(21, 3 * i + 2, int(N[i] * M[i])).reshape(N[i], M[i]) for i in range(total)]
+    gA, gB, gC = VarBatch(As, cuda), VarBatch(Bs, cuda), VarBatch(Cs, cuda)
+    dm, dn, dk = gC.ints(M), gC.ints(N), gC.ints(K)
+    vp = lambda t: C.c_void_p(t.data_ptr())
+    fn = getattr(q.lib, f"magmablas_dgemm_vbatched_{variant}")
+    fn(111, 111, vp(dm), vp(dn), vp(dk), 1.0, vp(gA.ptrs), vp(dm), vp(gB.ptrs), vp(dk), 0.5, vp(gC.ptrs), vp(dm),
+       live, 16, 24, 40, q.handle)
+    q.sync()
+    out = gC.unpack()
+    for i in range(total):
+        if i < live:
+            ref = As[i].T @ Bs[i].T + 0.5 * Cs[i].T
+            assert err(out[i].T, ref, As[i], Bs[i], Cs[i], K[i], 1.0, 0.5) < 30 * np.finfo(np.float64).eps, i
+        else:
+            assert np.array_equal(out[i], Cs[i]), i

@@ -21,8 +21,9 @@ def _rank_main(rank, world, port, out):
     try:
         import bench
 
-        # rank r's own timings: step ms, e2e ms, the second arm's ms
-        got = bench.max_over_ranks([1.0 + rank, 10.0 - rank, 0.0], dist)
+        # rank r's own timings: step ms, e2e ms, the second arm's ms, and its accuracy-bar
+        # miss flag (rank 1 missed): every rank must learn of a miss on any rank
+        got = bench.max_over_ranks([1.0 + rank, 10.0 - rank, 0.0, float(rank == 1)], dist)
         dist.barrier()
         out.put((rank, got))
     finally:
@@ -42,7 +43,7 @@ def test_max_over_ranks_world2_gloo():
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    assert results == {0: [2.0, 10.0, 0.0], 1: [2.0, 10.0, 0.0]}
+    assert results == {0: [2.0, 10.0, 0.0, 1.0], 1: [2.0, 10.0, 0.0, 1.0]}
 
 
 def test_max_over_ranks_single_rank():
@@ -67,3 +68,22 @@ def test_dist_setup_reference_arm_needs_no_process_group(monkeypatch):
     monkeypatch.setenv("LOCAL_RANK", "1")
     rank, world, local, dist = bench.dist_setup(types.SimpleNamespace(impl="reference"))
     assert (rank, world, local, dist) == (1, 2, 1, None)
+
+
+def test_accuracy_gate():
+    """The metric's bar: every instance at backward error <= 1e-14 with info 0; a NaN
+    backward error is a miss."""
+    import torch
+
+    import bench
+
+    be = torch.tensor([1e-16, 9.9e-15, 2e-15], dtype=torch.float64)
+    info = torch.zeros(3, dtype=torch.int32)
+    g, ok = bench.accuracy_gate("x", be, info)
+    assert ok and g == {"x_bwd_err_max": 9.9e-15, "x_over_bar": 0, "x_info_nonzero": 0}
+    _, ok = bench.accuracy_gate("x", torch.tensor([1e-16, 1.1e-14], dtype=torch.float64), info[:2])
+    assert not ok
+    _, ok = bench.accuracy_gate("x", torch.tensor([1e-16, float("nan")], dtype=torch.float64), info[:2])
+    assert not ok
+    _, ok = bench.accuracy_gate("x", be, torch.tensor([0, 3, 0], dtype=torch.int32))
+    assert not ok

@@ -55,6 +55,27 @@ def test_noalloc_matches_allocating_entry_twice(cuda):
             assert np.array_equal(np.tril(got[i].T), np.tril(ref[i].T)), (call, i, n)
 
 
+def test_noalloc_leaves_device_memory_unchanged(cuda):
+    """After one warm call (which loads the kernels), a call changes the device's free
+    memory by nothing: it allocates no device memory of its own."""
+    import torch
+
+    from magma_b200.api import VarBatch, _vp, default_queue
+    q = default_queue()
+    ns, mats = _batch(800, 400, 43)
+    A = VarBatch(mats, cuda)
+    dn = A.ints(ns)
+    info = torch.zeros(len(ns) + 1, dtype=torch.int32, device=cuda)
+    call = lambda: q.lib.magma_dpotrf_vbatched_max_nocheck_noalloc(122, _vp(dn), _vp(A.ptrs), _vp(dn), _vp(info),
+                                                                   len(ns), int(ns.max()), q.handle)
+    assert call() == 0
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(cuda)[0]
+    assert call() == 0
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info(cuda)[0] == free0
+
+
 def test_noalloc_rejects_oversized_batch(cuda, capfd):
     import torch
 
