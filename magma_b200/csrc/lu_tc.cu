@@ -35,6 +35,77 @@ namespace mb200 {
 constexpr int kTcNT = 256;        // threads = matrix rows (n <= 256)
 constexpr int kTcTrail = 224;     // trailing columns of the first panel at n = 256
 
+// Panel factorisation of the FP32 LU (8 warps, thread t = row t, 32 columns in
+// registers). The pivot choice need not match LAPACK's bit for bit here (the FP64
+// refinement and its fallback own the accuracy), which allows a cheaper step than
+// the FP64 kernels' exact one:
+//  * packed keys: |a(i,k)|'s bit pattern without its low 8 mantissa bits, plus one,
+//    shifted back up, with 255 - row in the low byte, so one unsigned max reduction
+//    picks the largest magnitude (to 15 mantissa bits: a pivot within a factor
+//    1 + 2^-15 of the column maximum) and names its row; no ballot or position
+//    reduction follows, and every candidate's key is above a non-candidate's 0;
+//  * one barrier per step: before it, each warp's best row publishes its key,
+//    position, approximate reciprocal and columns into its warp's slot (slots
+//    double-buffered by step parity); after it, every warp reduces the 8 slot keys
+//    and reads the winner's row;
+//  * the multiplier is a(i,k) * (1/pivot) with the reciprocal to ~2 ulp.
+struct TcPanelShared {
+    alignas(16) float cand[2][kTcNT / 32][32];
+    float cinv[2][kTcNT / 32];
+    int cpos[2][kTcNT / 32];
+    unsigned ckey[2][kTcNT / 32];
+};
+
+__device__ __forceinline__ void tc_panel_steps(float (&a)[32], int n, int k0, int t, int& pos, int& my_ipiv,
+                                               int& info, TcPanelShared& sh) {
+    const int lane = t & 31, w = t >> 5;
+    static_for<0, 32>([&](auto kc) {
+        constexpr int k = decltype(kc)::value;
+        constexpr int buf = k & 1;
+        constexpr int jw = k & ~3;
+        const int g = k0 + k;
+        const bool cand = (pos >= g) && (t < n);
+        // candidates: ((|x| bits >> 8) + 1) << 8 | (255 - row) >= 0x100 > 0 = not a candidate
+        const unsigned key = cand ? ((((__float_as_uint(fabsf(a[k])) >> 8) + 1u) << 8) | (255u - unsigned(t))) : 0u;
+        const unsigned wmax = __reduce_max_sync(kFullMask, key);
+        if (lane == 0) sh.ckey[buf][w] = wmax;
+        if (wmax != 0u && key == wmax) {   // this warp's best row (unique: the key names it)
+            sh.cpos[buf][w] = pos;
+            sh.cinv[buf][w] = __fdividef(1.0f, a[k]);
+            float4* dst = reinterpret_cast<float4*>(&sh.cand[buf][w][0]);
+#pragma unroll
+            for (int j = jw; j < 32; j += 4) dst[j / 4] = make_float4(a[j], a[j + 1], a[j + 2], a[j + 3]);
+        }
+        __syncthreads();
+        const unsigned gmax = __reduce_max_sync(kFullMask, lane < kTcNT / 32 ? sh.ckey[buf][lane] : 0u);
+        const int s = 255 - int(gmax & 0xFFu);   // the pivot row's thread
+        const int ws = (s >> 5) & (kTcNT / 32 - 1);
+        const float* prow = &sh.cand[buf][ws][0];
+        const float piv = prow[k];
+        const int p = sh.cpos[buf][ws];
+        if (t == g) my_ipiv = (piv != 0.0f) ? p + 1 : g + 1;   // a zero pivot interchanges nothing
+        if (piv != 0.0f) {
+            if (pos == g) pos = p;   // the row at position g takes the pivot's old position
+            if (t == s) pos = g;
+        } else if (info == 0) {
+            info = g + 1;
+        }
+        if (pos > g && t < n) {
+            if (piv != 0.0f) a[k] = a[k] * sh.cinv[buf][ws];
+            const float l = a[k];
+            const float4* r4 = reinterpret_cast<const float4*>(prow);
+#pragma unroll
+            for (int j = jw; j < 32; j += 4) {
+                const float4 u = r4[j / 4];
+                if (j > k) a[j] = fmaf(l, -u.x, a[j]);
+                if (j + 1 > k) a[j + 1] = fmaf(l, -u.y, a[j + 1]);
+                if (j + 2 > k) a[j + 2] = fmaf(l, -u.z, a[j + 2]);
+                if (j + 3 > k) a[j + 3] = fmaf(l, -u.w, a[j + 3]);
+            }
+        }
+    });
+}
+
 struct TcLuSmem {
     // The L21 operand is built after the pivot rows' entries (Ug) have been solved and
     // copied into the B operand, and the MMA that reads it completes before the next
@@ -45,7 +116,7 @@ struct TcLuSmem {
     };
     float B[2][kTcTrail * 32];      // U12 operand: [hi, lo], K-major canonical (28 KB each)
     float L11[32][33];
-    SmallLuShared<float, 32, 8> lu;
+    TcPanelShared pan;
     double red[kTcNT / 32];
     unsigned long long mbar;
     uint32_t tmem_base;
@@ -147,7 +218,7 @@ lu_tf32x3_kernel(TcLuArgs g) {
             tc::tmem_ld32(trow + k0, a);
             tc::wait_ld();
             int my_ipiv = 0;
-            lu_panel_steps<float, 32, kTcNT / 32>(a, n, 32, 32, k0, t, pos, my_ipiv, info, sh.lu);
+            tc_panel_steps(a, n, k0, t, pos, my_ipiv, info, sh.pan);
             if (t >= k0 && t < k0 + 32) g.ipiv[id][t] = my_ipiv;
             const bool piv = (t < n) && pos >= k0 && pos < k0 + 32;
             const int ncols = n - k0 - 32;
