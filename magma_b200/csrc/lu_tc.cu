@@ -214,6 +214,10 @@ lu_tf32x3_kernel(TcLuArgs g) {
         int pos = (t < n) ? t : INT_MAX / 2;
         int info = 0;
         for (int k0 = 0; k0 < n && !failed; k0 += 32) {
+            // the next instance's FP64 columns into L2 while this one finishes (thread t:
+            // column t), so its conversion reads from L2 instead of HBM
+            if (k0 == (n >= 64 ? n - 64 : 0) && id + (int)gridDim.x < g.batch && t < n)
+                prefetch_l2(g.dA[id + gridDim.x] + (size_t)t * g.lda, unsigned(n) * 8u);
             float a[32];
             tc::tmem_ld32(trow + k0, a);
             tc::wait_ld();
@@ -227,18 +231,10 @@ lu_tf32x3_kernel(TcLuArgs g) {
 #pragma unroll
                 for (int c = 0; c < 32; ++c) sh.L11[pos - k0][c] = a[c];
             }
-            // a pivot row is final: columns left of the panel from TMEM, the panel from
-            // registers; its trailing entries go to shared memory for the U12 solve
+            // a pivot row is final: the panel from registers now, its trailing entries to
+            // shared memory for the U12 solve, and its columns left of the panel (which
+            // stay untouched in TMEM) once the whole factorisation is done
             if (__any_sync(kFullMask, piv)) {
-                for (int c0 = 0; c0 < k0; c0 += 32) {
-                    float v[32];
-                    tc::tmem_ld32(trow + c0, v);
-                    tc::wait_ld();
-                    if (piv) {
-#pragma unroll
-                        for (int c = 0; c < 32; ++c) S[pos + (size_t)(c0 + c) * n] = v[c];
-                    }
-                }
                 for (int c0 = k0 + 32; c0 < n; c0 += 32) {
                     float v[32];
                     tc::tmem_ld32(trow + c0, v);
@@ -320,6 +316,20 @@ lu_tf32x3_kernel(TcLuArgs g) {
                 if (t == 0) atomicExch(g.err, 1);
             }
             tc::fence_after_sync();
+        }
+        if (!failed) {
+            // every row's L entries left of the panel that chose it, at its final position
+            const int myk = (t < n) ? (pos & ~31) : 0;
+            const int wk = (int)__reduce_max_sync(kFullMask, (unsigned)myk);
+            for (int c0 = 0; c0 < wk; c0 += 32) {
+                float v[32];
+                tc::tmem_ld32(trow + c0, v);
+                tc::wait_ld();
+                if (c0 < myk) {
+#pragma unroll
+                    for (int c = 0; c < 32; ++c) S[pos + (size_t)(c0 + c) * n] = v[c];
+                }
+            }
         }
         if (t == 0) g.sinfo[id] = info;
         if (failed && t == 0) {
