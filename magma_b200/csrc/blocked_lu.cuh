@@ -16,26 +16,38 @@
 //     3. for the trailing columns, in chunks of CW: the NB pivot rows are
 //        gathered into shared memory and solved with L11 (U12 = L11^-1 A12,
 //        one thread per column, in registers), then every other live row applies
-//        A22 -= L21 U12 from its registers while moving to its new position,
-//        and the U12 rows are stored.
+//        A22 -= L21 U12 while moving to its new position -- in FP64 on the tensor
+//        cores (mma.sync m8n8k4 .f64: each warp's 32 rows as four 8-row groups,
+//        8-column tiles, the multipliers as A fragments read back from the stored
+//        panel), in FP32 from registers -- and the U12 rows are stored.
 //   After each panel the matrix is again in LAPACK's row order, so the next
 //   panel starts with thread t = position t.
 //
 // Every element receives its updates as single fma's in increasing step
 // order, exactly like the unblocked dgetf2 (DGER per step), so factors,
 // pivots and info are bit-identical to the oracle restatement at every size.
+// This holds on the tensor cores too: an m8n8k4 FP64 MMA gives each element the
+// four products as a chain of fma's in ascending k, each rounded (measured on
+// B200 against the fma chain: 1.28 M of 1.28 M elements equal), and the k-steps
+// are issued in ascending order.
 #pragma once
 
 #include "small_lu.cuh"
+#include <type_traits>
 
 namespace mb200 {
 
-template <typename T, int NB, int NT, int CW>
+template <typename T, int NB, int NT, int CW, bool DMMA = false>
 struct BlockedLuShared {
     SmallLuShared<T, NB, NT / 32> lu;
     T   L11[NB][NB + 1];
-    T   U[NB][CW];
+    // pivot rows' trailing columns, then U12; rows padded to CW + 1 so that a warp
+    // reading one column across 32 rows (gather, U12 store) hits every bank pair twice
+    T   U[NB][CW + 1];
     int src[NB];
+    // DMMA update: the panel's multipliers as tensor-core A fragments,
+    // [warp][row group][k-step][lane] (each lane reads its own 8 bytes)
+    T   af[DMMA ? NT / 32 : 1][4][DMMA ? NB / 4 : 1][32];
 };
 
 // U12 = L11^-1 A12 for column c of the staged pivot rows (sh.U[0..NB-1][c]),
@@ -44,8 +56,8 @@ struct BlockedLuShared {
 // in registers. Every entry receives fma(L11(r, rr), -U(rr, c), x) for rr
 // ascending -- the unblocked order. Rows past the panel's last step hold
 // unused values and are never stored.
-template <typename T, int NB, int NT, int CW>
-__device__ __forceinline__ void blocked_trsm_column(BlockedLuShared<T, NB, NT, CW>& sh, int c) {
+template <typename T, int NB, int NT, int CW, bool DMMA>
+__device__ __forceinline__ void blocked_trsm_column(BlockedLuShared<T, NB, NT, CW, DMMA>& sh, int c) {
     constexpr int H = 8;
     static_assert(NB % H == 0, "panel width must be a multiple of the TRSM group");
 #pragma unroll 1
@@ -69,9 +81,83 @@ __device__ __forceinline__ void blocked_trsm_column(BlockedLuShared<T, NB, NT, C
     }
 }
 
-template <typename T, int NB, int NT, int CW, int CB>
+// One FP64 tensor-core step D = A B + D on an 8x8 tile (A 8x4 row-major, B 4x8
+// column-major; lane l holds A(l/4, l%4), B(l%4, l/4), D(l/4, 2(l%4) .. +1)). Each
+// element of D receives fma(a(i,0), b(0,j), d) then k = 1, 2, 3 in ascending order,
+// rounded after every step -- the same operations as four single fma's in k order,
+// which keeps the blocked update bit-identical to the unblocked elimination.
+__device__ __forceinline__ void dmma_884(double& d0, double& d1, double a, double b) {
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+        : "+d"(d0), "+d"(d1)
+        : "d"(a), "d"(b));
+}
+
+// A22 -= L21 U12 for the warp's 32 rows and the chunk's cw columns on the FP64
+// tensor cores. The A fragment of row group g (rows 8g..8g+7 of the warp) and k-step
+// s (panel columns 4s..4s+3) is the row's multiplier, read from the panel stored at
+// the row's new position rpos[g]; 0 for rows that take no update and for columns
+// past the panel's steps. Row 8g + l/4 of the warp
+// reads its C entries at its current position and writes them to rpos[g] (rupd[g]
+// false: not read, not written). B = -U12 from shared memory, 0 past the chunk. The
+// C entries of the next 8-column tile are loaded while the current tile computes.
+template <int NB, int NT, int CW>
+__device__ __forceinline__ void blocked_update_dmma(double* A, int lda, int k0, int j0, int cw, int nbp,
+                                                    const int (&rpos)[4], const bool (&rupd)[4],
+                                                    const double (&U)[NB][CW + 1], const double (&af)[4][NB / 4][32]) {
+    constexpr int KS = NB / 4;
+    const int lane = threadIdx.x & 31;
+    const int row0 = (threadIdx.x & ~31) + (lane >> 2);   // warp's first row + this lane's row in a group
+    const int q = lane & 3;
+    const int ks = (nbp + 3) / 4;                         // k-steps with a panel column
+    bool gact[4];                                         // groups with a row to update
+#pragma unroll
+    for (int g = 0; g < 4; ++g) gact[g] = __any_sync(kFullMask, rupd[g]);
+    if (!(gact[0] || gact[1] || gact[2] || gact[3])) return;   // every row of the warp is done
+    double cn[4][2];
+    auto load_c = [&](int jt) {
+        const int c0 = jt + 2 * q;
+        const double* src0 = A + (size_t)(j0 + c0) * lda;
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+            const int r = row0 + 8 * g;                   // the row's position before this panel
+            cn[g][0] = (c0 < cw && rupd[g]) ? src0[r] : 0.0;
+            cn[g][1] = (c0 + 1 < cw && rupd[g]) ? src0[r + lda] : 0.0;
+        }
+    };
+    load_c(0);
+#pragma unroll 1
+    for (int jt = 0; jt < cw; jt += 8) {
+        double cc[4][2];
+#pragma unroll
+        for (int g = 0; g < 4; ++g) { cc[g][0] = cn[g][0]; cc[g][1] = cn[g][1]; }
+        if (jt + 8 < cw) load_c(jt + 8);
+        double b[KS];
+        const int cb = jt + (lane >> 2);                  // B column of this lane
+#pragma unroll
+        for (int s = 0; s < KS; ++s) b[s] = (cb < cw && 4 * s + q < nbp) ? -U[4 * s + q][cb] : 0.0;
+#pragma unroll
+        for (int s = 0; s < KS; ++s) {
+            if (s < ks) {
+#pragma unroll
+                for (int g = 0; g < 4; ++g)
+                    if (gact[g]) dmma_884(cc[g][0], cc[g][1], af[g][s][lane], b[s]);
+            }
+        }
+        const int c0 = jt + 2 * q;
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+            if (rupd[g]) {
+                double* dst = A + (size_t)(j0 + c0) * lda + rpos[g];
+                if (c0 < cw) dst[0] = cc[g][0];
+                if (c0 + 1 < cw) dst[lda] = cc[g][1];
+            }
+        }
+    }
+}
+
+template <typename T, int NB, int NT, int CW, int CB, bool DMMA>
 __device__ void blocked_getrf(T* __restrict__ A, int m, int n, int lda, int* __restrict__ ipiv, int& info,
-                              BlockedLuShared<T, NB, NT, CW>& sh) {
+                              BlockedLuShared<T, NB, NT, CW, DMMA>& sh) {
     constexpr int NW = NT / 32;
     const int tid = threadIdx.x;
     const int kmax = min(m, n);
@@ -123,8 +209,34 @@ __device__ void blocked_getrf(T* __restrict__ A, int m, int n, int lda, int* __r
         // next CB of them are loaded one group ahead (across the barriers) to hide
         // the load latency behind the current group's arithmetic.
         const bool upd = live && !pivot_row;
+        constexpr bool kDmma = DMMA && std::is_same<T, double>::value;
+        // FP64: the update runs on the tensor cores; the A fragments (the rows'
+        // multipliers) of the warp's four row groups go to shared memory once per
+        // panel, gathered by shuffles.
+        int rpos[4];
+        bool rupd[4];
+        if constexpr (kDmma) {
+            const int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+            for (int g = 0; g < 4; ++g) {
+                const int srcl = 8 * g + (lane >> 2);
+                rpos[g] = __shfl_sync(kFullMask, pos, srcl);
+                rupd[g] = __shfl_sync(kFullMask, (int)upd, srcl) != 0;
+#pragma unroll
+                for (int s = 0; s < NB / 4; ++s) {
+                    double v = 0.0;
+#pragma unroll
+                    for (int qq = 0; qq < 4; ++qq) {
+                        const double x = __shfl_sync(kFullMask, (double)a[4 * s + qq], srcl);
+                        if ((lane & 3) == qq) v = x;
+                    }
+                    sh.af[warp][g][s][lane] = (rupd[g] && 4 * s + (lane & 3) < nbp) ? v : 0.0;
+                }
+            }
+        }
         T nxt[CB];
         auto prefetch = [&](int j) {
+            if constexpr (kDmma) return;
 #pragma unroll
             for (int c = 0; c < CB; ++c) nxt[c] = (upd && j + c < n) ? A[tid + (size_t)(j + c) * lda] : T(0);
         };
@@ -139,12 +251,16 @@ __device__ void blocked_getrf(T* __restrict__ A, int m, int n, int lda, int* __r
             __syncthreads();
             // U12 = L11^-1 A12, one thread per column, in two halves of H rows held in
             // registers; each entry gets its fma's in ascending step order.
-            for (int c = tid; c < cw; c += NT) blocked_trsm_column<T, NB, NT, CW>(sh, c);
+            for (int c = tid; c < cw; c += NT) blocked_trsm_column<T, NB, NT, CW, DMMA>(sh, c);
             __syncthreads();
             // A22 -= L21 U12 for the non-pivot live rows, stored at their new positions.
             // A row only ever overwrites the old row of a pivot (already gathered above),
             // so no barrier is needed between these loads and stores.
-            if (upd) {
+            if constexpr (kDmma) {
+                blocked_update_dmma<NB, NT, CW>(reinterpret_cast<double*>(A), lda, k0, j0, cw, nbp, rpos, rupd,
+                                                reinterpret_cast<const double(&)[NB][CW + 1]>(sh.U),
+                                                reinterpret_cast<const double(&)[4][NB / 4][32]>(sh.af[tid >> 5]));
+            } else if (upd) {
                 for (int c0 = 0; c0 < cw; c0 += CB) {
                     T acc[CB];
 #pragma unroll

@@ -1,8 +1,9 @@
 // tuning.cu -- kernel-variant table and its autotuner.
 //
-// The dispatchers of the variable-size GEMM (tile shape per size bucket) and of
-// the mixed-precision solve (tensor-core or CUDA-core FP32 LU) read one
-// process-wide table. Defaults are built in; MAGMA_B200_TUNING=<file> loads a
+// The dispatchers of the variable-size GEMM (tile shape per size bucket), of
+// the mixed-precision solve (tensor-core or CUDA-core FP32 LU) and of the FP64
+// blocked LU (trailing update on the tensor cores or the FP64 pipe, per size
+// bucket) read one process-wide table. Defaults are built in; MAGMA_B200_TUNING=<file> loads a
 // saved table at first use; magma_b200_autotune() measures every variant on the
 // queue's device with synthetic problems of each bucket and keeps the fastest.
 // Every variant of a family computes bit-identical results (same fma order per
@@ -10,6 +11,7 @@
 #include "internal.h"
 #include "tuning.h"
 #include "../../include/magma_b200.h"
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -29,6 +31,10 @@ static void set_defaults(TuningTable& t) {
         for (int b = 0; b < kGemmBuckets; ++b) t.gemm_variant[p][b] = gemm[p][b];
     const char* e = std::getenv("MAGMA_B200_TENSOR_CORE_LU");
     t.mixed_tc_lu = (e && e[0] == '0') ? 0 : 1;
+    // measured on a B200 (uniform[-1,1] batches of 1 GB): the FMA update is faster up to
+    // m = 512 (n = 256: 4.58 against 4.74 ms), DMMA at m = 1,024 (23.4 against 23.9 ms)
+    const int dmma[kLuBlockedBuckets] = {0, 0, 0, 1};
+    for (int b = 0; b < kLuBlockedBuckets; ++b) t.lu_dmma[b] = dmma[b];
 }
 
 static void to_values(const TuningTable& t, int* v) {
@@ -36,17 +42,23 @@ static void to_values(const TuningTable& t, int* v) {
     for (int p = 0; p < 2; ++p)
         for (int b = 0; b < kGemmBuckets; ++b) v[i++] = t.gemm_variant[p][b];
     v[i++] = t.mixed_tc_lu;
+    for (int b = 0; b < kLuBlockedBuckets; ++b) v[i++] = t.lu_dmma[b];
 }
 
+// count kTuningValues, or kTuningValuesV1 (a table saved before the LU entries
+// existed: those keep their current values).
 static bool from_values(const int* v, int count, TuningTable& t) {
-    if (count != kTuningValues) return false;
+    if (count != kTuningValues && count != kTuningValuesV1) return false;
     for (int i = 0; i < 2 * kGemmBuckets; ++i)
         if (v[i] < 0 || v[i] > 2) return false;
-    if (v[2 * kGemmBuckets] != 0 && v[2 * kGemmBuckets] != 1) return false;
+    for (int i = 2 * kGemmBuckets; i < count; ++i)
+        if (v[i] != 0 && v[i] != 1) return false;
     int i = 0;
     for (int p = 0; p < 2; ++p)
         for (int b = 0; b < kGemmBuckets; ++b) t.gemm_variant[p][b] = v[i++];
-    t.mixed_tc_lu = v[i];
+    t.mixed_tc_lu = v[i++];
+    if (count == kTuningValues)
+        for (int b = 0; b < kLuBlockedBuckets; ++b) t.lu_dmma[b] = v[i++];
     return true;
 }
 
@@ -55,10 +67,13 @@ static bool load_file(const char* path, TuningTable& t) {
     if (!f) return false;
     char magic[64] = {0};
     int v[kTuningValues];
-    bool ok = std::fscanf(f, "%63s", magic) == 1 && std::strcmp(magic, "magma_b200_tuning_v1") == 0;
-    for (int i = 0; ok && i < kTuningValues; ++i) ok = std::fscanf(f, "%d", &v[i]) == 1;
+    bool ok = std::fscanf(f, "%63s", magic) == 1;
+    const int count = !ok ? 0 : std::strcmp(magic, "magma_b200_tuning_v2") == 0 ? kTuningValues
+                             : std::strcmp(magic, "magma_b200_tuning_v1") == 0 ? kTuningValuesV1 : 0;
+    ok = ok && count > 0;
+    for (int i = 0; ok && i < count; ++i) ok = std::fscanf(f, "%d", &v[i]) == 1;
     std::fclose(f);
-    return ok && from_values(v, kTuningValues, t);
+    return ok && from_values(v, count, t);
 }
 
 static void init_once() {
@@ -235,6 +250,45 @@ static magma_int_t tune_mixed(magma_queue_t q, unsigned seed) {
     return MAGMA_SUCCESS;
 }
 
+// FP64 blocked LU: for each bucket, the two trailing-update variants on a batch of
+// about 256 MB of uniform[-1,1] matrices of the bucket's largest order, through
+// magma_dgetrf_batched (both variants give bit-identical factors).
+static magma_int_t tune_lu_update(magma_queue_t q, unsigned seed) {
+    const int orders[kLuBlockedBuckets] = {128, 256, 512, 1024};
+    for (int b = 0; b < kLuBlockedBuckets; ++b) {
+        const int n = orders[b];
+        const int batch = std::max(16, (256 << 20) / (8 * n * n));
+        const size_t an = (size_t)n * n * batch;
+        DevBuf dA, dA0, dP, dI;
+        if (!dA.alloc(8 * an) || !dA0.alloc(8 * an) || !dP.alloc(sizeof(void*) * 2 * batch) ||
+            !dI.alloc(sizeof(int) * ((size_t)n * batch + batch)))
+            return MAGMA_ERR_DEVICE_ALLOC;
+        tune_fill_kernel<double><<<1024, 256, 0, q->stream>>>((double*)dA0.p, an, seed + b);
+        std::vector<void*> ptr(2 * batch);
+        for (int i = 0; i < batch; ++i) {
+            ptr[i] = (double*)dA.p + (size_t)i * n * n;
+            ptr[batch + i] = (int*)dI.p + (size_t)i * n;
+        }
+        cudaMemcpyAsync(dP.p, ptr.data(), sizeof(void*) * 2 * batch, cudaMemcpyHostToDevice, q->stream);
+        cudaStreamSynchronize(q->stream);
+        void** p = (void**)dP.p;
+        int* info = (int*)dI.p + (size_t)n * batch;
+        float best = 1e30f;
+        int best_v = tuning().lu_dmma[b];
+        for (int v = 0; v < 2; ++v) {
+            tuning_mut().lu_dmma[b] = v;
+            const float ms = time_ms(q->stream, [&] {
+                cudaMemcpyAsync(dA.p, dA0.p, 8 * an, cudaMemcpyDeviceToDevice, q->stream);
+                magma_dgetrf_batched(n, n, (double**)p, n, (int**)(p + batch), info, batch, q);
+            }, 3);
+            if (cudaGetLastError() != cudaSuccess) return MAGMA_ERR_UNKNOWN;
+            if (ms < best) { best = ms; best_v = v; }
+        }
+        tuning_mut().lu_dmma[b] = best_v;
+    }
+    return MAGMA_SUCCESS;
+}
+
 }  // namespace mb200
 
 using namespace mb200;
@@ -247,6 +301,7 @@ magma_int_t magma_b200_autotune(magma_queue_t queue) {
     magma_int_t rc = tune_gemm<double>(0, queue, 17);
     if (!rc) rc = tune_gemm<float>(1, queue, 23);
     if (!rc) rc = tune_mixed(queue, 29);
+    if (!rc) rc = tune_lu_update(queue, 31);
     cudaStreamSynchronize(queue->stream);
     return rc;
 }
@@ -270,7 +325,7 @@ magma_int_t magma_b200_tuning_save(const char* path) {
     if (!f) return MAGMA_ERR_UNKNOWN;
     int v[kTuningValues];
     to_values(tuning(), v);
-    std::fprintf(f, "magma_b200_tuning_v1\n");
+    std::fprintf(f, "magma_b200_tuning_v2\n");
     for (int i = 0; i < kTuningValues; ++i) std::fprintf(f, "%d%c", v[i], i + 1 < kTuningValues ? ' ' : '\n');
     return std::fclose(f) == 0 ? MAGMA_SUCCESS : MAGMA_ERR_UNKNOWN;
 }

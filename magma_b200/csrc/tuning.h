@@ -9,13 +9,17 @@ namespace mb200 {
 
 constexpr int kGemmBuckets = 4;   // max(M, N) <= 16, <= 32, <= 64, larger
 
+constexpr int kLuBlockedBuckets = 4;   // blocked LU by max(m): <= 128, <= 256, <= 512, <= 1024
+
 struct TuningTable {
     int gemm_variant[2][kGemmBuckets];   // [FP64, FP32][bucket]: tile variant (0: 64x64, 1: 32x32, 2: 16x16)
     int mixed_tc_lu;                     // 1: tensor-core LU in the mixed solve for n = 96..256, step 32
+    int lu_dmma[kLuBlockedBuckets];      // 1: FP64 blocked LU trailing update on the tensor cores (DMMA)
 };
 
 const TuningTable& tuning();   // defaults, or the file named by MAGMA_B200_TUNING, or the last autotune/set
 TuningTable& tuning_mut();
-constexpr int kTuningValues = 2 * kGemmBuckets + 1;
+constexpr int kTuningValuesV1 = 2 * kGemmBuckets + 1;
+constexpr int kTuningValues = kTuningValuesV1 + kLuBlockedBuckets;
 
 }  // namespace mb200

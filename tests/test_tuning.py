@@ -10,7 +10,7 @@ import pytest
 
 from magma_b200 import _lib
 
-N_VALUES = 9
+N_VALUES = 13
 
 
 def _get(lib):
@@ -29,17 +29,23 @@ def test_tuning_roundtrip(tmp_path):
     assert lib.magma_b200_tuning_get(None, 0) == N_VALUES           # size query
     orig = _get(lib)
     try:
-        new = [0, 1, 2, 0, 2, 1, 0, 0, 0]
+        new = [0, 1, 2, 0, 2, 1, 0, 0, 0, 1, 0, 1, 1]
         assert _set(lib, new) == 0 and _get(lib) == new
         f = tmp_path / "tune.txt"
         assert lib.magma_b200_tuning_save(str(f).encode()) == 0
-        assert f.read_text().split()[0] == "magma_b200_tuning_v1"
+        assert f.read_text().split()[0] == "magma_b200_tuning_v2"
         assert _set(lib, orig) == 0 and _get(lib) == orig
         assert lib.magma_b200_tuning_load(str(f).encode()) == 0 and _get(lib) == new
         # rejected: wrong count, out-of-range values, unreadable or malformed files
         assert _set(lib, new[:-1]) == _lib.MAGMA_ERR_ILLEGAL_VALUE
         assert _set(lib, [3] + new[1:]) == _lib.MAGMA_ERR_ILLEGAL_VALUE
         assert _set(lib, new[:-1] + [2]) == _lib.MAGMA_ERR_ILLEGAL_VALUE
+        # a 9-value table (saved before the LU update entries) sets the first 9 only
+        assert _set(lib, orig[:9]) == 0 and _get(lib) == orig[:9] + new[9:]
+        v1 = tmp_path / "v1.txt"
+        v1.write_text("magma_b200_tuning_v1\n" + " ".join(map(str, new[:9])) + "\n")
+        assert lib.magma_b200_tuning_load(str(v1).encode()) == 0 and _get(lib) == new
+        assert _set(lib, new) == 0
         assert lib.magma_b200_tuning_load(str(tmp_path / "missing").encode()) == _lib.MAGMA_ERR_ILLEGAL_VALUE
         bad = tmp_path / "bad.txt"
         bad.write_text("magma_b200_tuning_v1\n0 1 2\n")
@@ -97,8 +103,41 @@ def test_autotune_runs(cuda, tmp_path):
         q = default_queue()
         assert lib.magma_b200_autotune(q.handle) == 0
         vals = _get(lib)
-        assert all(0 <= v <= 2 for v in vals[:8]) and vals[8] in (0, 1)
+        assert all(0 <= v <= 2 for v in vals[:8]) and all(v in (0, 1) for v in vals[8:])
         f = tmp_path / "tuned.txt"
         assert lib.magma_b200_tuning_save(str(f).encode()) == 0
     finally:
         _set(lib, orig)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [100, 256, 300, 700])
+def test_lu_update_variants_bit_identical(cuda, n):
+    """The FP64 blocked LU's trailing update on the tensor cores (DMMA) and on the FP64
+    pipe give the same factors, pivots and info bit for bit, and both equal the oracle."""
+    import torch
+
+    import magma_b200 as mb
+    import oracle
+    from magma_b200 import testing as T
+    lib = _lib.load()
+    orig = _get(lib)
+    batch = max(2, 3_000_000 // (n * n))
+    A_np, _ = T.lu_uniform(batch, n, 1, seed=n)
+    A_np[0, 7, :] = 0.0                      # a singular instance (zero column 8)
+    res = {}
+    try:
+        for v in (0, 1):
+            assert _set(lib, orig[:9] + [v] * 4) == 0
+            A = torch.from_numpy(A_np).to(cuda)
+            ipiv, info = mb.dgetrf_batched(A)
+            torch.cuda.synchronize()
+            res[v] = (A.cpu().numpy(), ipiv.cpu().numpy(), info.cpu().numpy())
+    finally:
+        _set(lib, orig)
+    for a, b in zip(res[0], res[1]):
+        assert np.array_equal(a, b)
+    O = A_np[:3].copy()
+    oip, oinf = oracle.dgetrf_batched(O, n)
+    assert np.array_equal(res[1][0][:3], O) and np.array_equal(res[1][1][:3], oip)
+    assert np.array_equal(res[1][2][:3], oinf) and oinf[0] == 8
