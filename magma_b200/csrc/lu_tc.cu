@@ -27,6 +27,7 @@
 #include "tc_ptx.cuh"
 #include "lu_tc.h"
 #include <cfloat>
+#include <cstddef>
 #include <atomic>
 #include <climits>
 
@@ -115,7 +116,9 @@ struct TcLuSmem {
         float Ug[32][kTcTrail + 1]; // pivot rows' trailing entries; U12 after the solve
     };
     float B[2][kTcTrail * 32];      // U12 operand: [hi, lo], K-major canonical (28 KB each)
-    float L11[32][33];
+    // each panel's 32x32 diagonal block by position: L11 below the diagonal, U11 on
+    // and above it (the trsm reads the current one; the refinement inverts them all)
+    float dblk[kTcNT / 32][32][33];
     TcPanelShared pan;
     double red[kTcNT / 32];
     unsigned long long mbar;
@@ -130,7 +133,7 @@ __device__ __forceinline__ int kmajor(int row, int k) {
 constexpr uint32_t kLbo = 128, kSbo = 1024;
 
 // U12 = L11^-1 A12 for column c of sh.Ug (unit lower L11), rows in groups of 8.
-__device__ __forceinline__ void tc_trsm_column(TcLuSmem& sh, int c) {
+__device__ __forceinline__ void tc_trsm_column(TcLuSmem& sh, const float (&L11)[32][33], int c) {
 #pragma unroll 1
     for (int q0 = 0; q0 < 32; q0 += 8) {
         float x[8];
@@ -139,16 +142,342 @@ __device__ __forceinline__ void tc_trsm_column(TcLuSmem& sh, int c) {
         for (int rr = 0; rr < q0; ++rr) {
             const float u = sh.Ug[rr][c];
 #pragma unroll
-            for (int r = 0; r < 8; ++r) x[r] = fmaf(sh.L11[q0 + r][rr], -u, x[r]);
+            for (int r = 0; r < 8; ++r) x[r] = fmaf(L11[q0 + r][rr], -u, x[r]);
         }
         static_for<0, 8>([&](auto rc) {
             constexpr int rr = decltype(rc)::value;
 #pragma unroll
-            for (int r = rr + 1; r < 8; ++r) x[r] = fmaf(sh.L11[q0 + r][q0 + rr], -x[rr], x[r]);
+            for (int r = rr + 1; r < 8; ++r) x[r] = fmaf(L11[q0 + r][q0 + rr], -x[rr], x[r]);
         });
 #pragma unroll
         for (int r = 0; r < 8; ++r) sh.Ug[q0 + r][c] = x[r];
     }
+}
+
+// L2 retention policy and loads that carry it (PTX createpolicy / ld .L2::cache_hint).
+__device__ __forceinline__ uint64_t l2_evict_last_policy() {
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ double ld_keep(const double* p, uint64_t pol) {
+    double v;
+    asm("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ double2 ld_keep2(const double* p, uint64_t pol) {   // p 16-byte aligned
+    double2 v;
+    asm("ld.global.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(p), "l"(pol));
+    return v;
+}
+
+// ---------------------------------------------------------------------------
+// Refinement in the block that factored the instance (magma_dsgesv_gpu's loop,
+// src/zcgesv_gpu.cpp:251-362: ITERMAX 30, BWDMAX 1). The single-precision solves
+// read L from tensor memory (each row's own TMEM lane holds its multipliers), U12
+// from the rows stored in global memory during the factorisation (L2-resident),
+// and the inverses of the 32x32 diagonal blocks formed here from the panels'
+// diagonal blocks; the FP64 residual reads A again (kept in L2 at a high retention
+// priority since the conversion read it). Thread t owns row t of A, B and the residual, and the
+// solution entry of column pos (the position its row took).
+constexpr int kTcR = 4;          // right-hand sides per refinement pass (the residual reads them as a double4)
+constexpr int kTcItermax = 30;
+
+struct TcRefineSmem {            // overlays the operand buffers once the factorisation is done
+    float inv[kTcNT / 32][2][32][33];   // [block][0: L^-1 (unit lower), 1: U^-1][row][col]
+    float f[kTcNT][kTcR];               // single-precision vectors by position
+    alignas(32) double xs[kTcNT][kTcR]; // FP64 solution by column, for the residual
+    double red[2][kTcNT / 32][kTcR];
+    alignas(32) double part[2][kTcNT][kTcR];   // the residual's two column halves, per row
+};
+
+// L^-1 (unit lower part) and U^-1 (upper part) of one diagonal block, one warp:
+// lane j forms column j of each by substitution on e_j.
+__device__ __forceinline__ void tc_invert_block(const float (&blk)[32][33], float (&linv)[32][33],
+                                                float (&uinv)[32][33], int lane) {
+    float x[32];
+    static_for<0, 32>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        float s = (i == lane) ? 1.0f : 0.0f;
+#pragma unroll
+        for (int k = 0; k < i; ++k) s = fmaf(-blk[i][k], x[k], s);
+        x[i] = (i < lane) ? 0.0f : s;
+    });
+#pragma unroll
+    for (int i = 0; i < 32; ++i) linv[i][lane] = x[i];
+    static_for<0, 32>([&](auto ic) {
+        constexpr int i = 31 - decltype(ic)::value;
+        float s = (i == lane) ? 1.0f : 0.0f;
+#pragma unroll
+        for (int k = i + 1; k < 32; ++k) s = fmaf(-blk[i][k], x[k], s);
+        x[i] = (i > lane) ? 0.0f : s / blk[i][i];
+    });
+#pragma unroll
+    for (int i = 0; i < 32; ++i) uinv[i][lane] = x[i];
+}
+
+// c_J = inv * f_J for the 32 positions of block J, by warp J (lane i: row i).
+// Four partial sums per entry keep the dependent fma chains 8 long.
+__device__ __forceinline__ void tc_block_diag(const float (&inv)[32][33], float (&f)[kTcNT][kTcR], int j0, int lane) {
+    float c[4][kTcR];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int r = 0; r < kTcR; ++r) c[q][r] = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 32; ++k) {
+        const float l = inv[lane][k];
+        const float4 fk = *reinterpret_cast<const float4*>(&f[j0 + k][0]);
+        c[k & 3][0] = fmaf(l, fk.x, c[k & 3][0]);
+        c[k & 3][1] = fmaf(l, fk.y, c[k & 3][1]);
+        c[k & 3][2] = fmaf(l, fk.z, c[k & 3][2]);
+        c[k & 3][3] = fmaf(l, fk.w, c[k & 3][3]);
+    }
+    __syncwarp();   // every lane has read f_J before it is overwritten
+#pragma unroll
+    for (int r = 0; r < kTcR; ++r) f[j0 + lane][r] = (c[0][r] + c[1][r]) + (c[2][r] + c[3][r]);
+}
+
+// fo -= sum_k v[k] * f[j0 + k], with four partial sums (chains 8 long).
+__device__ __forceinline__ void tc_block_update(float (&fo)[kTcR], const float (&v)[32],
+                                                const float (&f)[kTcNT][kTcR], int j0) {
+    float d[4][kTcR];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int r = 0; r < kTcR; ++r) d[q][r] = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 32; ++k) {
+        const float4 fk = *reinterpret_cast<const float4*>(&f[j0 + k][0]);
+        d[k & 3][0] = fmaf(v[k], fk.x, d[k & 3][0]);
+        d[k & 3][1] = fmaf(v[k], fk.y, d[k & 3][1]);
+        d[k & 3][2] = fmaf(v[k], fk.z, d[k & 3][2]);
+        d[k & 3][3] = fmaf(v[k], fk.w, d[k & 3][3]);
+    }
+#pragma unroll
+    for (int r = 0; r < kTcR; ++r) fo[r] -= (d[0][r] + d[1][r]) + (d[2][r] + d[3][r]);
+}
+
+// L U c = f in single precision, f by position in rf.f (written by the caller);
+// on return fo holds c at this thread's position. One barrier pair per 32-row block.
+__device__ __forceinline__ void tc_solve(float (&fo)[kTcR], int pos, bool live, int lane, int w, int nb,
+                                         uint32_t trow, const float* __restrict__ S, int n, TcRefineSmem& rf) {
+    // forward: unit lower L, blocks ascending; rows below the block take its update
+    for (int J = 0; J < nb; ++J) {
+        const int j0 = J << 5;
+        float lv[32];
+        tc::tmem_ld32(trow + j0, lv);   // this row's columns j0..j0+31 (L entries when pos >= j0 + 32)
+        if (w == J) tc_block_diag(rf.inv[J][0], rf.f, j0, lane);
+        tc::wait_ld();
+        __syncthreads();
+        if (J + 1 < nb) {
+            if (live && pos >= j0 + 32) {
+                tc_block_update(fo, lv, rf.f, j0);
+#pragma unroll
+                for (int r = 0; r < kTcR; ++r) rf.f[pos][r] = fo[r];
+            }
+            __syncthreads();
+        }
+    }
+    if (live) {
+#pragma unroll
+        for (int r = 0; r < kTcR; ++r) fo[r] = rf.f[pos][r];
+    }
+    // backward: U, blocks descending; rows above the block take its update. A row's
+    // U entries of block J are 32 contiguous floats of its row-major U12 row; the next
+    // block's are loaded while this block's step runs.
+    float uv[32], un[32];
+    auto load_u = [&](int J, float (&dst)[32]) {
+        if (live && pos < (J << 5)) {
+            const float4* src = reinterpret_cast<const float4*>(S + (size_t)pos * n + (J << 5));
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const float4 v = src[q];
+                dst[4 * q] = v.x; dst[4 * q + 1] = v.y; dst[4 * q + 2] = v.z; dst[4 * q + 3] = v.w;
+            }
+        }
+    };
+    load_u(nb - 1, uv);
+    for (int J = nb - 1; J >= 0; --J) {
+        const int j0 = J << 5;
+        const bool above = live && pos < j0;
+        if (J > 0) load_u(J - 1, un);
+        if (w == J) tc_block_diag(rf.inv[J][1], rf.f, j0, lane);
+        __syncthreads();
+        if (J > 0) {
+            if (above) {
+                tc_block_update(fo, uv, rf.f, j0);
+#pragma unroll
+                for (int r = 0; r < kTcR; ++r) rf.f[pos][r] = fo[r];
+            }
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < 32; ++k) uv[k] = un[k];
+        }
+    }
+    if (live) {
+#pragma unroll
+        for (int r = 0; r < kTcR; ++r) fo[r] = rf.f[pos][r];
+    }
+}
+
+// Block-wide maxima of v and u per right-hand side (every thread gets them).
+__device__ __forceinline__ void tc_max2(double (&v)[kTcR], double (&u)[kTcR], int lane, int w, TcRefineSmem& rf) {
+#pragma unroll
+    for (int r = 0; r < kTcR; ++r) {
+        for (int off = 16; off > 0; off >>= 1) {
+            v[r] = fmax(v[r], __shfl_xor_sync(kFullMask, v[r], off));
+            u[r] = fmax(u[r], __shfl_xor_sync(kFullMask, u[r], off));
+        }
+    }
+    __syncthreads();   // the previous maxima have been read
+    if (lane == 0) {
+#pragma unroll
+        for (int r = 0; r < kTcR; ++r) {
+            rf.red[0][w][r] = v[r];
+            rf.red[1][w][r] = u[r];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kTcR; ++r) {
+        v[r] = 0.0;
+        u[r] = 0.0;
+        for (int k = 0; k < kTcNT / 32; ++k) {
+            v[r] = fmax(v[r], rf.red[0][k][r]);
+            u[r] = fmax(u[r], rf.red[1][k][r]);
+        }
+    }
+}
+
+// Returns iter: >= 0 refinement passes after the first solve, -2 when a residual does
+// not fit single precision, -31 when it does not converge (or stalls: the ratio of
+// residual to its bound fails to halve twice in a row).
+__device__ int tc_refine_instance(const TcLuArgs& g, int id, int t, int lane, int w, int pos, uint32_t trow,
+                                  const float* __restrict__ S, TcRefineSmem& rf, uint64_t keep) {
+    const int n = g.n, nb = n >> 5;
+    const bool live = t < n;
+    const double* A = g.dA[id];
+    const double* Bv = g.dB[id];
+    double* X = g.dX[id];
+    const double cte = g.anrm[id] * (DBL_EPSILON * 0.5) * sqrt((double)n);
+    // residual by row pairs when every row pair is 16-byte aligned (even lda, aligned A)
+    const bool pairs = (g.lda % 2 == 0) && ((reinterpret_cast<uintptr_t>(A) & 15) == 0);
+    int iter_out = 0;
+    for (int c0 = 0; c0 < g.nrhs && iter_out >= 0; c0 += kTcR) {
+        double b[kTcR], x[kTcR], res[kTcR];
+#pragma unroll
+        for (int r = 0; r < kTcR; ++r) {
+            b[r] = (live && c0 + r < g.nrhs) ? Bv[t + (size_t)(c0 + r) * g.ldb] : 0.0;
+            x[r] = 0.0;
+            res[r] = b[r];
+        }
+        int iiter = 0, stalls = 0;
+        double prev_ratio = 1e300;
+        for (;;) {
+            bool ovf = false;
+            float fo[kTcR];
+#pragma unroll
+            for (int r = 0; r < kTcR; ++r) {
+                ovf |= !(fabs(res[r]) <= (double)FLT_MAX);
+                fo[r] = (float)res[r];
+            }
+            if (__syncthreads_or(ovf)) { iter_out = -2; break; }
+            if (live) {
+#pragma unroll
+                for (int r = 0; r < kTcR; ++r) rf.f[pos][r] = fo[r];   // P r
+            }
+            __syncthreads();
+            tc_solve(fo, pos, live, lane, w, nb, trow, S, n, rf);
+            if (live) {
+#pragma unroll
+                for (int r = 0; r < kTcR; ++r) {
+                    x[r] += (double)fo[r];
+                    rf.xs[pos][r] = x[r];
+                }
+            }
+            __syncthreads();
+            // R = B - A X in double precision
+#pragma unroll
+            for (int r = 0; r < kTcR; ++r) res[r] = b[r];
+            if (pairs) {
+                // thread t: rows 2(t%128) and 2(t%128)+1 over column half t/128, 16-byte
+                // loads (two rows per load), 16 columns in flight; halves summed per row
+                const int rp = 2 * (t & 127), h = t >> 7, jh = n >> 1;
+                double p0[kTcR], p1[kTcR];
+#pragma unroll
+                for (int r = 0; r < kTcR; ++r) p0[r] = p1[r] = 0.0;
+                for (int j0 = h * jh; rp < n && j0 < (h + 1) * jh; j0 += 16) {
+                    double2 av[16];
+#pragma unroll
+                    for (int jj = 0; jj < 16; ++jj) av[jj] = ld_keep2(A + rp + (size_t)(j0 + jj) * g.lda, keep);
+#pragma unroll
+                    for (int jj = 0; jj < 16; ++jj) {
+                        const double4 xj = *reinterpret_cast<const double4*>(&rf.xs[j0 + jj][0]);
+                        p0[0] = fma(av[jj].x, xj.x, p0[0]); p1[0] = fma(av[jj].y, xj.x, p1[0]);
+                        p0[1] = fma(av[jj].x, xj.y, p0[1]); p1[1] = fma(av[jj].y, xj.y, p1[1]);
+                        p0[2] = fma(av[jj].x, xj.z, p0[2]); p1[2] = fma(av[jj].y, xj.z, p1[2]);
+                        p0[3] = fma(av[jj].x, xj.w, p0[3]); p1[3] = fma(av[jj].y, xj.w, p1[3]);
+                    }
+                }
+                if (rp < n) {
+                    *reinterpret_cast<double4*>(&rf.part[h][rp][0]) = make_double4(p0[0], p0[1], p0[2], p0[3]);
+                    *reinterpret_cast<double4*>(&rf.part[h][rp + 1][0]) = make_double4(p1[0], p1[1], p1[2], p1[3]);
+                }
+                __syncthreads();
+                if (live) {
+#pragma unroll
+                    for (int r = 0; r < kTcR; ++r) res[r] = b[r] - (rf.part[0][t][r] + rf.part[1][t][r]);
+                }
+            } else if (live) {
+                // 32 columns at a time: all 32 loads in flight before their fma's
+                for (int j0 = 0; j0 < n; j0 += 32) {
+                    double av[32];
+#pragma unroll
+                    for (int jj = 0; jj < 32; ++jj) av[jj] = ld_keep(A + t + (size_t)(j0 + jj) * g.lda, keep);
+#pragma unroll
+                    for (int jj = 0; jj < 32; ++jj) {
+                        const double4 xj = *reinterpret_cast<const double4*>(&rf.xs[j0 + jj][0]);
+                        res[0] = fma(-av[jj], xj.x, res[0]);
+                        res[1] = fma(-av[jj], xj.y, res[1]);
+                        res[2] = fma(-av[jj], xj.z, res[2]);
+                        res[3] = fma(-av[jj], xj.w, res[3]);
+                    }
+                }
+            }
+            double xn[kTcR], rn[kTcR];
+#pragma unroll
+            for (int r = 0; r < kTcR; ++r) {
+                const bool v = live && c0 + r < g.nrhs;
+                xn[r] = v ? fabs(x[r]) : 0.0;
+                rn[r] = v ? fabs(res[r]) : 0.0;
+            }
+            tc_max2(xn, rn, lane, w, rf);
+            bool ok = true;
+            double ratio = 0.0;
+#pragma unroll
+            for (int r = 0; r < kTcR; ++r) {
+                if (c0 + r < g.nrhs) {
+                    ok &= (rn[r] <= xn[r] * cte);
+                    ratio = fmax(ratio, rn[r] / fmax(xn[r] * cte, DBL_MIN));
+                }
+            }
+            if (ok) break;
+            ++iiter;
+            stalls = (ratio > 0.5 * prev_ratio) ? stalls + 1 : 0;
+            prev_ratio = ratio;
+            if (iiter >= kTcItermax || stalls >= 2) { iter_out = -kTcItermax - 1; break; }
+        }
+        if (iter_out < 0) break;
+        iter_out = max(iter_out, iiter);
+        if (live) {
+#pragma unroll
+            for (int r = 0; r < kTcR; ++r)
+                if (c0 + r < g.nrhs) X[pos + (size_t)(c0 + r) * g.ldx] = x[r];
+        }
+        __syncthreads();
+    }
+    return iter_out;
 }
 
 __global__ void __launch_bounds__(kTcNT, 1)
@@ -176,17 +505,20 @@ lu_tf32x3_kernel(TcLuArgs g) {
     const uint32_t trow = tbase + (uint32_t(32 * (w & 3)) << 16) + uint32_t(half * 256);
     uint32_t phase = 0;
     bool failed = false;
+    const uint64_t keep = l2_evict_last_policy();
     for (int id = blockIdx.x; id < g.batch && !failed; id += gridDim.x) {
         const double* A = g.dA[id];
         float* S = g.SA + (size_t)id * n * n;
         // ---- 1. FP64 row -> FP32 TMEM, row sums, overflow ----
+        // A is read with a high L2 retention priority: the refinement passes read it
+        // again, and the instances in flight (one per SM, 512 KB each at n = 256) fit L2
         double rs = 0.0;
         bool ovf = false;
         for (int c0 = 0; c0 < n; c0 += 32) {
             float v[32];
 #pragma unroll
             for (int c = 0; c < 32; ++c) {
-                const double a = (t < n) ? A[t + (size_t)(c0 + c) * g.lda] : 0.0;
+                const double a = (t < n) ? ld_keep(A + t + (size_t)(c0 + c) * g.lda, keep) : 0.0;
                 rs += fabs(a);
                 ovf |= !(fabs(a) <= (double)FLT_MAX);
                 v[c] = (float)a;
@@ -214,10 +546,6 @@ lu_tf32x3_kernel(TcLuArgs g) {
         int pos = (t < n) ? t : INT_MAX / 2;
         int info = 0;
         for (int k0 = 0; k0 < n && !failed; k0 += 32) {
-            // the next instance's FP64 columns into L2 while this one finishes (thread t:
-            // column t), so its conversion reads from L2 instead of HBM
-            if (k0 == (n >= 64 ? n - 64 : 0) && id + (int)gridDim.x < g.batch && t < n)
-                prefetch_l2(g.dA[id + gridDim.x] + (size_t)t * g.lda, unsigned(n) * 8u);
             float a[32];
             tc::tmem_ld32(trow + k0, a);
             tc::wait_ld();
@@ -229,7 +557,7 @@ lu_tf32x3_kernel(TcLuArgs g) {
             tc::tmem_st32(trow + k0, a);   // this row's panel entries, kept until it is stored
             if (piv) {
 #pragma unroll
-                for (int c = 0; c < 32; ++c) sh.L11[pos - k0][c] = a[c];
+                for (int c = 0; c < 32; ++c) sh.dblk[k0 >> 5][pos - k0][c] = a[c];
             }
             // a pivot row is final: the panel from registers now, its trailing entries to
             // shared memory for the U12 solve, and its columns left of the panel (which
@@ -245,19 +573,17 @@ lu_tf32x3_kernel(TcLuArgs g) {
                     }
                 }
             }
-            if (piv) {
-#pragma unroll
-                for (int c = 0; c < 32; ++c) S[pos + (size_t)(k0 + c) * n] = a[c];
-            }
             tc::wait_st();
             __syncthreads();
             if (ncols <= 0) break;
-            for (int c = t; c < ncols; c += kTcNT) tc_trsm_column(sh, c);
+            for (int c = t; c < ncols; c += kTcNT) tc_trsm_column(sh, sh.dblk[k0 >> 5], c);
             __syncthreads();
-            // U12 rows to the output, and the split B operand
+            // U12 rows to global memory (read by the refinement's backward sweeps), and the
+            // split B operand
+            // (row-major: position k0 + r, columns k0 + 32 ..; one row is contiguous)
             for (int idx = t; idx < 32 * ncols; idx += kTcNT) {
-                const int r = idx & 31, c = idx >> 5;
-                S[(k0 + r) + (size_t)(k0 + 32 + c) * n] = sh.Ug[r][c];
+                const int c = idx % ncols, r = idx / ncols;
+                S[(size_t)(k0 + r) * n + (k0 + 32 + c)] = sh.Ug[r][c];
             }
             for (int f = t; f < 32 * ncols; f += kTcNT) {
                 const int k = (f & 3) | (((f >> 5) & 7) << 2);
@@ -317,21 +643,25 @@ lu_tf32x3_kernel(TcLuArgs g) {
             }
             tc::fence_after_sync();
         }
+        if (t == 0) g.sinfo[id] = info;
         if (!failed) {
-            // every row's L entries left of the panel that chose it, at its final position
-            const int myk = (t < n) ? (pos & ~31) : 0;
-            const int wk = (int)__reduce_max_sync(kFullMask, (unsigned)myk);
-            for (int c0 = 0; c0 < wk; c0 += 32) {
-                float v[32];
-                tc::tmem_ld32(trow + c0, v);
-                tc::wait_ld();
-                if (c0 < myk) {
-#pragma unroll
-                    for (int c = 0; c < 32; ++c) S[pos + (size_t)(c0 + c) * n] = v[c];
+            __syncthreads();   // the factorisation is done: its operand buffers are free
+            TcRefineSmem& rf = *reinterpret_cast<TcRefineSmem*>(&sh.A[0][0][0]);
+            if (info != 0) {   // singular in single precision (block-uniform)
+                if (t == 0) {
+                    g.iter[id] = -3;
+                    g.fail_list[atomicAdd(g.fail_count, 1)] = id;
+                }
+            } else {
+                if (w < (n >> 5)) tc_invert_block(sh.dblk[w], rf.inv[w][0], rf.inv[w][1], lane);
+                __syncthreads();
+                const int it = tc_refine_instance(g, id, t, lane, w, pos, trow, S, rf, keep);
+                if (t == 0) {
+                    g.iter[id] = it;
+                    if (it < 0) g.fail_list[atomicAdd(g.fail_count, 1)] = id;
                 }
             }
         }
-        if (t == 0) g.sinfo[id] = info;
         if (failed && t == 0) {
             // hand this instance and the rest of this block's share to the FP64 fallback
             for (int j = id; j < g.batch; j += gridDim.x) {
@@ -346,6 +676,11 @@ lu_tf32x3_kernel(TcLuArgs g) {
     tc::fence_after_sync();
     if (w == 0) tc::tmem_dealloc(tbase, 512);
 }
+
+// The refinement's buffers overlay the L21 / U12 operand buffers (contiguous in TcLuSmem).
+static_assert(offsetof(TcLuSmem, B) == sizeof(float) * 2 * 2 * 128 * 32, "operand buffers contiguous");
+static_assert(sizeof(TcRefineSmem) <= offsetof(TcLuSmem, B) + sizeof(float) * 2 * kTcTrail * 32,
+              "refinement buffers fit the operand buffers");
 
 bool lu_tc_supported(int n) { return n >= 32 && n <= 256 && n % 32 == 0; }
 

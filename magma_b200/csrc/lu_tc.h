@@ -7,7 +7,7 @@ namespace mb200 {
 struct TcLuArgs {
     int n, batch, lda;
     double** dA;       // FP64 inputs (read only)
-    float* SA;         // FP32 LU factors, instance i at SA + i*n*n, ld n
+    float* SA;         // FP32 U12 blocks (above the diagonal blocks), instance i at SA + i*n*n, ld n
     int** ipiv;        // pivots (1-based)
     int* sinfo;        // FP32 getrf info
     double* anrm;      // ||A||_inf
@@ -17,6 +17,12 @@ struct TcLuArgs {
     int* err;          // set to 1 when a tensor-core wait timed out
     long long wait_limit;   // clock cycles a tensor-core completion wait may take
     int issue_mma;          // 0 only under the time-out test hook: no tensor-core work is issued
+    // the refinement that follows each instance's factorisation in the same block
+    int nrhs;
+    double** dB;       // right-hand sides (read only)
+    int ldb;
+    double** dX;       // solutions
+    int ldx;
 };
 
 bool lu_tc_supported(int n);

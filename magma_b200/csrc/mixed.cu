@@ -270,11 +270,14 @@ magma_int_t dsgesv_batched(int n, int nrhs, double** dA, int lda, int** ipiv, do
     cudaMemsetAsync(w.fail_count, 0, sizeof(int), s);
     magma_int_t rc = 0;
     queue_stage_begin(queue);   // stages: LU, refinement, FP64 fallback
-    if (use_tensor_core_lu(n)) {
-        // 1+2. conversion, norm and an FP32-accurate LU on the tensor cores, TMEM-resident
+    const bool tc = use_tensor_core_lu(n);
+    if (tc) {
+        // 1-3. conversion, norm, an FP32-accurate LU on the tensor cores (TMEM-resident)
+        // and the FP64 refinement, each instance in one block
         cudaMemsetAsync(w.err, 0, sizeof(int), s);
-        const TcLuArgs args{n, batch, lda, dA, w.SA, ipiv, w.sinfo, w.anrm, iter, w.fail_count, w.fail_list, w.err,
-                            0, 1};   // wait bound and MMA issue are set by lu_tc_launch
+        const TcLuArgs args{n,  batch, lda, dA, w.SA, ipiv, w.sinfo, w.anrm, iter, w.fail_count, w.fail_list, w.err,
+                            0, 1,   // wait bound and MMA issue are set by lu_tc_launch
+                            nrhs, dB, ldb, dX, ldx};
         if ((rc = lu_tc_launch(args, s))) return rc;
     } else {
         // 1. conversion + norm
@@ -288,12 +291,14 @@ magma_int_t dsgesv_batched(int n, int nrhs, double** dA, int lda, int** ipiv, do
         if (rc) return rc;
     }
     queue_stage_mark(queue);
-    // 3. refinement
-    if (n <= 64) launch_refine<64, R>(n, nrhs, dA, lda, ipiv, dB, ldb, dX, ldx, w, iter, batch, s);
-    else if (n <= 128) launch_refine<128, R>(n, nrhs, dA, lda, ipiv, dB, ldb, dX, ldx, w, iter, batch, s);
-    else if (n <= 256) launch_refine<256, R>(n, nrhs, dA, lda, ipiv, dB, ldb, dX, ldx, w, iter, batch, s);
-    else launch_refine<512, R>(n, nrhs, dA, lda, ipiv, dB, ldb, dX, ldx, w, iter, batch, s);
-    if ((rc = launch_status())) return rc;
+    // 3. refinement (already done inside the tensor-core kernel)
+    if (!tc) {
+        if (n <= 64) launch_refine<64, R>(n, nrhs, dA, lda, ipiv, dB, ldb, dX, ldx, w, iter, batch, s);
+        else if (n <= 128) launch_refine<128, R>(n, nrhs, dA, lda, ipiv, dB, ldb, dX, ldx, w, iter, batch, s);
+        else if (n <= 256) launch_refine<256, R>(n, nrhs, dA, lda, ipiv, dB, ldb, dX, ldx, w, iter, batch, s);
+        else launch_refine<512, R>(n, nrhs, dA, lda, ipiv, dB, ldb, dX, ldx, w, iter, batch, s);
+        if ((rc = launch_status())) return rc;
+    }
     queue_stage_mark(queue);
     // 4. FP64 fallback on the listed instances (the list length stays on the device)
     const WorkList failed{w.fail_list, w.fail_count, 0};
