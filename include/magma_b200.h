@@ -364,8 +364,8 @@ magma_int_t magma_dposv_vbatched_max_nocheck(magma_uplo_t uplo, magma_int_t* n, 
  * Kernel-variant tuning (no reference counterpart; takes the role of the
  * reference's static tables control/batched_kernel_param.h and the headers
  * under magmablas/gemm_config/). The table holds 13 values: the GEMM tile variant
- * (0: 64x64, 1: 32x32, 2: 16x16) for max(M,N) <= 16, <= 32, <= 64 and larger,
- * first for FP64 then FP32; 1/0 for the tensor-core LU in magma_dsgesv_batched
+ * (0: 64x64, 1: 32x32, 2: 16x16; for FP64 also 3: 64x64 on the tensor cores) for
+ * max(M,N) <= 16, <= 32, <= 64 and larger, first for FP64 then FP32; 1/0 for the tensor-core LU in magma_dsgesv_batched
  * (n = 96..256, step 32); and 1/0 for the FP64 blocked LU's trailing update on the
  * tensor cores (DMMA) instead of the FP64 pipe, for max(m) <= 128, <= 256, <= 512,
  * <= 1024. A 9-value table (saved before the LU entries existed) is accepted and

@@ -2,8 +2,9 @@
 //
 // Replaces magmablas_{d,s}gemm_batched_core (magmablas/dgemm_batched_core.cu:161-436) and
 // magmablas_{d,s}gemm_vbatched_core (magmablas/dgemm_vbatched_core.cu:28-266). One
-// thread block computes one BM x BN tile of one instance's C (three tile shapes:
-// 64x64 with 256 threads, 32x32 and 16x16 with 64 threads); op(A) and op(B) are
+// thread block computes one BM x BN tile of one instance's C (three CUDA-core tile
+// shapes: 64x64 with 256 threads, 32x32 and 16x16 with 64 threads, and for FP64 a
+// 64x64 tile on the tensor cores, gemm_dmma_kernel); op(A) and op(B) are
 // staged through shared memory in K chunks of 16, transposed at load time so the
 // inner loop always reads contiguous vectors, with the next chunk prefetched into
 // registers while the current one is used. Every shape accumulates each output
@@ -153,6 +154,241 @@ gemm_tile_kernel(GemmSizes g, T alpha, const T* const* __restrict__ A_arr, const
     }
 }
 
+// NN form of the CUDA-core tiles with an asynchronous operand pipeline: each K chunk
+// of op(A) and op(B) is copied global -> shared by cp.async (element-sized copies,
+// zero-filled past the instance's edges), three chunks in flight, so the loads of
+// chunks c+1 and c+2 overlap the arithmetic of chunk c without passing through
+// registers. The staged layout and the inner loop are gemm_tile_kernel's, so each
+// output receives the same fma's in the same order (bit-identical variants).
+template <int STAGES, typename T, typename S>
+struct GemmAsyncSmem {
+    T a[STAGES][S::BK][S::BM + 1];
+    T b[STAGES][S::BK][S::BN + 1];
+};
+
+__device__ __forceinline__ void cp_async_elem(void* dst, const void* src, bool valid, int bytes) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    const int sz = valid ? bytes : 0;   // src-size 0: the destination is zero-filled, nothing is read
+    if (bytes == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(sz) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(sz) : "memory");
+}
+
+template <typename T, typename S>
+__global__ void __launch_bounds__(S::NT, (sizeof(T) == 8 ? S::MINB_D : S::MINB_F))
+gemm_async_kernel(GemmSizes g, T alpha, const T* const* __restrict__ A_arr, const T* const* __restrict__ B_arr,
+                  T beta, T** __restrict__ C_arr, int tiles_m, int tiles_n, WorkList wl) {
+    constexpr int BM = S::BM, BN = S::BN, BK = S::BK, TM = S::TM, TN = S::TN, NT = S::NT, ST = 3;
+    constexpr int EA = S::EA, EB = S::EB;
+    extern __shared__ __align__(16) unsigned char gemm_async_raw[];
+    GemmAsyncSmem<ST, T, S>& sm = *reinterpret_cast<GemmAsyncSmem<ST, T, S>*>(gemm_async_raw);
+    const int tiles = tiles_m * tiles_n;
+    const int w = blockIdx.x / tiles;
+    if (w >= wl.size()) return;
+    const int id = wl.at(w);
+    const int t = blockIdx.x - w * tiles;
+    const int i0 = (t / tiles_n) * BM, j0 = (t % tiles_n) * BN;
+    const int m = g.M(id), n = g.N(id), k = g.K(id);
+    if (i0 >= m || j0 >= n) return;
+    if ((g.tri == 1 && j0 > i0 + BM - 1) || (g.tri == 2 && i0 > j0 + BN - 1)) return;
+    const int lda = g.LDA(id), ldb = g.LDB(id), ldc = g.LDC(id);
+    const T* A = A_arr[id];
+    const T* B = B_arr[id];
+    T* C = C_arr[id];
+    const int tid = threadIdx.x;
+    const int tx = tid % (BM / TM), ty = tid / (BM / TM);
+    T acc[TM][TN];
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+        for (int j = 0; j < TN; ++j) acc[i][j] = T(0);
+    auto issue = [&](int chunk) {
+        const int st = chunk % ST, k0 = chunk * BK;
+#pragma unroll
+        for (int e = 0; e < EA; ++e) {   // A (M x K, column-major): rows fastest, contiguous
+            const int idx = tid + e * NT, r = idx % BM, c = idx / BM;
+            const bool v = (i0 + r < m) && (k0 + c < k);
+            cp_async_elem(&sm.a[st][c][r], v ? A + (i0 + r) + (size_t)(k0 + c) * lda : A, v, sizeof(T));
+        }
+#pragma unroll
+        for (int e = 0; e < EB; ++e) {   // B (K x N, column-major): k fastest, contiguous
+            const int idx = tid + e * NT, c = idx % BK, j = idx / BK;
+            const bool v = (k0 + c < k) && (j0 + j < n);
+            cp_async_elem(&sm.b[st][c][j], v ? B + (k0 + c) + (size_t)(j0 + j) * ldb : B, v, sizeof(T));
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    const int nchunks = (k + BK - 1) / BK;
+    issue(0);
+    if (nchunks > 1) issue(1); else asm volatile("cp.async.commit_group;" ::: "memory");
+    for (int c = 0; c < nchunks; ++c) {
+        asm volatile("cp.async.wait_group 1;" ::: "memory");   // chunk c has landed (c+1 may be in flight)
+        __syncthreads();                                         // ... for every thread; stage (c+2)%3 is free
+        if (c + 2 < nchunks) issue(c + 2); else asm volatile("cp.async.commit_group;" ::: "memory");
+        const int st = c % ST;
+#pragma unroll
+        for (int kk = 0; kk < BK; ++kk) {
+            T a[TM], b[TN];
+#pragma unroll
+            for (int i = 0; i < TM; ++i) a[i] = sm.a[st][kk][tx + (BM / TM) * i];
+#pragma unroll
+            for (int j = 0; j < TN; ++j) b[j] = sm.b[st][kk][ty * TN + j];
+#pragma unroll
+            for (int i = 0; i < TM; ++i)
+#pragma unroll
+                for (int j = 0; j < TN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        }
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+        const int gj = j0 + ty * TN + j;
+        if (gj >= n) continue;
+#pragma unroll
+        for (int i = 0; i < TM; ++i) {
+            const int gi = i0 + tx + (BM / TM) * i;
+            if (gi >= m || (g.tri == 1 && gj > gi) || (g.tri == 2 && gi > gj)) continue;
+            T* cp = C + gi + (size_t)gj * ldc;
+            *cp = (beta == T(0)) ? alpha * acc[i][j] : alpha * acc[i][j] + beta * (*cp);
+        }
+    }
+}
+
+// FP64 tile on the tensor cores (variant 3): a 64x64 tile of C per 256-thread block,
+// each warp a 32x16 sub-tile as 4x2 tiles of 8x8 updated by mma.sync m8n8k4 .f64.
+// Staging is that of gemm_tile_kernel (K chunks of 16, transposed at load time, the
+// next chunk prefetched into registers); the fragments are read from the staged
+// chunk (rows padded to 68 doubles: the four k rows a fragment load touches fall on
+// different banks). An m8n8k4 FP64 MMA applies its four products to each element as
+// fma's in ascending k, and the k-steps run in ascending order, so every output gets
+// exactly the fma chain of the CUDA-core tiles: the variants stay bit-identical.
+__device__ __forceinline__ void gemm_dmma(double& d0, double& d1, double a, double b) {
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+        : "+d"(d0), "+d"(d1)
+        : "d"(a), "d"(b));
+}
+
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(256, 2)
+gemm_dmma_kernel(GemmSizes g, double alpha, const double* const* __restrict__ A_arr,
+                 const double* const* __restrict__ B_arr, double beta, double** __restrict__ C_arr, int tiles_m,
+                 int tiles_n, WorkList wl) {
+    constexpr int BM = 64, BN = 64, BK = 16, NT = 256, PAD = 68;
+    constexpr int EA = BM * BK / NT, EB = BK * BN / NT;
+    __shared__ __align__(16) double sA[BK][PAD];
+    __shared__ __align__(16) double sB[BK][PAD];
+    const int tiles = tiles_m * tiles_n;
+    const int w = blockIdx.x / tiles;
+    if (w >= wl.size()) return;
+    const int id = wl.at(w);
+    const int t = blockIdx.x - w * tiles;
+    const int i0 = (t / tiles_n) * BM, j0 = (t % tiles_n) * BN;
+    const int m = g.M(id), n = g.N(id), k = g.K(id);
+    if (i0 >= m || j0 >= n) return;
+    if ((g.tri == 1 && j0 > i0 + BM - 1) || (g.tri == 2 && i0 > j0 + BN - 1)) return;
+    const int lda = g.LDA(id), ldb = g.LDB(id), ldc = g.LDC(id);
+    const double* A = A_arr[id];
+    const double* B = B_arr[id];
+    double* C = C_arr[id];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;   // warp's sub-tile
+    const int q = lane & 3, r8 = lane >> 2;
+    double acc[4][2][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    double ra[EA], rb[EB];
+    auto load_chunk = [&](int k0) {
+#pragma unroll
+        for (int e = 0; e < EA; ++e) {
+            const int idx = tid + e * NT;
+            int r, c;
+            if (!TA) { r = idx % BM; c = idx / BM; } else { c = idx % BK; r = idx / BK; }
+            const int gi = i0 + r, gk = k0 + c;
+            ra[e] = (gi < m && gk < k) ? (TA ? A[gk + (size_t)gi * lda] : A[gi + (size_t)gk * lda]) : 0.0;
+        }
+#pragma unroll
+        for (int e = 0; e < EB; ++e) {
+            const int idx = tid + e * NT;
+            int c, j;
+            if (!TB) { c = idx % BK; j = idx / BK; } else { j = idx % BN; c = idx / BN; }
+            const int gk = k0 + c, gj = j0 + j;
+            rb[e] = (gk < k && gj < n) ? (TB ? B[gj + (size_t)gk * ldb] : B[gk + (size_t)gj * ldb]) : 0.0;
+        }
+    };
+    auto store_chunk = [&]() {
+#pragma unroll
+        for (int e = 0; e < EA; ++e) {
+            const int idx = tid + e * NT;
+            int r, c;
+            if (!TA) { r = idx % BM; c = idx / BM; } else { c = idx % BK; r = idx / BK; }
+            sA[c][r] = ra[e];
+        }
+#pragma unroll
+        for (int e = 0; e < EB; ++e) {
+            const int idx = tid + e * NT;
+            int c, j;
+            if (!TB) { c = idx % BK; j = idx / BK; } else { j = idx % BN; c = idx / BN; }
+            sB[c][j] = rb[e];
+        }
+    };
+    if (k > 0) load_chunk(0);
+    for (int k0 = 0; k0 < k; k0 += BK) {
+        __syncthreads();
+        store_chunk();
+        __syncthreads();
+        if (k0 + BK < k) load_chunk(k0 + BK);   // prefetch the next chunk while computing
+#pragma unroll
+        for (int s4 = 0; s4 < BK / 4; ++s4) {
+            double af[4], bf[2];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) af[i] = sA[4 * s4 + q][wm + 8 * i + r8];
+#pragma unroll
+            for (int j = 0; j < 2; ++j) bf[j] = sB[4 * s4 + q][wn + 8 * j + r8];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) gemm_dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int gi = i0 + wm + 8 * i + r8;
+        if (gi >= m) continue;
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int gj = j0 + wn + 8 * j + 2 * q + h;
+                if (gj >= n || (g.tri == 1 && gj > gi) || (g.tri == 2 && gi > gj)) continue;
+                double* c = C + gi + (size_t)gj * ldc;
+                *c = (beta == 0.0) ? alpha * acc[i][j][h] : alpha * acc[i][j][h] + beta * (*c);
+            }
+        }
+    }
+}
+
+template <typename T>
+static magma_int_t gemm_launch_dmma(bool TA, bool TB, const GemmSizes& g, T alpha, const T* const* A,
+                                    const T* const* B, T beta, T** C, const WorkList& wl, int bound, int max_m,
+                                    int max_n, cudaStream_t s) {
+    if constexpr (sizeof(T) != 8) {
+        return MAGMA_ERR_NOT_SUPPORTED;
+    } else {
+        const int tiles_m = ceildiv(max_m, 64), tiles_n = ceildiv(max_n, 64);
+        const long blocks = (long)bound * tiles_m * tiles_n;
+        if (blocks > 0x7fffffffL) return MAGMA_ERR_NOT_SUPPORTED;
+        const dim3 grid((unsigned)blocks);
+        if (!TA && !TB) gemm_dmma_kernel<false, false><<<grid, 256, 0, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n, wl);
+        else if (!TA && TB) gemm_dmma_kernel<false, true><<<grid, 256, 0, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n, wl);
+        else if (TA && !TB) gemm_dmma_kernel<true, false><<<grid, 256, 0, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n, wl);
+        else gemm_dmma_kernel<true, true><<<grid, 256, 0, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n, wl);
+        return 0;
+    }
+}
+
 template <typename T, typename S>
 static magma_int_t gemm_launch_tile(bool TA, bool TB, const GemmSizes& g, T alpha, const T* const* A, const T* const* B,
                                     T beta, T** C, const WorkList& wl, int bound, int max_m, int max_n,
@@ -161,7 +397,13 @@ static magma_int_t gemm_launch_tile(bool TA, bool TB, const GemmSizes& g, T alph
     const long blocks = (long)bound * tiles_m * tiles_n;
     if (blocks > 0x7fffffffL) return MAGMA_ERR_NOT_SUPPORTED;
     const dim3 grid((unsigned)blocks);
-    if (!TA && !TB) gemm_tile_kernel<T, false, false, S><<<grid, S::NT, 0, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n, wl);
+    if (!TA && !TB && sizeof(T) == 8) {   // FP64 NN: the asynchronous-copy pipeline (measured faster
+                                          // for FP64 on the C2 mix, slower for FP32)
+        auto kern = gemm_async_kernel<T, S>;
+        const int smem = (int)sizeof(GemmAsyncSmem<3, T, S>);
+        ensure_dynamic_smem((const void*)kern, smem);
+        kern<<<grid, S::NT, smem, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n, wl);
+    } else if (!TA && !TB) gemm_tile_kernel<T, false, false, S><<<grid, S::NT, 0, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n, wl);
     else if (!TA && TB) gemm_tile_kernel<T, false, true, S><<<grid, S::NT, 0, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n, wl);
     else if (TA && !TB) gemm_tile_kernel<T, true, false, S><<<grid, S::NT, 0, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n, wl);
     else gemm_tile_kernel<T, true, true, S><<<grid, S::NT, 0, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n, wl);
@@ -176,6 +418,9 @@ static magma_int_t gemm_launch_variant(int variant, magma_trans_t ta, magma_tran
     switch (variant) {
         case 1: return gemm_launch_tile<T, GemmTile1>(TA, TB, g, alpha, A, B, beta, C, wl, bound, max_m, max_n, s);
         case 2: return gemm_launch_tile<T, GemmTile2>(TA, TB, g, alpha, A, B, beta, C, wl, bound, max_m, max_n, s);
+        case 3:   // FP64 tensor cores; FP32 has no such variant and takes the 64x64 tile
+            if (sizeof(T) == 8) return gemm_launch_dmma<T>(TA, TB, g, alpha, A, B, beta, C, wl, bound, max_m, max_n, s);
+            return gemm_launch_tile<T, GemmTile0>(TA, TB, g, alpha, A, B, beta, C, wl, bound, max_m, max_n, s);
         default: return gemm_launch_tile<T, GemmTile0>(TA, TB, g, alpha, A, B, beta, C, wl, bound, max_m, max_n, s);
     }
 }

@@ -50,7 +50,7 @@ static void to_values(const TuningTable& t, int* v) {
 static bool from_values(const int* v, int count, TuningTable& t) {
     if (count != kTuningValues && count != kTuningValuesV1) return false;
     for (int i = 0; i < 2 * kGemmBuckets; ++i)
-        if (v[i] < 0 || v[i] > 2) return false;
+        if (v[i] < 0 || v[i] > (i < kGemmBuckets ? 3 : 2)) return false;   // 3: FP64 tensor-core tile
     for (int i = 2 * kGemmBuckets; i < count; ++i)
         if (v[i] != 0 && v[i] != 1) return false;
     int i = 0;
@@ -190,7 +190,7 @@ static magma_int_t tune_gemm(int prec, magma_queue_t q, unsigned seed) {
         T** pA = (T**)dP.p; T** pB = pA + count; T** pC = pB + count;
         float best = 1e30f;
         int best_v = tuning().gemm_variant[prec][b];
-        for (int v = 0; v < 3; ++v) {
+        for (int v = 0; v < (sizeof(T) == 8 ? 4 : 3); ++v) {
             tuning_mut().gemm_variant[prec][b] = v;
             const float ms = time_ms(q->stream, [&] {
                 if (sizeof(T) == 8)

@@ -12,7 +12,8 @@ constexpr int kGemmBuckets = 4;   // max(M, N) <= 16, <= 32, <= 64, larger
 constexpr int kLuBlockedBuckets = 4;   // blocked LU by max(m): <= 128, <= 256, <= 512, <= 1024
 
 struct TuningTable {
-    int gemm_variant[2][kGemmBuckets];   // [FP64, FP32][bucket]: tile variant (0: 64x64, 1: 32x32, 2: 16x16)
+    int gemm_variant[2][kGemmBuckets];   // [FP64, FP32][bucket]: tile variant (0: 64x64, 1: 32x32, 2: 16x16,
+                                         // 3: FP64 only, 64x64 on the tensor cores)
     int mixed_tc_lu;                     // 1: tensor-core LU in the mixed solve for n = 96..256, step 32
     int lu_dmma[kLuBlockedBuckets];      // 1: FP64 blocked LU trailing update on the tensor cores (DMMA)
 };

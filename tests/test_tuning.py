@@ -38,7 +38,10 @@ def test_tuning_roundtrip(tmp_path):
         assert lib.magma_b200_tuning_load(str(f).encode()) == 0 and _get(lib) == new
         # rejected: wrong count, out-of-range values, unreadable or malformed files
         assert _set(lib, new[:-1]) == _lib.MAGMA_ERR_ILLEGAL_VALUE
-        assert _set(lib, [3] + new[1:]) == _lib.MAGMA_ERR_ILLEGAL_VALUE
+        assert _set(lib, [4] + new[1:]) == _lib.MAGMA_ERR_ILLEGAL_VALUE      # FP64 tiles: 0..3
+        assert _set(lib, new[:4] + [3] + new[5:]) == _lib.MAGMA_ERR_ILLEGAL_VALUE   # FP32 tiles: 0..2
+        assert _set(lib, [3] + new[1:]) == 0 and _get(lib)[0] == 3
+        assert _set(lib, new) == 0
         assert _set(lib, new[:-1] + [2]) == _lib.MAGMA_ERR_ILLEGAL_VALUE
         # a 9-value table (saved before the LU update entries) sets the first 9 only
         assert _set(lib, orig[:9]) == 0 and _get(lib) == orig[:9] + new[9:]
@@ -72,7 +75,7 @@ def test_gemm_variants_bit_identical(cuda):
             As = [rng.standard_normal((int(k), int(m))) for m, k in zip(M, K)]
             Bs = [rng.standard_normal((int(n), int(k))) for k, n in zip(K, N)]
             Cs = [rng.standard_normal((int(n), int(m))) for m, n in zip(M, N)]
-            for v in range(3):
+            for v in range(4 if prec == "d" else 3):
                 vals = list(orig)
                 for b in range(4):
                     vals[(0 if prec == "d" else 4) + b] = v
@@ -83,6 +86,8 @@ def test_gemm_variants_bit_identical(cuda):
                 outs[(prec, v)] = gC.buf.cpu().numpy()
             assert np.array_equal(outs[(prec, 0)], outs[(prec, 1)])
             assert np.array_equal(outs[(prec, 0)], outs[(prec, 2)])
+            if prec == "d":   # the FP64 tensor-core tile
+                assert np.array_equal(outs[(prec, 0)], outs[(prec, 3)])
             # and the result is right (FP64 reference)
             ref = [a.T @ b.T + 0.5 * c.T for a, b, c in zip(As, Bs, Cs)]
             got = VarBatch(Cs, cuda, dt)
@@ -103,7 +108,8 @@ def test_autotune_runs(cuda, tmp_path):
         q = default_queue()
         assert lib.magma_b200_autotune(q.handle) == 0
         vals = _get(lib)
-        assert all(0 <= v <= 2 for v in vals[:8]) and all(v in (0, 1) for v in vals[8:])
+        assert all(0 <= v <= 3 for v in vals[:4]) and all(0 <= v <= 2 for v in vals[4:8])
+        assert all(v in (0, 1) for v in vals[8:])
         f = tmp_path / "tuned.txt"
         assert lib.magma_b200_tuning_save(str(f).encode()) == 0
     finally:
