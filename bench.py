@@ -342,7 +342,7 @@ class C3Mixed:
         self.h2d = self.hA.numel() * 8 + self.hB.numel() * 8
         self.d2h = self.hX.numel() * 8 + 8 * self.batch
 
-    e2e_api = "magma_b200.api.HostDsgesv, 8 chunks: uploads, solves and read-backs overlapped"
+    e2e_api = "magma_b200_host_solve (C++; Python binding HostDsgesv), 8 chunks: uploads, solves and read-backs overlapped"
 
     def e2e_step(self, q, i):
         if getattr(self, "pipe", None) is None:
@@ -479,7 +479,7 @@ class C1DgesvSmall:
         self.h2d = self.hA.numel() * 8 + self.hB.numel() * 8
         self.d2h = self.hX.numel() * 8 + self.hP.numel() * 4 + self.hI.numel() * 4
 
-    e2e_api = "magma_b200.api.HostDgesv, 4 chunks: uploads, solves and read-backs overlapped"
+    e2e_api = "magma_b200_host_solve (C++; Python binding HostDgesv), 4 chunks: uploads, solves and read-backs overlapped"
 
     def e2e_step(self, q, i):
         if getattr(self, "pipe", None) is None:

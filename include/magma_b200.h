@@ -53,6 +53,11 @@ void magma_setdevice(magma_device_t dev);
 magma_int_t magma_malloc(magma_ptr* ptr_ptr, size_t bytes);
 magma_int_t magma_free_internal(magma_ptr ptr, const char* func, const char* file, int line);
 #define magma_free(ptr) magma_free_internal(ptr, __func__, __FILE__, __LINE__)
+/* interface_cuda/alloc.cpp:242 (magma_malloc_pinned), :276 (magma_free_pinned_internal):
+ * page-locked host memory, MAGMA_ERR_HOST_ALLOC / MAGMA_ERR_INVALID_PTR on failure */
+magma_int_t magma_malloc_pinned(void** ptr_ptr, size_t bytes);
+magma_int_t magma_free_pinned_internal(void* ptr, const char* func, const char* file, int line);
+#define magma_free_pinned(ptr) magma_free_pinned_internal(ptr, __func__, __FILE__, __LINE__)
 
 /* include/magma_auxiliary.h:248-281 (queue support; the public names are
  * macros over the *_internal symbols, exactly as in MAGMA). */
@@ -359,6 +364,36 @@ magma_int_t magma_dposv_vbatched_max_nocheck(magma_uplo_t uplo, magma_int_t* n, 
                                              double** dA_array, magma_int_t* ldda, double** dB_array,
                                              magma_int_t* lddb, magma_int_t* dinfo_array, magma_int_t batchCount,
                                              magma_int_t max_n, magma_int_t max_nrhs, magma_queue_t queue);
+
+/* ------------------------------------------------------------------------
+ * Systems in host memory (no reference counterpart: MAGMA's batched routines take
+ * device pointer arrays only, and its testers upload, solve and read back in
+ * sequence, testing/testing_zgesv_batched.cpp:111-125). A solver owns device
+ * staging buffers, pointer arrays, two copy streams and per-chunk events for
+ * `batch` systems of order n with nrhs right-hand sides, cut into `chunks` chunks;
+ * magma_b200_host_solve queues every chunk's upload on one copy stream, solves each
+ * chunk on the queue's stream as soon as it has landed (magma_dsgesv_batched for
+ * MAGMA_B200_HOST_DSGESV, magma_dgesv_batched for MAGMA_B200_HOST_DGESV) and reads its
+ * results back on a second copy stream, so transfers overlap the solves. Host layouts
+ * are packed batches of column-major matrices: hA batch x (n x lda), hB batch x
+ * (n x nrhs, ldb); outputs hX (DSGESV: batch x (n x nrhs, ld n); DGESV: the solutions
+ * in hB's layout), hI (DSGESV: iter per system; DGESV: batch x n pivots) and hInfo
+ * (batch). A solve returns once everything is queued (the first solver error, or
+ * MAGMA_SUCCESS); synchronising the queue covers the whole sequence. Page-locked
+ * host memory is needed for the copies to overlap (pageable memory gives the same
+ * results in sequence). create returns -1..-9 for an illegal argument or
+ * MAGMA_ERR_DEVICE_ALLOC; chunk_start returns chunk c's first system (c = chunks:
+ * batch), -1 out of range. */
+enum { MAGMA_B200_HOST_DSGESV = 0, MAGMA_B200_HOST_DGESV = 1 };
+struct magma_b200_host_solver;
+typedef struct magma_b200_host_solver* magma_b200_host_solver_t;
+magma_int_t magma_b200_host_solver_create(magma_int_t kind, magma_int_t batch, magma_int_t n, magma_int_t nrhs,
+                                          magma_int_t lda, magma_int_t ldb, magma_int_t chunks, magma_queue_t queue,
+                                          magma_b200_host_solver_t* solver);
+magma_int_t magma_b200_host_solve(magma_b200_host_solver_t solver, const double* hA, const double* hB, double* hX,
+                                  magma_int_t* hI, magma_int_t* hInfo);
+magma_int_t magma_b200_host_solver_chunk_start(magma_b200_host_solver_t solver, magma_int_t c);
+magma_int_t magma_b200_host_solver_destroy(magma_b200_host_solver_t solver);
 
 /* ------------------------------------------------------------------------
  * Kernel-variant tuning (no reference counterpart; takes the role of the

@@ -43,6 +43,8 @@ SIGNATURES: dict[str, tuple] = {
     "magma_setdevice": (None, [_i]),
     "magma_malloc": (_i, [C.POINTER(_p), _sz]),
     "magma_free_internal": (_i, [_p, _s, _s, _i]),
+    "magma_malloc_pinned": (_i, [C.POINTER(_p), _sz]),
+    "magma_free_pinned_internal": (_i, [_p, _s, _s, _i]),
     "magma_queue_create_internal": (None, [_i, C.POINTER(_p), _s, _s, _i]),
     "magma_queue_create_from_cuda_internal": (None, [_i, _p, _p, _p, C.POINTER(_p), _s, _s, _i]),
     "magma_queue_destroy_internal": (None, [_p, _s, _s, _i]),
@@ -149,6 +151,10 @@ SIGNATURES: dict[str, tuple] = {
     "magma_b200_tuning_save": (_i, [_s]),
     "magma_b200_tuning_load": (_i, [_s]),
     # request loop (include/magma_b200_serve.h)
+    "magma_b200_host_solver_create": (_i, [_i, _i, _i, _i, _i, _i, _i, _p, C.POINTER(_p)]),
+    "magma_b200_host_solve": (_i, [_p, _p, _p, _p, _p, _p]),
+    "magma_b200_host_solver_chunk_start": (_i, [_p, _i]),
+    "magma_b200_host_solver_destroy": (_i, [_p]),
     "magma_b200_server_create": (_i, [_i, _sz, _i, _i, C.POINTER(_p)]),
     "magma_b200_server_submit": (_i, [_p, _i, _i, _i, _p, _i, _p, _i, _p, _i, C.c_longlong]),
     "magma_b200_server_poll": (_i, [_p, _p, _p, _p, _p, _i]),

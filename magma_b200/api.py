@@ -264,7 +264,8 @@ def dsgesv_batched(A: torch.Tensor, B: torch.Tensor, queue: Queue | None = None)
 
 class _HostPipeline:
     """Batched solve of systems that live in pinned host memory, with the transfers
-    pipelined against the solves.
+    pipelined against the solves: a binding of the library's magma_b200_host_solver
+    (include/magma_b200.h).
 
     The batch is cut into `chunks` slices. All slices' uploads are queued on one copy
     stream, back to back, so the host-to-device link never idles; slice c is solved on the
@@ -275,7 +276,9 @@ class _HostPipeline:
     A call is asynchronous: it returns once everything is queued, and the queue's stream
     waits for the last read-back, so a stream synchronize (or an event recorded on that
     stream) covers the whole transfer-solve-transfer sequence. Device staging buffers,
-    streams and pointer arrays are allocated once, at construction."""
+    streams, events and pointer arrays are allocated once, by the library, at construction."""
+
+    _kind = 0
 
     def __init__(self, batch: int, n: int, nrhs: int, chunks: int, queue: Queue | None, lda: int | None,
                  ldb: int | None):
@@ -286,94 +289,87 @@ class _HostPipeline:
         self.lda, self.ldb = lda or n, ldb or n
         if self.lda < n or self.ldb < n:
             raise ValueError("lda and ldb must be at least n")
-        self.dev = torch.device("cuda", torch.cuda.current_device())
-        f64 = dict(dtype=torch.float64, device=self.dev)
-        self.A = torch.empty((batch, n, self.lda), **f64)
-        self.B = torch.empty((batch, nrhs, self.ldb), **f64)
-        self.ipiv = torch.zeros((batch, n), dtype=torch.int32, device=self.dev)
-        self.info = torch.zeros(batch, dtype=torch.int32, device=self.dev)
-        self.pA, self.pB, self.pP = ptr_array(self.A), ptr_array(self.B), ptr_array(self.ipiv)
-        per = -(-batch // chunks)
-        self.bounds = [(c0, min(batch, c0 + per)) for c0 in range(0, batch, per)]
-        self.up, self.down = torch.cuda.Stream(self.dev), torch.cuda.Stream(self.dev)
+        h = C.c_void_p()
+        _check(self.q.lib.magma_b200_host_solver_create(self._kind, batch, n, nrhs, self.lda, self.ldb, chunks,
+                                                        self.q.handle, C.byref(h)), "magma_b200_host_solver_create")
+        self.h = h
+        starts = []
+        c = 0
+        while True:
+            st = self.q.lib.magma_b200_host_solver_chunk_start(h, c)
+            if st < 0:
+                break
+            starts.append(st)
+            c += 1
+        self.bounds = list(zip(starts[:-1], starts[1:]))
 
-    def _run(self, hA, hB, reads, solve) -> None:
-        """Uploads hA/hB, calls solve(c0, c1) per slice on the queue's stream and copies
-        each (host, device) pair of `reads` back slice by slice."""
-        for t in (hA, hB, *(h for h, _ in reads)):
+    def _shapes(self):
+        raise NotImplementedError
+
+    def _run(self, hA, hB, hX, hI, hInfo) -> None:
+        shapes = self._shapes()
+        for t, (shape, dtype), name in zip((hA, hB, hX, hI, hInfo), shapes, ("hA", "hB", "hX", "hI", "hInfo")):
             if t.is_cuda or not t.is_pinned():
-                raise ValueError(f"{type(self).__name__} takes pinned host tensors")
-        if tuple(hA.shape) != tuple(self.A.shape) or tuple(hB.shape) != tuple(self.B.shape):
-            raise ValueError("hA/hB shapes differ from the ones the solver was built for")
-        for h, d in reads:
-            if tuple(h.shape) != tuple(d.shape) or h.dtype != d.dtype:
-                raise ValueError(f"output of shape {tuple(h.shape)} ({h.dtype}) expected {tuple(d.shape)} ({d.dtype})")
-        ws = self.q.stream
-        self.up.wait_stream(ws)       # earlier work on the staging buffers is ordered first
-        self.down.wait_stream(ws)
-        landed = []
-        with torch.cuda.stream(self.up):
-            for c0, c1 in self.bounds:
-                self.A[c0:c1].copy_(hA[c0:c1], non_blocking=True)
-                self.B[c0:c1].copy_(hB[c0:c1], non_blocking=True)
-                landed.append(self.up.record_event())
-        for (c0, c1), ev in zip(self.bounds, landed):
-            ws.wait_event(ev)
-            solve(c0, c1)
-            solved = ws.record_event()
-            self.down.wait_event(solved)
-            with torch.cuda.stream(self.down):
-                for h, d in reads:
-                    h[c0:c1].copy_(d[c0:c1], non_blocking=True)
-        ws.wait_stream(self.down)
+                raise ValueError(f"{type(self).__name__} takes pinned host tensors ({name})")
+            if tuple(t.shape) != shape or t.dtype != dtype or not t.is_contiguous():
+                raise ValueError(f"{name} of shape {tuple(t.shape)} ({t.dtype}) expected {shape} ({dtype}), contiguous")
+        _check(self.q.lib.magma_b200_host_solve(self.h, _vp(hA), _vp(hB), _vp(hX), _vp(hI), _vp(hInfo)),
+               "magma_b200_host_solve")
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.q.lib.magma_b200_host_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class HostDsgesv(_HostPipeline):
     """magma_dsgesv_batched (FP32 LU, FP64 refinement, FP64 fallback) on systems in pinned
     host memory, uploads and read-backs overlapped with the solves chunk by chunk."""
 
+    _kind = 0   # MAGMA_B200_HOST_DSGESV
+
     def __init__(self, batch: int, n: int, nrhs: int, chunks: int = 8, queue: Queue | None = None,
                  lda: int | None = None, ldb: int | None = None):
         super().__init__(batch, n, nrhs, chunks, queue, lda, ldb)
-        self.X = torch.empty((batch, nrhs, n), dtype=torch.float64, device=self.dev)
-        self.iter = torch.zeros(batch, dtype=torch.int32, device=self.dev)
-        self.pX = ptr_array(self.X)
+
+    def _shapes(self):
+        b, n, r = self.batch, self.n, self.nrhs
+        f64, i32 = torch.float64, torch.int32
+        return [((b, n, self.lda), f64), ((b, r, self.ldb), f64), ((b, r, n), f64), ((b,), i32), ((b,), i32)]
 
     def __call__(self, hA: torch.Tensor, hB: torch.Tensor, hX: torch.Tensor, hIter: torch.Tensor,
                  hInfo: torch.Tensor) -> None:
         """hA (batch, n, lda) and hB (batch, nrhs, ldb) in, hX (batch, nrhs, n), hIter and
         hInfo (batch, int32) out; all pinned host tensors."""
-        L = self.q.lib
-
-        def solve(c0, c1):
-            _check(L.magma_dsgesv_batched(self.n, self.nrhs, _vp(self.pA[c0:]), self.lda, _vp(self.pP[c0:]),
-                                          _vp(self.pB[c0:]), self.ldb, _vp(self.pX[c0:]), self.n,
-                                          _vp(self.iter[c0:]), _vp(self.info[c0:]), c1 - c0, self.q.handle),
-                   "magma_dsgesv_batched")
-
-        self._run(hA, hB, [(hX, self.X), (hIter, self.iter), (hInfo, self.info)], solve)
+        self._run(hA, hB, hX, hIter, hInfo)
 
 
 class HostDgesv(_HostPipeline):
     """magma_dgesv_batched (FP64 LU with partial pivoting + solve) on systems in pinned host
     memory, uploads and read-backs overlapped with the solves chunk by chunk."""
 
+    _kind = 1   # MAGMA_B200_HOST_DGESV
+
     def __init__(self, batch: int, n: int, nrhs: int, chunks: int = 4, queue: Queue | None = None,
                  lda: int | None = None, ldb: int | None = None):
         super().__init__(batch, n, nrhs, chunks, queue, lda, ldb)
+
+    def _shapes(self):
+        b, n, r = self.batch, self.n, self.nrhs
+        f64, i32 = torch.float64, torch.int32
+        return [((b, n, self.lda), f64), ((b, r, self.ldb), f64), ((b, r, self.ldb), f64), ((b, n), i32), ((b,), i32)]
 
     def __call__(self, hA: torch.Tensor, hB: torch.Tensor, hX: torch.Tensor, hIpiv: torch.Tensor,
                  hInfo: torch.Tensor) -> None:
         """hA (batch, n, lda) and hB (batch, nrhs, ldb) in; hX (batch, nrhs, ldb) = the
         solutions, hIpiv (batch, n) and hInfo (batch,) int32 out; all pinned host tensors."""
-        L = self.q.lib
-
-        def solve(c0, c1):
-            _check(L.magma_dgesv_batched(self.n, self.nrhs, _vp(self.pA[c0:]), self.lda, _vp(self.pP[c0:]),
-                                         _vp(self.pB[c0:]), self.ldb, _vp(self.info[c0:]), c1 - c0, self.q.handle),
-                   "magma_dgesv_batched")
-
-        self._run(hA, hB, [(hX, self.B), (hIpiv, self.ipiv), (hInfo, self.info)], solve)
+        self._run(hA, hB, hX, hIpiv, hInfo)
 
 
 # ------------------------------------------------------------------------------- GEMM

@@ -110,6 +110,29 @@ magma_int_t magma_free_internal(magma_ptr ptr, const char* func, const char* fil
     return MAGMA_SUCCESS;
 }
 
+// interface_cuda/alloc.cpp:242 -- page-locked host memory (portable across contexts);
+// zero-byte requests allocate a minimal block, as the reference.
+magma_int_t magma_malloc_pinned(void** ptr_ptr, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (cudaHostAlloc(ptr_ptr, bytes, cudaHostAllocPortable) != cudaSuccess) {
+        cudaGetLastError();
+        *ptr_ptr = nullptr;
+        return MAGMA_ERR_HOST_ALLOC;
+    }
+    return MAGMA_SUCCESS;
+}
+
+// interface_cuda/alloc.cpp:276
+magma_int_t magma_free_pinned_internal(void* ptr, const char* func, const char* file, int line) {
+    cudaError_t e = cudaFreeHost(ptr);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        std::fprintf(stderr, "magma_free_pinned: %s at %s:%d in %s\n", cudaGetErrorString(e), file, line, func);
+        return MAGMA_ERR_INVALID_PTR;
+    }
+    return MAGMA_SUCCESS;
+}
+
 // interface_cuda/interface.cpp:690 -- a queue with its own (non-blocking) stream.
 void magma_queue_create_internal(magma_device_t device, magma_queue_t* queue_ptr,
                                  const char*, const char*, int) {
