@@ -29,11 +29,13 @@ magma_int_t chol_var(bool upper, const int* n, const int* nrhs, T** A, const int
                      int* info, int batch, int max_n, int max_nrhs, bool factor, bool solve, magma_queue_t queue) {
     const int top = chol_bucket_of(max_n);
     if (top < 0) return MAGMA_ERR_NOT_SUPPORTED;
-    int* ws = static_cast<int*>(queue_workspace(queue, sizeof(int) * bucketize_ws_ints(batch, kCholBuckets)));
+    const size_t bw = bucketize_ws_ints(batch, kCholBuckets);
+    int* ws = static_cast<int*>(queue_workspace(queue, sizeof(int) * (bw + bucket_sort_ws_ints(batch, kCholBuckets))));
     if (!ws) return MAGMA_ERR_DEVICE_ALLOC;
     if (info) cudaMemsetAsync(info, 0, sizeof(int) * batch, queue->stream);   // n = 0 instances
     int *counts, *lists;
     magma_int_t rc = bucketize(n, batch, kCholEdges, kCholBuckets, queue->stream, ws, &counts, &lists);
+    if (!rc) rc = sort_buckets_desc(n, nullptr, batch, kCholEdges, kCholBuckets, queue->stream, counts, lists, ws + bw);
     if (rc) return rc;
     LuSizes sz{0, 0, 0, 0, 0, n, n, lda, ldb, nrhs};
     // buckets are independent: each runs on its own auxiliary stream

@@ -30,12 +30,16 @@ static magma_int_t lu_var(LuOp op, bool trans, const int* m, const int* n, const
                           magma_queue_t queue) {
     const int top = lu_bucket_of(max_mn);
     if (top < 0) return MAGMA_ERR_NOT_SUPPORTED;
-    int* ws = static_cast<int*>(queue_workspace(queue, sizeof(int) * bucketize_ws_ints(batch, kLuBuckets)));
+    const size_t bw = bucketize_ws_ints(batch, kLuBuckets);
+    int* ws = static_cast<int*>(queue_workspace(queue, sizeof(int) * (bw + bucket_sort_ws_ints(batch, kLuBuckets))));
     if (!ws) return MAGMA_ERR_DEVICE_ALLOC;
     if (info) cudaMemsetAsync(info, 0, sizeof(int) * batch, queue->stream);   // empty instances
     int *counts, *lists;
     magma_int_t rc = bucketize2(m, op == LuOp::Getrf ? n : nullptr, batch, kLuEdges, kLuBuckets, queue->stream, ws,
                                 &counts, &lists);
+    if (!rc)
+        rc = sort_buckets_desc(m, op == LuOp::Getrf ? n : nullptr, batch, kLuEdges, kLuBuckets, queue->stream, counts,
+                               lists, ws + bw);
     if (rc) return rc;
     const LuSizes sz{0, 0, 0, 0, 0, m, n, lda, ldb, nrhs};
     // buckets are independent: each runs on its own auxiliary stream

@@ -372,7 +372,8 @@ magma_int_t magma_b200_server_create(magma_int_t device, size_t budget_bytes, ma
         magma_queue_create_from_cuda_internal(device, s.stream, nullptr, nullptr, &s.queue, "server", __FILE__,
                                               __LINE__);
         // bucket lists of the vbatched calls: reserve once so batches never grow the workspace
-        magma_queue_reserve_workspace(s.queue, sizeof(int) * mb200::bucketize_ws_ints(max_batch, 16));
+        magma_queue_reserve_workspace(s.queue, sizeof(int) * (mb200::bucketize_ws_ints(max_batch, 16) +
+                                                              mb200::bucket_sort_ws_ints(max_batch, 16)));
         cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming);
         if (cudaHostAlloc(reinterpret_cast<void**>(&s.h_meta), 2 * sv->meta.bytes, cudaHostAllocDefault) !=
                 cudaSuccess ||

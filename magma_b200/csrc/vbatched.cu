@@ -86,6 +86,66 @@ magma_int_t bucketize2(const int* key, const int* key2, int batch, const int* ed
 
 size_t bucketize_ws_ints(int batch, int nb) { return (size_t)2 * nb + (size_t)nb * batch; }
 
+// One block per bucket: a counting sort of the bucket's list by key, descending.
+constexpr int kSortBins = 1024;
+__global__ void __launch_bounds__(1024)
+bucket_sort_kernel(const int* __restrict__ key, const int* __restrict__ key2, int batch, BucketEdges edges,
+                   const int* __restrict__ counts, int* __restrict__ lists, int* __restrict__ tmp) {
+    __shared__ int hist[kSortBins];
+    __shared__ int warp_sum[32];
+    const int b = blockIdx.x, cnt = counts[b];
+    if (cnt <= 1) return;
+    const int lo = (b == 0) ? 1 : edges.e[b - 1] + 1;
+    int* list = lists + (size_t)b * batch;
+    int* out = tmp + (size_t)b * batch;
+    for (int i = threadIdx.x; i < kSortBins; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    auto bin_of = [&](int id) {
+        const int v = key2 ? max(key[id], key2[id]) : key[id];
+        return kSortBins - 1 - min(max(v - lo, 0), kSortBins - 1);   // largest keys first
+    };
+    for (int i = threadIdx.x; i < cnt; i += blockDim.x) atomicAdd(&hist[bin_of(list[i])], 1);
+    __syncthreads();
+    // exclusive scan of the 1024 bins: one bin per thread, warp scans, then the warp totals
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    int v = hist[t], x = v;
+    for (int off = 1; off < 32; off <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, off);
+        if (lane >= off) x += y;
+    }
+    if (lane == 31) warp_sum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int s = warp_sum[lane];
+        for (int off = 1; off < 32; off <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, s, off);
+            if (lane >= off) s += y;
+        }
+        warp_sum[lane] = s;   // inclusive
+    }
+    __syncthreads();
+    hist[t] = x - v + (w > 0 ? warp_sum[w - 1] : 0);   // exclusive start of bin t
+    __syncthreads();
+    for (int i = t; i < cnt; i += blockDim.x) {
+        const int id = list[i];
+        out[atomicAdd(&hist[bin_of(id)], 1)] = id;
+    }
+    __syncthreads();
+    for (int i = t; i < cnt; i += blockDim.x) list[i] = out[i];
+}
+
+size_t bucket_sort_ws_ints(int batch, int nb) { return (size_t)nb * batch; }
+
+magma_int_t sort_buckets_desc(const int* key, const int* key2, int batch, const int* edges_host, int nb,
+                              cudaStream_t s, const int* counts, int* lists, int* tmp) {
+    if (nb > BucketEdges::kMax) return MAGMA_ERR_NOT_SUPPORTED;
+    BucketEdges edges;
+    edges.n = nb;
+    for (int b = 0; b < nb; ++b) edges.e[b] = edges_host[b];
+    bucket_sort_kernel<<<nb, kSortBins, 0, s>>>(key, key2, batch, edges, counts, lists, tmp);
+    return launch_status();
+}
+
 // Device reduction of up to three size arrays, copied back to the host
 // (the reference does the same with magma_imax_size_* + getvector + sync).
 magma_int_t reduce_sizes(const int* a, const int* b, const int* c, int batch, magma_queue_t queue, int out[6]) {

@@ -23,6 +23,15 @@ size_t bucketize_ws_ints(int batch, int nb);
 magma_int_t bucketize2(const int* key, const int* key2, int batch, const int* edges_host, int nb, cudaStream_t s,
                        int* ws, int** counts_out, int** lists_out);
 
+// Reorders every bucket's list (as bucketize / bucketize2 left it) by key descending,
+// so that the kernels' blocks, walking a list round-robin, start on the costliest
+// instances and finish together (largest-first). tmp must hold
+// bucket_sort_ws_ints(batch, nb) ints. Keys above a bucket's lower edge + 1023 share
+// the first place. The instances themselves are unchanged: each is processed alone.
+magma_int_t sort_buckets_desc(const int* key, const int* key2, int batch, const int* edges_host, int nb,
+                              cudaStream_t s, const int* counts, int* lists, int* tmp);
+size_t bucket_sort_ws_ints(int batch, int nb);
+
 // out[0..2] = max of a, b, c (null arrays give 0), out[3..5] = their minima. Synchronises the queue.
 magma_int_t reduce_sizes(const int* a, const int* b, const int* c, int batch, magma_queue_t queue, int out[6]);
 // *out = min over i of ld[i] - rows[i]. Synchronises the queue.
