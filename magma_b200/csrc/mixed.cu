@@ -253,9 +253,12 @@ static void launch_refine(int n, int nrhs, double** A, int lda, int** ipiv, doub
 bool dsgesv_supported(int n) { return n <= 512; }
 
 // The tensor-core LU serves n = 96..256 in steps of 32 (smaller orders use the
-// register kernels) unless the tuning table turns it off (it starts from
-// MAGMA_B200_TENSOR_CORE_LU=0 in the environment, or magma_b200_autotune measures).
-static bool use_tensor_core_lu(int n) { return tuning().mixed_tc_lu && n > 64 && lu_tc_supported(n); }
+// register kernels) unless the tuning table turns it off, as a whole (it starts from
+// MAGMA_B200_TENSOR_CORE_LU=0 in the environment) or per order (magma_b200_autotune
+// measures both paths at each order).
+static bool use_tensor_core_lu(int n) {
+    return tuning().mixed_tc_lu && n > 64 && lu_tc_supported(n) && tuning().mixed_tc_n[(n - 96) / 32];
+}
 
 magma_int_t dsgesv_batched(int n, int nrhs, double** dA, int lda, int** ipiv, double** dB, int ldb, double** dX,
                            int ldx, int* iter, int* info, int batch, magma_queue_t queue) {

@@ -35,6 +35,7 @@ static void set_defaults(TuningTable& t) {
     // m = 512 (n = 256: 4.58 against 4.74 ms), DMMA at m = 1,024 (23.4 against 23.9 ms)
     const int dmma[kLuBlockedBuckets] = {0, 0, 0, 1};
     for (int b = 0; b < kLuBlockedBuckets; ++b) t.lu_dmma[b] = dmma[b];
+    for (int i = 0; i < kMixedTcOrders; ++i) t.mixed_tc_n[i] = 1;
 }
 
 static void to_values(const TuningTable& t, int* v) {
@@ -43,12 +44,13 @@ static void to_values(const TuningTable& t, int* v) {
         for (int b = 0; b < kGemmBuckets; ++b) v[i++] = t.gemm_variant[p][b];
     v[i++] = t.mixed_tc_lu;
     for (int b = 0; b < kLuBlockedBuckets; ++b) v[i++] = t.lu_dmma[b];
+    for (int k = 0; k < kMixedTcOrders; ++k) v[i++] = t.mixed_tc_n[k];
 }
 
-// count kTuningValues, or kTuningValuesV1 (a table saved before the LU entries
-// existed: those keep their current values).
+// count kTuningValues, or kTuningValuesV1 / V2 (tables saved before the later
+// entries existed: those keep their current values).
 static bool from_values(const int* v, int count, TuningTable& t) {
-    if (count != kTuningValues && count != kTuningValuesV1) return false;
+    if (count != kTuningValues && count != kTuningValuesV1 && count != kTuningValuesV2) return false;
     for (int i = 0; i < 2 * kGemmBuckets; ++i)
         if (v[i] < 0 || v[i] > (i < kGemmBuckets ? 3 : 2)) return false;   // 3: FP64 tensor-core tile
     for (int i = 2 * kGemmBuckets; i < count; ++i)
@@ -57,8 +59,10 @@ static bool from_values(const int* v, int count, TuningTable& t) {
     for (int p = 0; p < 2; ++p)
         for (int b = 0; b < kGemmBuckets; ++b) t.gemm_variant[p][b] = v[i++];
     t.mixed_tc_lu = v[i++];
-    if (count == kTuningValues)
+    if (count >= kTuningValuesV2)
         for (int b = 0; b < kLuBlockedBuckets; ++b) t.lu_dmma[b] = v[i++];
+    if (count >= kTuningValues)
+        for (int k = 0; k < kMixedTcOrders; ++k) t.mixed_tc_n[k] = v[i++];
     return true;
 }
 
@@ -68,7 +72,8 @@ static bool load_file(const char* path, TuningTable& t) {
     char magic[64] = {0};
     int v[kTuningValues];
     bool ok = std::fscanf(f, "%63s", magic) == 1;
-    const int count = !ok ? 0 : std::strcmp(magic, "magma_b200_tuning_v2") == 0 ? kTuningValues
+    const int count = !ok ? 0 : std::strcmp(magic, "magma_b200_tuning_v3") == 0 ? kTuningValues
+                             : std::strcmp(magic, "magma_b200_tuning_v2") == 0 ? kTuningValuesV2
                              : std::strcmp(magic, "magma_b200_tuning_v1") == 0 ? kTuningValuesV1 : 0;
     ok = ok && count > 0;
     for (int i = 0; ok && i < count; ++i) ok = std::fscanf(f, "%d", &v[i]) == 1;
@@ -210,43 +215,51 @@ static magma_int_t tune_gemm(int prec, magma_queue_t q, unsigned seed) {
     return MAGMA_SUCCESS;
 }
 
-// Mixed solve: tensor-core against CUDA-core FP32 LU on 512 diagonally dominant
-// 256 x 256 systems, 4 right-hand sides.
+// Mixed solve, per order n = 96..256 (step 32): the tensor-core LU with its fused
+// refinement against the CUDA-core FP32 LU with the separate refinement kernel, on
+// about 128 MB of diagonally dominant systems with 4 right-hand sides each.
 static magma_int_t tune_mixed(magma_queue_t q, unsigned seed) {
-    const int n = 256, batch = 512, nrhs = 4;
-    DevBuf dA, dA0, dB, dX, dP, dIp, dI;
-    const size_t an = (size_t)n * n * batch;
-    if (!dA.alloc(8 * an) || !dA0.alloc(8 * an) || !dB.alloc(8 * (size_t)n * nrhs * batch) ||
-        !dX.alloc(8 * (size_t)n * nrhs * batch) || !dP.alloc(sizeof(void*) * 4 * batch) ||
-        !dIp.alloc(sizeof(int) * (size_t)n * batch) || !dI.alloc(sizeof(int) * 2 * batch))
-        return MAGMA_ERR_DEVICE_ALLOC;
-    tune_fill_kernel<double><<<1024, 256, 0, q->stream>>>((double*)dA0.p, an, seed + 11);
-    tune_shift_diag_kernel<<<256, 256, 0, q->stream>>>((double*)dA0.p, n, batch, 2.0 * n);
-    tune_fill_kernel<double><<<1024, 256, 0, q->stream>>>((double*)dB.p, (size_t)n * nrhs * batch, seed + 12);
-    std::vector<void*> ptr(4 * batch);
-    for (int i = 0; i < batch; ++i) {
-        ptr[i] = (double*)dA.p + (size_t)i * n * n;
-        ptr[batch + i] = (double*)dB.p + (size_t)i * n * nrhs;
-        ptr[2 * batch + i] = (double*)dX.p + (size_t)i * n * nrhs;
-        ptr[3 * batch + i] = (int*)dIp.p + (size_t)i * n;
+    const int nrhs = 4;
+    for (int o = 0; o < kMixedTcOrders; ++o) {
+        const int n = 96 + 32 * o;
+        const int batch = std::max(64, (128 << 20) / (8 * n * n));
+        DevBuf dA, dA0, dB, dX, dP, dIp, dI;
+        const size_t an = (size_t)n * n * batch;
+        if (!dA.alloc(8 * an) || !dA0.alloc(8 * an) || !dB.alloc(8 * (size_t)n * nrhs * batch) ||
+            !dX.alloc(8 * (size_t)n * nrhs * batch) || !dP.alloc(sizeof(void*) * 4 * batch) ||
+            !dIp.alloc(sizeof(int) * (size_t)n * batch) || !dI.alloc(sizeof(int) * 2 * batch))
+            return MAGMA_ERR_DEVICE_ALLOC;
+        tune_fill_kernel<double><<<1024, 256, 0, q->stream>>>((double*)dA0.p, an, seed + 11 + o);
+        tune_shift_diag_kernel<<<256, 256, 0, q->stream>>>((double*)dA0.p, n, batch, 2.0 * n);
+        tune_fill_kernel<double><<<1024, 256, 0, q->stream>>>((double*)dB.p, (size_t)n * nrhs * batch, seed + 12 + o);
+        std::vector<void*> ptr(4 * batch);
+        for (int i = 0; i < batch; ++i) {
+            ptr[i] = (double*)dA.p + (size_t)i * n * n;
+            ptr[batch + i] = (double*)dB.p + (size_t)i * n * nrhs;
+            ptr[2 * batch + i] = (double*)dX.p + (size_t)i * n * nrhs;
+            ptr[3 * batch + i] = (int*)dIp.p + (size_t)i * n;
+        }
+        cudaMemcpyAsync(dP.p, ptr.data(), sizeof(void*) * 4 * batch, cudaMemcpyHostToDevice, q->stream);
+        cudaStreamSynchronize(q->stream);
+        void** p = (void**)dP.p;
+        int* it = (int*)dI.p;
+        float best = 1e30f;
+        int best_v = tuning().mixed_tc_n[o];
+        const int master = tuning().mixed_tc_lu;
+        tuning_mut().mixed_tc_lu = 1;
+        for (int v = 0; v < 2; ++v) {
+            tuning_mut().mixed_tc_n[o] = v;
+            const float ms = time_ms(q->stream, [&] {
+                cudaMemcpyAsync(dA.p, dA0.p, 8 * an, cudaMemcpyDeviceToDevice, q->stream);
+                magma_dsgesv_batched(n, nrhs, (double**)p, n, (int**)(p + 3 * batch), (double**)(p + batch), n,
+                                     (double**)(p + 2 * batch), n, it, it + batch, batch, q);
+            }, 3);
+            if (cudaGetLastError() != cudaSuccess) return MAGMA_ERR_UNKNOWN;
+            if (ms < best) { best = ms; best_v = v; }
+        }
+        tuning_mut().mixed_tc_lu = master;
+        tuning_mut().mixed_tc_n[o] = best_v;
     }
-    cudaMemcpyAsync(dP.p, ptr.data(), sizeof(void*) * 4 * batch, cudaMemcpyHostToDevice, q->stream);
-    cudaStreamSynchronize(q->stream);
-    void** p = (void**)dP.p;
-    int* it = (int*)dI.p;
-    float best = 1e30f;
-    int best_v = tuning().mixed_tc_lu;
-    for (int v = 0; v < 2; ++v) {
-        tuning_mut().mixed_tc_lu = v;
-        const float ms = time_ms(q->stream, [&] {
-            cudaMemcpyAsync(dA.p, dA0.p, 8 * an, cudaMemcpyDeviceToDevice, q->stream);
-            magma_dsgesv_batched(n, nrhs, (double**)p, n, (int**)(p + 3 * batch), (double**)(p + batch), n,
-                                 (double**)(p + 2 * batch), n, it, it + batch, batch, q);
-        }, 3);
-        if (cudaGetLastError() != cudaSuccess) return MAGMA_ERR_UNKNOWN;
-        if (ms < best) { best = ms; best_v = v; }
-    }
-    tuning_mut().mixed_tc_lu = best_v;
     return MAGMA_SUCCESS;
 }
 
@@ -325,7 +338,7 @@ magma_int_t magma_b200_tuning_save(const char* path) {
     if (!f) return MAGMA_ERR_UNKNOWN;
     int v[kTuningValues];
     to_values(tuning(), v);
-    std::fprintf(f, "magma_b200_tuning_v2\n");
+    std::fprintf(f, "magma_b200_tuning_v3\n");
     for (int i = 0; i < kTuningValues; ++i) std::fprintf(f, "%d%c", v[i], i + 1 < kTuningValues ? ' ' : '\n');
     return std::fclose(f) == 0 ? MAGMA_SUCCESS : MAGMA_ERR_UNKNOWN;
 }

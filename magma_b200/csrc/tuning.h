@@ -10,17 +10,21 @@ namespace mb200 {
 constexpr int kGemmBuckets = 4;   // max(M, N) <= 16, <= 32, <= 64, larger
 
 constexpr int kLuBlockedBuckets = 4;   // blocked LU by max(m): <= 128, <= 256, <= 512, <= 1024
+constexpr int kMixedTcOrders = 6;      // the tensor-core LU's orders: n = 96, 128, ..., 256
 
 struct TuningTable {
     int gemm_variant[2][kGemmBuckets];   // [FP64, FP32][bucket]: tile variant (0: 64x64, 1: 32x32, 2: 16x16,
                                          // 3: FP64 only, 64x64 on the tensor cores)
-    int mixed_tc_lu;                     // 1: tensor-core LU in the mixed solve for n = 96..256, step 32
+    int mixed_tc_lu;                     // 1: tensor-core LU in the mixed solve (where mixed_tc_n allows it)
     int lu_dmma[kLuBlockedBuckets];      // 1: FP64 blocked LU trailing update on the tensor cores (DMMA)
+    int mixed_tc_n[kMixedTcOrders];      // per order n = 96 + 32 i: 1 tensor-core LU (+ fused refinement),
+                                         // 0 CUDA-core FP32 LU + separate refinement
 };
 
 const TuningTable& tuning();   // defaults, or the file named by MAGMA_B200_TUNING, or the last autotune/set
 TuningTable& tuning_mut();
 constexpr int kTuningValuesV1 = 2 * kGemmBuckets + 1;
-constexpr int kTuningValues = kTuningValuesV1 + kLuBlockedBuckets;
+constexpr int kTuningValuesV2 = kTuningValuesV1 + kLuBlockedBuckets;
+constexpr int kTuningValues = kTuningValuesV2 + kMixedTcOrders;
 
 }  // namespace mb200

@@ -10,7 +10,7 @@ import pytest
 
 from magma_b200 import _lib
 
-N_VALUES = 13
+N_VALUES = 19
 
 
 def _get(lib):
@@ -29,11 +29,11 @@ def test_tuning_roundtrip(tmp_path):
     assert lib.magma_b200_tuning_get(None, 0) == N_VALUES           # size query
     orig = _get(lib)
     try:
-        new = [0, 1, 2, 0, 2, 1, 0, 0, 0, 1, 0, 1, 1]
+        new = [0, 1, 2, 0, 2, 1, 0, 0, 0, 1, 0, 1, 1, 1, 0, 1, 1, 0, 1]
         assert _set(lib, new) == 0 and _get(lib) == new
         f = tmp_path / "tune.txt"
         assert lib.magma_b200_tuning_save(str(f).encode()) == 0
-        assert f.read_text().split()[0] == "magma_b200_tuning_v2"
+        assert f.read_text().split()[0] == "magma_b200_tuning_v3"
         assert _set(lib, orig) == 0 and _get(lib) == orig
         assert lib.magma_b200_tuning_load(str(f).encode()) == 0 and _get(lib) == new
         # rejected: wrong count, out-of-range values, unreadable or malformed files
@@ -43,11 +43,15 @@ def test_tuning_roundtrip(tmp_path):
         assert _set(lib, [3] + new[1:]) == 0 and _get(lib)[0] == 3
         assert _set(lib, new) == 0
         assert _set(lib, new[:-1] + [2]) == _lib.MAGMA_ERR_ILLEGAL_VALUE
-        # a 9-value table (saved before the LU update entries) sets the first 9 only
+        # 9- and 13-value tables (saved before the later entries existed) set their part only
         assert _set(lib, orig[:9]) == 0 and _get(lib) == orig[:9] + new[9:]
+        assert _set(lib, orig[:13]) == 0 and _get(lib) == orig[:13] + new[13:]
         v1 = tmp_path / "v1.txt"
         v1.write_text("magma_b200_tuning_v1\n" + " ".join(map(str, new[:9])) + "\n")
-        assert lib.magma_b200_tuning_load(str(v1).encode()) == 0 and _get(lib) == new
+        assert lib.magma_b200_tuning_load(str(v1).encode()) == 0 and _get(lib) == new[:9] + orig[9:13] + new[13:]
+        v2 = tmp_path / "v2.txt"
+        v2.write_text("magma_b200_tuning_v2\n" + " ".join(map(str, new[:13])) + "\n")
+        assert lib.magma_b200_tuning_load(str(v2).encode()) == 0 and _get(lib) == new
         assert _set(lib, new) == 0
         assert lib.magma_b200_tuning_load(str(tmp_path / "missing").encode()) == _lib.MAGMA_ERR_ILLEGAL_VALUE
         bad = tmp_path / "bad.txt"
@@ -134,7 +138,7 @@ def test_lu_update_variants_bit_identical(cuda, n):
     res = {}
     try:
         for v in (0, 1):
-            assert _set(lib, orig[:9] + [v] * 4) == 0
+            assert _set(lib, orig[:9] + [v] * 4 + orig[13:]) == 0
             A = torch.from_numpy(A_np).to(cuda)
             ipiv, info = mb.dgetrf_batched(A)
             torch.cuda.synchronize()
@@ -147,3 +151,28 @@ def test_lu_update_variants_bit_identical(cuda, n):
     oip, oinf = oracle.dgetrf_batched(O, n)
     assert np.array_equal(res[1][0][:3], O) and np.array_equal(res[1][1][:3], oip)
     assert np.array_equal(res[1][2][:3], oinf) and oinf[0] == 8
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [96, 160, 256])
+def test_mixed_paths_per_order(cuda, n):
+    """The tuning table's per-order switch between the tensor-core LU with its fused
+    refinement and the CUDA-core FP32 LU with the separate refinement kernel: both meet
+    the backward-error bound on the same systems."""
+    import torch
+
+    import magma_b200 as mb
+    from magma_b200 import testing as T
+    lib = _lib.load()
+    orig = _get(lib)
+    A_np, B_np, _ = T.svd_logrand(24, n, 1e2, 1e6, nrhs=4, seed=900 + n)
+    try:
+        for v in (0, 1):
+            vals = list(orig)
+            vals[13 + (n - 96) // 32] = v
+            assert _set(lib, vals) == 0
+            X, ipiv, it, info = mb.dsgesv_batched(torch.from_numpy(A_np).to(cuda), torch.from_numpy(B_np).to(cuda))
+            assert T.backward_error(A_np, X.cpu().numpy(), B_np, n).max() <= 1e-14
+            assert (it.cpu().numpy() >= 0).mean() >= 0.9 and not info.cpu().numpy().any()
+    finally:
+        _set(lib, orig)
