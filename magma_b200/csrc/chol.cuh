@@ -16,6 +16,7 @@
 // loop over cuBLAS dsyrk on 32 streams).
 #pragma once
 
+#include "lu_sizes.h"
 #include "small_lu.cuh"
 #include <type_traits>
 
@@ -39,9 +40,9 @@ struct CholShared {
 // from its first column on and looped over its CK steps at run time (the chunk's
 // own columns picked by selects), which keeps the kernel small enough for the
 // instruction cache; each element sees the same operations in the same order.
-template <typename T, int NC, int NW>
+template <typename T, int NC, int NW, typename Sync = MatSync<NW>>
 __device__ __forceinline__ int chol_panel_steps(T (&a)[NC], int n, int nsteps, int k0, int tid,
-                                                CholShared<T, NC>& sh) {
+                                                CholShared<T, NC>& sh, const Sync& sync = Sync{}) {
     constexpr int CK = NC < 8 ? NC : 8;
     static_assert(NC % CK == 0, "chunking");
     int info = 0;
@@ -57,7 +58,7 @@ __device__ __forceinline__ int chol_panel_steps(T (&a)[NC], int n, int nsteps, i
 #pragma unroll
             for (int q = 1; q < CK; ++q) ak = (k == c0 + q) ? a[c0 + q] : ak;
             if (tid >= g && tid < n && tid < k0 + NC) sh.col[buf][tid - k0] = ak;
-            mat_sync<NW>();
+            sync();
             const T d = sh.col[buf][k];
             if (!(d > T(0))) {      // not positive definite (or NaN): stop, A(g,g) keeps d
                 info = g + 1;
@@ -85,9 +86,9 @@ __device__ __forceinline__ int chol_panel_steps(T (&a)[NC], int n, int nsteps, i
 
 // The same steps fully unrolled: the blocked factorisation's 32-column panel, whose
 // code is small enough for the instruction cache and which spilled when chunked.
-template <typename T, int NC, int NW>
+template <typename T, int NC, int NW, typename Sync = MatSync<NW>>
 __device__ __forceinline__ int chol_panel_steps_unrolled(T (&a)[NC], int n, int nsteps, int k0, int tid,
-                                                         CholShared<T, NC>& sh) {
+                                                         CholShared<T, NC>& sh, const Sync& sync = Sync{}) {
     int info = 0;
     static_for<0, NC>([&](auto kc) {
         constexpr int k = decltype(kc)::value;
@@ -95,7 +96,7 @@ __device__ __forceinline__ int chol_panel_steps_unrolled(T (&a)[NC], int n, int 
         constexpr int buf = k & 1;
         const int g = k0 + k;
         if (tid >= g && tid < n && tid < k0 + NC) sh.col[buf][tid - k0] = a[k];
-        mat_sync<NW>();
+        sync();
         const T d = sh.col[buf][k];
         if (!(d > T(0))) {
             info = g + 1;
@@ -121,8 +122,9 @@ __device__ __forceinline__ int chol_panel_steps_unrolled(T (&a)[NC], int n, int 
 // The diagonal enters as its correctly rounded reciprocal, formed by each thread for its
 // own row before the sweeps, so no division sits on the step-to-step chain (an IEEE
 // division is ~127 cycles of it on B200); the oracle's dpotrs is restated the same way.
-template <typename T, int NC, int NW, int R>
-__device__ __forceinline__ void chol_solve(const T (&a)[NC], int n, int tid, T (&b)[R], CholShared<T, NC>& sh) {
+template <typename T, int NC, int NW, int R, typename Sync = MatSync<NW>>
+__device__ __forceinline__ void chol_solve(const T (&a)[NC], int n, int tid, T (&b)[R], CholShared<T, NC>& sh,
+                                           const Sync& sync = Sync{}) {
     static_assert(R <= 8, "CholShared::rhs holds 8 right-hand sides a group");
     constexpr int CK = NC < 8 ? NC : 8;
     T dk = T(1);
@@ -148,7 +150,7 @@ __device__ __forceinline__ void chol_solve(const T (&a)[NC], int n, int tid, T (
 #pragma unroll
                 for (int r = 0; r < R; ++r) { b[r] = b[r] * rk; sh.rhs[buf][r] = b[r]; }
             }
-            mat_sync<NW>();
+            sync();
             if (tid > k && tid < n) {
 #pragma unroll
                 for (int r = 0; r < R; ++r) b[r] = fma_rn(-sh.rhs[buf][r], ak, b[r]);
@@ -171,7 +173,7 @@ __device__ __forceinline__ void chol_solve(const T (&a)[NC], int n, int tid, T (
                 for (int j = c0; j < c0 + CK; ++j)
                     if (j < k) sh.row[buf][j] = a[j];
             }
-            mat_sync<NW>();
+            sync();
             if (tid < k) {
                 const T lki = sh.row[buf][tid];
 #pragma unroll
@@ -185,6 +187,72 @@ __device__ __forceinline__ void chol_solve(const T (&a)[NC], int n, int tid, T (
 template <typename T>
 __device__ __forceinline__ T& tri(T* A, int lda, bool upper, int i, int j) {
     return upper ? A[j + (size_t)i * lda] : A[i + (size_t)j * lda];
+}
+
+// One instance of the register-resident kernels: potrf (thread = row, n <= NC) and,
+// when SOLVE, potrs on its right-hand sides R at a time. n <= 0 writes info 0 only.
+template <typename T, int NC, int NW, int R, bool SOLVE, typename Sync = MatSync<NW>>
+__device__ __forceinline__ void chol_small_instance(int id, const LuSizes& sz, bool upper, T** dA_array,
+                                                    T** dB_array, int* info_array, int tid, CholShared<T, NC>& sh,
+                                                    const Sync& sync = Sync{}) {
+    const int n = sz.get_n(id), lda = sz.get_lda(id);
+    if (n <= 0) {
+        if (tid == 0 && info_array) info_array[id] = 0;
+        return;
+    }
+    T* A = dA_array[id];
+    T a[NC];
+#pragma unroll
+    for (int j = 0; j < NC; ++j) a[j] = (tid < n && j <= tid) ? tri(A, lda, upper, tid, j) : T(0);
+    const int info = chol_panel_steps<T, NC, NW>(a, n, n, 0, tid, sh, sync);
+    if (tid < n) {
+        // on failure the rows stay as the steps left them, like LAPACK's partial factor
+#pragma unroll
+        for (int j = 0; j < NC; ++j)
+            if (j <= tid) tri(A, lda, upper, tid, j) = a[j];
+    }
+    if (tid == 0 && info_array) info_array[id] = info;
+    if constexpr (SOLVE) {
+        // MAGMA's posv solves regardless of info (src/zposv_batched.cpp:123-141)
+        T* B = dB_array[id];
+        const int nrhs = sz.get_nrhs(id), ldb = sz.get_ldb(id);
+        for (int c0 = 0; c0 < nrhs; c0 += R) {
+            T b[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) b[r] = (tid < n && c0 + r < nrhs) ? B[tid + (size_t)(c0 + r) * ldb] : T(0);
+            chol_solve<T, NC, NW, R>(a, n, tid, b, sh, sync);
+            if (tid < n) {
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    if (c0 + r < nrhs) B[tid + (size_t)(c0 + r) * ldb] = b[r];
+            }
+        }
+    }
+}
+
+// One instance of potrs alone with the factor's rows in registers.
+template <typename T, int NC, int NW, int R, typename Sync = MatSync<NW>>
+__device__ __forceinline__ void potrs_small_instance(int id, const LuSizes& sz, bool upper, T** dA_array,
+                                                     T** dB_array, int tid, CholShared<T, NC>& sh,
+                                                     const Sync& sync = Sync{}) {
+    const int n = sz.get_n(id), lda = sz.get_lda(id), nrhs = sz.get_nrhs(id), ldb = sz.get_ldb(id);
+    if (n <= 0 || nrhs <= 0) return;
+    T* A = dA_array[id];
+    T* B = dB_array[id];
+    T a[NC];
+#pragma unroll
+    for (int j = 0; j < NC; ++j) a[j] = (tid < n && j <= tid) ? tri(A, lda, upper, tid, j) : T(0);
+    for (int c0 = 0; c0 < nrhs; c0 += R) {
+        T b[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) b[r] = (tid < n && c0 + r < nrhs) ? B[tid + (size_t)(c0 + r) * ldb] : T(0);
+        chol_solve<T, NC, NW, R>(a, n, tid, b, sh, sync);
+        if (tid < n) {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                if (c0 + r < nrhs) B[tid + (size_t)(c0 + r) * ldb] = b[r];
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -201,12 +269,14 @@ struct BlockedCholShared {
     T P[NT][NB + 1];     // panel entries of every row
 };
 
-template <typename T, int NB, int NT, int CW, int CB>
-__device__ int blocked_potrf(T* __restrict__ A, int n, int lda, bool upper, BlockedCholShared<T, NB, NT, CW>& sh) {
+template <typename T, int NB, int NT, int CW, int CB, typename Team = BlockTeam>
+__device__ int blocked_potrf(T* __restrict__ A, int n, int lda, bool upper, BlockedCholShared<T, NB, NT, CW>& sh,
+                             const Team& team = Team{}) {
     constexpr int NW = NT / 32;
     // tile rows x columns; 2 rows when the block size leaves 64 registers a thread (FP64)
     constexpr int TR = (NT >= 1024 && sizeof(T) == 8) ? 2 : 4, TC = 8, G = 8 / TR;
-    const int tid = threadIdx.x;
+    const int tid = team.tid();
+    auto sync = [&] { team.sync(); };
     for (int k0 = 0; k0 < n; k0 += NB) {
         const int nbp = min(NB, n - k0);
         const bool live = (tid >= k0 && tid < n);
@@ -214,7 +284,7 @@ __device__ int blocked_potrf(T* __restrict__ A, int n, int lda, bool upper, Bloc
 #pragma unroll
         for (int c = 0; c < NB; ++c)
             a[c] = (live && c < nbp && k0 + c <= tid) ? tri(A, lda, upper, tid, k0 + c) : T(0);
-        const int info = chol_panel_steps_unrolled<T, NB, NW>(a, n, nbp, k0, tid, sh.p);
+        const int info = chol_panel_steps_unrolled<T, NB, NW>(a, n, nbp, k0, tid, sh.p, sync);
         if (live) {
 #pragma unroll
             for (int c = 0; c < NB; ++c)
@@ -223,7 +293,7 @@ __device__ int blocked_potrf(T* __restrict__ A, int n, int lda, bool upper, Bloc
             for (int c = 0; c < NB; ++c) sh.P[tid][c] = a[c];
         }
         if (info) return info;
-        __syncthreads();
+        team.sync();
         // trailing lower triangle: rows/columns m0..n-1, square 8x8 blocks (bj <= bi),
         // each split into G work items of TR rows
         const int m0 = k0 + nbp;
@@ -263,7 +333,7 @@ __device__ int blocked_potrf(T* __restrict__ A, int n, int lda, bool upper, Bloc
                     if (i < n && j <= i) tri(A, lda, upper, i, j) = acc[ii][jj];
                 }
         }
-        __syncthreads();   // trailing entries visible before the next panel loads them
+        team.sync();   // trailing entries visible before the next panel loads them
     }
     return 0;
 }
@@ -295,10 +365,10 @@ __device__ __forceinline__ void load_diag_block(BlockedCholRsShared<T, NT, R>& s
     __syncwarp();
 }
 
-template <typename T, int NT, int R>
+template <typename T, int NT, int R, typename Team = BlockTeam>
 __device__ void blocked_potrs(const T* __restrict__ A, int n, int lda, bool upper, T* __restrict__ B, int nrhs,
-                              int ldb, BlockedCholRsShared<T, NT, R>& sh) {
-    const int t = threadIdx.x, lane = t & 31;
+                              int ldb, BlockedCholRsShared<T, NT, R>& sh, const Team& team = Team{}) {
+    const int t = team.tid(), lane = t & 31;
     const int nblk = (n + 31) / 32;
     auto L = [&](int i, int j) -> T { return upper ? A[j + (size_t)i * lda] : A[i + (size_t)j * lda]; };
     for (int c0 = 0; c0 < nrhs; c0 += R) {
@@ -308,7 +378,7 @@ __device__ void blocked_potrs(const T* __restrict__ A, int n, int lda, bool uppe
         // forward: L y = b, blocks ascending
         for (int J = 0; J < nblk; ++J) {
             const int j0 = J * 32, j1 = min(n, j0 + 32), cnt = j1 - j0;
-            __syncthreads();
+            team.sync();
             if ((t >> 5) == J) {
                 load_diag_block(sh, cnt, lane, [&](int i, int j) { return L(j0 + i, j0 + j); });
                 // steps unrolled over the block (no loop or branch overhead on the chain)
@@ -327,14 +397,14 @@ __device__ void blocked_potrs(const T* __restrict__ A, int n, int lda, bool uppe
                     }
                 });
             }
-            __syncthreads();
+            team.sync();
             if (t >= j1 && t < n)
                 block_update<T, R, false>(b, sh.sb, cnt, [&](int q) { return L(t, j0 + q); });
         }
         // backward: L^T x = y, blocks descending (column sweep of U = L^T)
         for (int J = nblk - 1; J >= 0; --J) {
             const int j0 = J * 32, j1 = min(n, j0 + 32), cnt = j1 - j0;
-            __syncthreads();
+            team.sync();
             if ((t >> 5) == J) {
                 load_diag_block(sh, cnt, lane, [&](int i, int j) { return L(j0 + i, j0 + j); });
                 static_for<0, 32>([&](auto kc) {
@@ -352,7 +422,7 @@ __device__ void blocked_potrs(const T* __restrict__ A, int n, int lda, bool uppe
                     }
                 });
             }
-            __syncthreads();
+            team.sync();
             if (t < j0)
                 block_update<T, R, true>(b, sh.sb, cnt, [&](int q) { return L(j0 + q, t); });
         }
@@ -361,7 +431,7 @@ __device__ void blocked_potrs(const T* __restrict__ A, int n, int lda, bool uppe
             for (int r = 0; r < R; ++r)
                 if (c0 + r < nrhs) B[t + (size_t)(c0 + r) * ldb] = b[r];
         }
-        __syncthreads();
+        team.sync();
     }
 }
 

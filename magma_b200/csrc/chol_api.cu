@@ -5,6 +5,7 @@
 #include "internal.h"
 #include "chol_launch.h"
 #include "vbatched.h"
+#include "tuning.h"
 #include <algorithm>
 
 using namespace mb200;
@@ -38,6 +39,24 @@ magma_int_t chol_var(bool upper, const int* n, const int* nrhs, T** A, const int
     if (!rc) rc = sort_buckets_desc(n, nullptr, batch, kCholEdges, kCholBuckets, queue->stream, counts, lists, ws + bw);
     if (rc) return rc;
     LuSizes sz{0, 0, 0, 0, 0, n, n, lda, ldb, nrhs};
+    if (tuning().chol_queue) {
+        // orders <= 512: one persistent launch over all buckets, largest first; the
+        // 1024-thread bucket (512 < n <= 1024) beside it on an auxiliary stream
+        int* head = counts + kCholBuckets;
+        if (top < kCholBuckets - 1) {
+            chol_queue<T>(counts, lists, batch, top, head, sz, upper, A, B, info, factor, solve, max_nrhs,
+                          queue->stream);
+            return launch_status();
+        }
+        if ((rc = queue_fork(queue))) return rc;
+        const int b = kCholBuckets - 1;
+        WorkList wl{lists + (size_t)b * batch, counts + b, 0};
+        chol_bucket<T>(b, wl, batch, true, sz, upper, A, B, info, factor, solve, max_nrhs, queue_aux(queue, 0));
+        chol_queue<T>(counts, lists, batch, top, head, sz, upper, A, B, info, factor, solve, max_nrhs,
+                      queue_aux(queue, 1));
+        queue_join(queue);
+        return launch_status();
+    }
     // buckets are independent: each runs on its own auxiliary stream
     if ((rc = queue_fork(queue))) return rc;
     for (int b = top; b >= 0; --b) {

@@ -19,40 +19,8 @@ chol_small_kernel(WorkList wl, LuSizes sz, bool upper, T** dA_array, T** dB_arra
     const int local = (NW == 1) ? (threadIdx.x >> 5) : 0;
     const int tid = (NW == 1) ? (threadIdx.x & 31) : threadIdx.x;
     for (int w = blockIdx.x * MPB + local; w < wl.size(); w += gridDim.x * MPB) {
-        const int id = wl.at(w);
-        const int n = sz.get_n(id), lda = sz.get_lda(id);
-        if (n <= 0) {
-            if (tid == 0 && info_array) info_array[id] = 0;
-            continue;
-        }
-        T* A = dA_array[id];
-        T a[NC];
-#pragma unroll
-        for (int j = 0; j < NC; ++j) a[j] = (tid < n && j <= tid) ? tri(A, lda, upper, tid, j) : T(0);
-        const int info = chol_panel_steps<T, NC, NW>(a, n, n, 0, tid, shm[local]);
-        if (tid < n) {
-            // on failure the rows stay as the steps left them, like LAPACK's partial factor
-#pragma unroll
-            for (int j = 0; j < NC; ++j)
-                if (j <= tid) tri(A, lda, upper, tid, j) = a[j];
-        }
-        if (tid == 0 && info_array) info_array[id] = info;
-        if constexpr (SOLVE) {
-            // MAGMA's posv solves regardless of info (src/zposv_batched.cpp:123-141)
-            T* B = dB_array[id];
-            const int nrhs = sz.get_nrhs(id), ldb = sz.get_ldb(id);
-            for (int c0 = 0; c0 < nrhs; c0 += R) {
-                T b[R];
-#pragma unroll
-                for (int r = 0; r < R; ++r) b[r] = (tid < n && c0 + r < nrhs) ? B[tid + (size_t)(c0 + r) * ldb] : T(0);
-                chol_solve<T, NC, NW, R>(a, n, tid, b, shm[local]);
-                if (tid < n) {
-#pragma unroll
-                    for (int r = 0; r < R; ++r)
-                        if (c0 + r < nrhs) B[tid + (size_t)(c0 + r) * ldb] = b[r];
-                }
-            }
-        }
+        chol_small_instance<T, NC, NW, R, SOLVE>(wl.at(w), sz, upper, dA_array, dB_array, info_array, tid,
+                                                 shm[local]);
         mat_sync<NW>();
     }
 }
@@ -66,25 +34,7 @@ potrs_small_kernel(WorkList wl, LuSizes sz, bool upper, T** dA_array, T** dB_arr
     const int local = (NW == 1) ? (threadIdx.x >> 5) : 0;
     const int tid = (NW == 1) ? (threadIdx.x & 31) : threadIdx.x;
     for (int w = blockIdx.x * MPB + local; w < wl.size(); w += gridDim.x * MPB) {
-        const int id = wl.at(w);
-        const int n = sz.get_n(id), lda = sz.get_lda(id), nrhs = sz.get_nrhs(id), ldb = sz.get_ldb(id);
-        if (n <= 0 || nrhs <= 0) continue;
-        T* A = dA_array[id];
-        T* B = dB_array[id];
-        T a[NC];
-#pragma unroll
-        for (int j = 0; j < NC; ++j) a[j] = (tid < n && j <= tid) ? tri(A, lda, upper, tid, j) : T(0);
-        for (int c0 = 0; c0 < nrhs; c0 += R) {
-            T b[R];
-#pragma unroll
-            for (int r = 0; r < R; ++r) b[r] = (tid < n && c0 + r < nrhs) ? B[tid + (size_t)(c0 + r) * ldb] : T(0);
-            chol_solve<T, NC, NW, R>(a, n, tid, b, shm[local]);
-            if (tid < n) {
-#pragma unroll
-                for (int r = 0; r < R; ++r)
-                    if (c0 + r < nrhs) B[tid + (size_t)(c0 + r) * ldb] = b[r];
-            }
-        }
+        potrs_small_instance<T, NC, NW, R>(wl.at(w), sz, upper, dA_array, dB_array, tid, shm[local]);
         mat_sync<NW>();
     }
 }
@@ -138,8 +88,11 @@ static void launch_chol_small(const WorkList& wl, int bound, bool persistent, co
     } else if (max_nrhs <= 1) {
         auto k = chol_small_kernel<T, NC, NW, 1, true>;
         k<<<grid_for(k, threads, items, persistent), threads, 0, s>>>(wl, sz, upper, A, B, info);
-    } else {
+    } else if (max_nrhs <= 4) {
         auto k = chol_small_kernel<T, NC, NW, 4, true>;
+        k<<<grid_for(k, threads, items, persistent), threads, 0, s>>>(wl, sz, upper, A, B, info);
+    } else {
+        auto k = chol_small_kernel<T, NC, NW, 8, true>;
         k<<<grid_for(k, threads, items, persistent), threads, 0, s>>>(wl, sz, upper, A, B, info);
     }
 }
@@ -153,8 +106,11 @@ static void launch_potrs_small(const WorkList& wl, int bound, bool persistent, c
     if (max_nrhs <= 1) {
         auto k = potrs_small_kernel<T, NC, NW, 1>;
         k<<<grid_for(k, threads, items, persistent), threads, 0, s>>>(wl, sz, upper, A, B);
-    } else {
+    } else if (max_nrhs <= 4) {
         auto k = potrs_small_kernel<T, NC, NW, 4>;
+        k<<<grid_for(k, threads, items, persistent), threads, 0, s>>>(wl, sz, upper, A, B);
+    } else {
+        auto k = potrs_small_kernel<T, NC, NW, 8>;
         k<<<grid_for(k, threads, items, persistent), threads, 0, s>>>(wl, sz, upper, A, B);
     }
 }
@@ -174,8 +130,11 @@ static void launch_potrs_blocked(const WorkList& wl, int bound, bool persistent,
     if (max_nrhs <= 1) {
         auto k = potrs_blocked_kernel<T, NT, 1>;
         k<<<grid_for(k, NT, bound, persistent), NT, 0, s>>>(wl, sz, upper, A, B);
-    } else {
+    } else if (max_nrhs <= 4) {
         auto k = potrs_blocked_kernel<T, NT, 4>;
+        k<<<grid_for(k, NT, bound, persistent), NT, 0, s>>>(wl, sz, upper, A, B);
+    } else {
+        auto k = potrs_blocked_kernel<T, NT, 8>;
         k<<<grid_for(k, NT, bound, persistent), NT, 0, s>>>(wl, sz, upper, A, B);
     }
 }

@@ -19,4 +19,11 @@ template <typename T>
 void chol_bucket(int b, const WorkList& wl, int bound, bool persistent, const LuSizes& sz, bool upper, T** A, T** B,
                  int* info, bool factor, bool solve, int max_nrhs, cudaStream_t s);
 
+// One launch for buckets min(top, 6)..0 of a bucketize() result (orders up to 512):
+// the persistent queue kernel of chol_queue.cuh. `head` must hold 0 and is used
+// as the ticket counter. Same work and results as chol_bucket over those buckets.
+template <typename T>
+void chol_queue(const int* counts, const int* lists, int batch, int top, int* head, const LuSizes& sz, bool upper,
+                T** A, T** B, int* info, bool factor, bool solve, int max_nrhs, cudaStream_t s);
+
 }  // namespace mb200

@@ -72,6 +72,34 @@ __device__ __forceinline__ void mat_sync() {
     if (NW == 1) __syncwarp(); else __syncthreads();
 }
 
+// The threads that share one matrix as a barrier functor: the whole block or one
+// warp (MatSync), or a team of warps inside a larger block (BarSync: a named
+// barrier of `count` threads, which orders their shared-memory accesses as
+// __syncthreads does for the block).
+template <int NW>
+struct MatSync {
+    __device__ __forceinline__ void operator()() const { mat_sync<NW>(); }
+};
+struct BarSync {
+    int id, count;
+    __device__ __forceinline__ void operator()() const {
+        asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+    }
+};
+
+// A matrix's threads for the one-matrix-per-team kernels: rank within the team and
+// the team's barrier. BlockTeam is the whole thread block; WarpRangeTeam is the
+// warps [first, first + count / 32) of a larger block on named barrier `id`.
+struct BlockTeam {
+    __device__ __forceinline__ int tid() const { return threadIdx.x; }
+    __device__ __forceinline__ void sync() const { __syncthreads(); }
+};
+struct WarpRangeTeam {
+    int first_thread, id, count;
+    __device__ __forceinline__ int tid() const { return threadIdx.x - first_thread; }
+    __device__ __forceinline__ void sync() const { BarSync{id, count}(); }
+};
+
 // Pivot key: |x| as an ordered unsigned integer (the bit pattern of a
 // non-negative IEEE number is monotonic in its value), split into two 32-bit
 // halves for the warp REDUX instructions. Order: rows that are not candidates

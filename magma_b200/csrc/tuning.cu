@@ -12,6 +12,7 @@
 #include "tuning.h"
 #include "../../include/magma_b200.h"
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -36,6 +37,7 @@ static void set_defaults(TuningTable& t) {
     const int dmma[kLuBlockedBuckets] = {0, 0, 0, 1};
     for (int b = 0; b < kLuBlockedBuckets; ++b) t.lu_dmma[b] = dmma[b];
     for (int i = 0; i < kMixedTcOrders; ++i) t.mixed_tc_n[i] = 1;
+    t.chol_queue = 1;
 }
 
 static void to_values(const TuningTable& t, int* v) {
@@ -45,12 +47,15 @@ static void to_values(const TuningTable& t, int* v) {
     v[i++] = t.mixed_tc_lu;
     for (int b = 0; b < kLuBlockedBuckets; ++b) v[i++] = t.lu_dmma[b];
     for (int k = 0; k < kMixedTcOrders; ++k) v[i++] = t.mixed_tc_n[k];
+    v[i++] = t.chol_queue;
 }
 
-// count kTuningValues, or kTuningValuesV1 / V2 (tables saved before the later
+// count kTuningValues, or kTuningValuesV1 / V2 / V3 (tables saved before the later
 // entries existed: those keep their current values).
 static bool from_values(const int* v, int count, TuningTable& t) {
-    if (count != kTuningValues && count != kTuningValuesV1 && count != kTuningValuesV2) return false;
+    if (count != kTuningValues && count != kTuningValuesV1 && count != kTuningValuesV2 &&
+        count != kTuningValuesV3)
+        return false;
     for (int i = 0; i < 2 * kGemmBuckets; ++i)
         if (v[i] < 0 || v[i] > (i < kGemmBuckets ? 3 : 2)) return false;   // 3: FP64 tensor-core tile
     for (int i = 2 * kGemmBuckets; i < count; ++i)
@@ -61,8 +66,9 @@ static bool from_values(const int* v, int count, TuningTable& t) {
     t.mixed_tc_lu = v[i++];
     if (count >= kTuningValuesV2)
         for (int b = 0; b < kLuBlockedBuckets; ++b) t.lu_dmma[b] = v[i++];
-    if (count >= kTuningValues)
+    if (count >= kTuningValuesV3)
         for (int k = 0; k < kMixedTcOrders; ++k) t.mixed_tc_n[k] = v[i++];
+    if (count >= kTuningValues) t.chol_queue = v[i++];
     return true;
 }
 
@@ -72,7 +78,8 @@ static bool load_file(const char* path, TuningTable& t) {
     char magic[64] = {0};
     int v[kTuningValues];
     bool ok = std::fscanf(f, "%63s", magic) == 1;
-    const int count = !ok ? 0 : std::strcmp(magic, "magma_b200_tuning_v3") == 0 ? kTuningValues
+    const int count = !ok ? 0 : std::strcmp(magic, "magma_b200_tuning_v4") == 0 ? kTuningValues
+                             : std::strcmp(magic, "magma_b200_tuning_v3") == 0 ? kTuningValuesV3
                              : std::strcmp(magic, "magma_b200_tuning_v2") == 0 ? kTuningValuesV2
                              : std::strcmp(magic, "magma_b200_tuning_v1") == 0 ? kTuningValuesV1 : 0;
     ok = ok && count > 0;
@@ -302,6 +309,79 @@ static magma_int_t tune_lu_update(magma_queue_t q, unsigned seed) {
     return MAGMA_SUCCESS;
 }
 
+// Sets each n x n matrix's diagonal to 2n + its value: with the other lower-triangle
+// entries in [-1, 1) the symmetric matrix the lower triangle defines is diagonally
+// dominant, hence positive definite.
+__global__ void tune_spd_diag_kernel(double* A, const long long* off, const int* n, int count) {
+    for (int i = blockIdx.x; i < count; i += gridDim.x) {
+        const int ni = n[i];
+        for (int d = threadIdx.x; d < ni; d += blockDim.x) A[off[i] + d + (size_t)d * ni] += 2.0 * ni;
+    }
+}
+
+// Variable-size Cholesky: one persistent launch against one launch per size bucket,
+// on 8,192 SPD systems with n on [4, 512] (density ~ n^-1.5) and 1-8 right-hand
+// sides, through magma_dposv_vbatched_max_nocheck (both give bit-identical results).
+static magma_int_t tune_chol_queue(magma_queue_t q, unsigned seed) {
+    const int count = 8192;
+    std::vector<int> n(count + 1), r(count + 1);
+    std::vector<long long> offA(count), offB(count);
+    unsigned long long st = seed * 1000003ull;
+    auto unit = [&] {
+        st = st * 6364136223846793005ull + 1442695040888963407ull;
+        return double(st >> 11) * (1.0 / 9007199254740992.0);
+    };
+    const double a = 0.5, b = 1.0 / std::sqrt(512.0);   // 4^-1/2, 512^-1/2: inverse CDF of n^-1.5
+    long long na = 0, nb = 0;
+    int max_n = 0;
+    for (int i = 0; i < count; ++i) {
+        const double x = a - unit() * (a - b);
+        n[i] = std::min(512, std::max(4, (int)std::lround(1.0 / (x * x))));
+        r[i] = 1 + (int)(unit() * 8.0) % 8;
+        offA[i] = na;
+        offB[i] = nb;
+        na += (long long)n[i] * n[i];
+        nb += (long long)n[i] * r[i];
+        max_n = std::max(max_n, n[i]);
+    }
+    n[count] = r[count] = 0;
+    DevBuf dA, dA0, dB, dP, dI, dO;
+    if (!dA.alloc(8 * na) || !dA0.alloc(8 * na) || !dB.alloc(8 * nb) || !dP.alloc(sizeof(double*) * 2 * count) ||
+        !dI.alloc(sizeof(int) * 3 * (count + 1)) || !dO.alloc(sizeof(long long) * count))
+        return MAGMA_ERR_DEVICE_ALLOC;
+    std::vector<double*> ptr(2 * count);
+    for (int i = 0; i < count; ++i) {
+        ptr[i] = (double*)dA.p + offA[i];
+        ptr[count + i] = (double*)dB.p + offB[i];
+    }
+    int* dn = (int*)dI.p;
+    int* dr = dn + count + 1;
+    int* dinfo = dr + count + 1;
+    cudaMemcpyAsync(dP.p, ptr.data(), sizeof(double*) * 2 * count, cudaMemcpyHostToDevice, q->stream);
+    cudaMemcpyAsync(dn, n.data(), sizeof(int) * (count + 1), cudaMemcpyHostToDevice, q->stream);
+    cudaMemcpyAsync(dr, r.data(), sizeof(int) * (count + 1), cudaMemcpyHostToDevice, q->stream);
+    cudaMemcpyAsync(dO.p, offA.data(), sizeof(long long) * count, cudaMemcpyHostToDevice, q->stream);
+    tune_fill_kernel<double><<<1024, 256, 0, q->stream>>>((double*)dA0.p, (size_t)na, seed + 1);
+    tune_spd_diag_kernel<<<1024, 128, 0, q->stream>>>((double*)dA0.p, (const long long*)dO.p, dn, count);
+    tune_fill_kernel<double><<<1024, 256, 0, q->stream>>>((double*)dB.p, (size_t)nb, seed + 2);
+    cudaStreamSynchronize(q->stream);
+    double** pA = (double**)dP.p;
+    double** pB = pA + count;
+    float best = 1e30f;
+    int best_v = tuning().chol_queue;
+    for (int v = 0; v < 2; ++v) {
+        tuning_mut().chol_queue = v;
+        const float ms = time_ms(q->stream, [&] {
+            cudaMemcpyAsync(dA.p, dA0.p, 8 * na, cudaMemcpyDeviceToDevice, q->stream);
+            magma_dposv_vbatched_max_nocheck(MagmaLower, dn, dr, pA, dn, pB, dn, dinfo, count, max_n, 8, q);
+        }, 3);
+        if (cudaGetLastError() != cudaSuccess) return MAGMA_ERR_UNKNOWN;
+        if (ms < best) { best = ms; best_v = v; }
+    }
+    tuning_mut().chol_queue = best_v;
+    return MAGMA_SUCCESS;
+}
+
 }  // namespace mb200
 
 using namespace mb200;
@@ -315,6 +395,7 @@ magma_int_t magma_b200_autotune(magma_queue_t queue) {
     if (!rc) rc = tune_gemm<float>(1, queue, 23);
     if (!rc) rc = tune_mixed(queue, 29);
     if (!rc) rc = tune_lu_update(queue, 31);
+    if (!rc) rc = tune_chol_queue(queue, 37);
     cudaStreamSynchronize(queue->stream);
     return rc;
 }
@@ -338,7 +419,7 @@ magma_int_t magma_b200_tuning_save(const char* path) {
     if (!f) return MAGMA_ERR_UNKNOWN;
     int v[kTuningValues];
     to_values(tuning(), v);
-    std::fprintf(f, "magma_b200_tuning_v3\n");
+    std::fprintf(f, "magma_b200_tuning_v4\n");
     for (int i = 0; i < kTuningValues; ++i) std::fprintf(f, "%d%c", v[i], i + 1 < kTuningValues ? ' ' : '\n');
     return std::fclose(f) == 0 ? MAGMA_SUCCESS : MAGMA_ERR_UNKNOWN;
 }

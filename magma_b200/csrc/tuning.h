@@ -19,12 +19,15 @@ struct TuningTable {
     int lu_dmma[kLuBlockedBuckets];      // 1: FP64 blocked LU trailing update on the tensor cores (DMMA)
     int mixed_tc_n[kMixedTcOrders];      // per order n = 96 + 32 i: 1 tensor-core LU (+ fused refinement),
                                          // 0 CUDA-core FP32 LU + separate refinement
+    int chol_queue;                      // variable-size FP64 Cholesky: 1 one persistent launch over all
+                                         // sizes <= 512 (largest first), 0 one launch per size bucket
 };
 
 const TuningTable& tuning();   // defaults, or the file named by MAGMA_B200_TUNING, or the last autotune/set
 TuningTable& tuning_mut();
 constexpr int kTuningValuesV1 = 2 * kGemmBuckets + 1;
 constexpr int kTuningValuesV2 = kTuningValuesV1 + kLuBlockedBuckets;
-constexpr int kTuningValues = kTuningValuesV2 + kMixedTcOrders;
+constexpr int kTuningValuesV3 = kTuningValuesV2 + kMixedTcOrders;
+constexpr int kTuningValues = kTuningValuesV3 + 1;
 
 }  // namespace mb200

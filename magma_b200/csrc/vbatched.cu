@@ -77,7 +77,7 @@ magma_int_t bucketize2(const int* key, const int* key2, int batch, const int* ed
     for (int b = 0; b < nb; ++b) edges.e[b] = edges_host[b];
     int* d_counts = ws;
     int* d_lists = ws + 2 * nb;
-    cudaMemsetAsync(d_counts, 0, sizeof(int) * nb, s);
+    cudaMemsetAsync(d_counts, 0, sizeof(int) * 2 * nb, s);   // counts and the nb spare counters after them
     bucketize_kernel<<<ceildiv(batch, 256), 256, 0, s>>>(key, key2, batch, edges, d_counts, d_lists);
     *counts_out = d_counts;
     *lists_out = d_lists;

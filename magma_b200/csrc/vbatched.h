@@ -15,7 +15,8 @@ struct BucketEdges {
 // Counting-sorts instances 0..batch-1 into nb buckets by key[i] (bucket b
 // holds keys <= edges[b]; keys <= 0 are dropped). ws must hold
 // bucketize_ws_ints(batch, nb) ints. Outputs device pointers to the counts
-// (nb ints) and the lists (bucket b at lists + b*batch).
+// (nb ints, followed by nb more ints set to zero that callers may use as
+// counters) and the lists (bucket b at lists + b*batch).
 magma_int_t bucketize(const int* key, int batch, const int* edges_host, int nb, cudaStream_t s, int* ws,
                       int** counts_out, int** lists_out);
 size_t bucketize_ws_ints(int batch, int nb);
