@@ -857,7 +857,14 @@ class C4CholVbatched:
                 "graph": "one captured CUDA graph per step", "gflop_per_step": self.flops / 1e9}
 
     def launches_per_step(self):
-        return 1 + 8 * 2   # bucketize + per-bucket factor/solve kernels (graph-replayed)
+        # bucketize + largest-first sort, then the persistent queue kernel (tuning value 19 = 1)
+        # or the per-bucket kernels of orders <= 512: factor + solve fused for n <= 64 (4
+        # buckets), separate for the 3 blocked buckets
+        from magma_b200 import _lib
+        lib = _lib.load()
+        vals = (C.c_int * 20)()
+        queue = lib.magma_b200_tuning_get(vals, 20) == 20 and vals[19] == 1
+        return 2 + (1 if queue else 4 + 3 * 2)
 
     def _raw_fp64(self, q):
         return q.lib.magma_dposv_vbatched_max_nocheck(122, vp(self.dn), vp(self.dr), vp(self.pA), vp(self.dn),
@@ -955,8 +962,9 @@ class C4CholVbatched:
     def dominant_kernel(self, q, stream, reps=5):
         ms = timed_restore(stream, lambda i: self.step(q, i), self.restore, reps) / reps
         alg = float((16.0 * self.n ** 2 + 16.0 * self.n * self.nrhs + 4).sum())
-        return {"kernel": "posv_vbatched (graph: potrf/potrs bucket kernels)", "ms": ms, "alg_bytes": alg,
-                "tflops": self.flops / ms / 1e9}
+        name = ("chol_queue_kernel<double,1,1,8> (posv_vbatched: one persistent launch after bucketize + sort)"
+                if self.launches_per_step() == 3 else "posv_vbatched (graph: potrf/potrs bucket kernels)")
+        return {"kernel": name, "ms": ms, "alg_bytes": alg, "tflops": self.flops / ms / 1e9}
 
     def extras(self, q, stream, reps=3):
         """Per-bucket roofline: each size bucket's instances solved alone (eager calls on a

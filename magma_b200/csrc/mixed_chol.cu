@@ -20,6 +20,7 @@
 // the _max_nocheck form.
 #include "internal.h"
 #include "chol_launch.h"
+#include "tuning.h"
 #include "small_lu.cuh"
 #include "vbatched.h"
 #include <algorithm>
@@ -326,6 +327,29 @@ __global__ void copy_rhs_vkernel(WorkList wl, const int* n_arr, const int* nrhs_
     }
 }
 
+// X = B for every instance with fkey set: each warp scans 32 instances with a ballot
+// and copies the flagged ones together (the fallback is rare, so most warps copy nothing).
+__global__ void copy_rhs_flagged_kernel(const int* fkey, int batch, const int* n_arr, const int* nrhs_arr,
+                                        double** dB_array, const int* lddb, double** dX_array, const int* lddx) {
+    const int lane = threadIdx.x & 31;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    for (int c0 = gw * 32; c0 < batch; c0 += nw * 32) {
+        const int i = c0 + lane;
+        unsigned m = __ballot_sync(0xffffffffu, i < batch && fkey[i] != 0);
+        while (m) {
+            const int id = c0 + __ffs(m) - 1;
+            m &= m - 1;
+            const int n = n_arr[id], nrhs = nrhs_arr[id], ldb = lddb[id], ldx = lddx[id];
+            const double* B = dB_array[id];
+            double* X = dX_array[id];
+            for (int idx = lane; idx < n * nrhs; idx += 32) {
+                const int r = idx % n, c = idx / n;
+                X[r + (size_t)c * ldx] = B[r + (size_t)c * ldb];
+            }
+        }
+    }
+}
+
 // ---- host driver ----
 static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
@@ -402,6 +426,14 @@ magma_int_t dsposv_var(const int* n, const int* nrhs, double** A, const int* lda
     rc = bucketize(ws.fkey, batch, kCholEdges, kCholBuckets, s, bws_f, &counts, &lists);
     if (rc) return rc;
     const LuSizes sz64{0, 0, 0, 0, 0, n, n, lda, ldx, nrhs};
+    if (tuning().chol_queue && top < kCholBuckets - 1) {
+        // one copy and one persistent factor + solve launch over every size
+        copy_rhs_flagged_kernel<<<std::max(1, std::min(ceildiv(batch, 256), 1184)), 256, 0, s>>>(
+            ws.fkey, batch, n, nrhs, B, ldb, X, ldx);
+        chol_queue<double>(counts, lists, batch, top, counts + kCholBuckets, sz64, false, A, X, info, true, true,
+                           max_nrhs, s);
+        return launch_status();
+    }
     if ((rc = queue_fork(queue))) return rc;
     for (int b = top; b >= 0; --b) {
         cudaStream_t sb = queue_aux(queue, top - b);
