@@ -862,8 +862,9 @@ class C4CholVbatched:
         # buckets), separate for the 3 blocked buckets
         from magma_b200 import _lib
         lib = _lib.load()
-        vals = (C.c_int * 20)()
-        queue = lib.magma_b200_tuning_get(vals, 20) == 20 and vals[19] == 1
+        count = lib.magma_b200_tuning_get(None, 0)
+        vals = (C.c_int * count)()
+        queue = lib.magma_b200_tuning_get(vals, count) == count and vals[19] == 1
         return 2 + (1 if queue else 4 + 3 * 2)
 
     def _raw_fp64(self, q):

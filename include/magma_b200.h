@@ -398,23 +398,24 @@ magma_int_t magma_b200_host_solver_destroy(magma_b200_host_solver_t solver);
 /* ------------------------------------------------------------------------
  * Kernel-variant tuning (no reference counterpart; takes the role of the
  * reference's static tables control/batched_kernel_param.h and the headers
- * under magmablas/gemm_config/). The table holds 20 values: the GEMM tile variant
+ * under magmablas/gemm_config/). The table holds 21 values: the GEMM tile variant
  * (0: 64x64, 1: 32x32, 2: 16x16; for FP64 also 3: 64x64 on the tensor cores) for
  * max(M,N) <= 16, <= 32, <= 64 and larger, first for FP64 then FP32; 1/0 for the
  * tensor-core LU in magma_dsgesv_batched (n = 96..256, step 32) as a whole; 1/0 for
  * the FP64 blocked LU's trailing update on the tensor cores (DMMA) instead of the
  * FP64 pipe, for max(m) <= 128, <= 256, <= 512, <= 1024; and 1/0 for the tensor-core
- * LU (with its fused refinement) at each order n = 96, 128, ..., 256; and 1/0 for
- * the variable-size FP64 Cholesky (potrf / potrs / posv vbatched) as one persistent
- * launch over all orders <= 512 instead of one launch per size bucket. Tables of 9,
- * 13 or 19 values (saved before the later entries existed) are accepted and leave
+ * LU (with its fused refinement) at each order n = 96, 128, ..., 256; 1/0 for the
+ * variable-size FP64 Cholesky (potrf / potrs / posv vbatched) as one persistent
+ * launch over all orders <= 512 instead of one launch per size bucket; and 1/0 for
+ * the same choice in the variable-size FP64 LU (getrf / gesv vbatched). Tables of 9,
+ * 13, 19 or 20 values (saved before the later entries existed) are accepted and leave
  * the rest unchanged. Defaults are built in;
  * MAGMA_B200_TUNING=<file> loads a saved table at first use. Variants of one
  * family compute bit-identical results; tuning changes speed only. Not to be
  * called while other calls of this library are in flight.
  * magma_b200_autotune times every variant on the queue's device with synthetic
  * problems and keeps the fastest (synchronises the queue). tuning_get returns
- * the number of values (20) and fills `values` when count >= 20; tuning_set
+ * the number of values (21) and fills `values` when count >= 21; tuning_set
  * returns MAGMA_ERR_ILLEGAL_VALUE for a wrong count or an out-of-range value. */
 magma_int_t magma_b200_autotune(magma_queue_t queue);
 magma_int_t magma_b200_tuning_get(magma_int_t* values, magma_int_t count);

@@ -30,6 +30,14 @@ template <typename T>
 magma_int_t getrs_blocked(const WorkList& wl, int bound, bool persistent, bool trans, const LuSizes& sz, int max_n,
                           int max_nrhs, T** A, int** ipiv, T** B, cudaStream_t s);
 
+// One launch for buckets min(top, 6)..0 of a bucketize() result keyed by max(m, n)
+// (orders up to 512): the persistent queue kernel of lu_queue.cuh. getrf when !solve,
+// else gesv (getrf + getrs NoTrans). `head` must hold 0 (ticket counter). Same work
+// and results as the per-bucket getrf / gesv kernels over those buckets.
+template <typename T>
+void lu_queue(bool solve, const int* counts, const int* lists, int batch, int top, int* head, const LuSizes& sz,
+              T** A, int** ipiv, T** B, int* info, int max_nrhs, cudaStream_t s);
+
 // Mixed-precision LU solve (mixed.cu): FP32 factor, FP64 refinement, FP64 fallback; n <= 512.
 bool dsgesv_supported(int n);
 magma_int_t dsgesv_batched(int n, int nrhs, double** dA, int lda, int** ipiv, double** dB, int ldb, double** dX,

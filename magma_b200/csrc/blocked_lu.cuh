@@ -103,10 +103,11 @@ __device__ __forceinline__ void dmma_884(double& d0, double& d1, double a, doubl
 template <int NB, int NT, int CW>
 __device__ __forceinline__ void blocked_update_dmma(double* A, int lda, int k0, int j0, int cw, int nbp,
                                                     const int (&rpos)[4], const bool (&rupd)[4],
-                                                    const double (&U)[NB][CW + 1], const double (&af)[4][NB / 4][32]) {
+                                                    const double (&U)[NB][CW + 1], const double (&af)[4][NB / 4][32],
+                                                    int tid) {
     constexpr int KS = NB / 4;
-    const int lane = threadIdx.x & 31;
-    const int row0 = (threadIdx.x & ~31) + (lane >> 2);   // warp's first row + this lane's row in a group
+    const int lane = tid & 31;
+    const int row0 = (tid & ~31) + (lane >> 2);   // warp's first row + this lane's row in a group
     const int q = lane & 3;
     const int ks = (nbp + 3) / 4;                         // k-steps with a panel column
     bool gact[4];                                         // groups with a row to update
@@ -155,11 +156,12 @@ __device__ __forceinline__ void blocked_update_dmma(double* A, int lda, int k0, 
     }
 }
 
-template <typename T, int NB, int NT, int CW, int CB, bool DMMA>
+template <typename T, int NB, int NT, int CW, int CB, bool DMMA, typename Team = BlockTeam>
 __device__ void blocked_getrf(T* __restrict__ A, int m, int n, int lda, int* __restrict__ ipiv, int& info,
-                              BlockedLuShared<T, NB, NT, CW, DMMA>& sh) {
+                              BlockedLuShared<T, NB, NT, CW, DMMA>& sh, const Team& team = Team{}) {
     constexpr int NW = NT / 32;
-    const int tid = threadIdx.x;
+    const int tid = team.tid();
+    auto sync = [&] { team.sync(); };
     const int kmax = min(m, n);
     info = 0;
     for (int k0 = 0; k0 < kmax; k0 += NB) {
@@ -171,7 +173,7 @@ __device__ void blocked_getrf(T* __restrict__ A, int m, int n, int lda, int* __r
         for (int c = 0; c < NB; ++c) a[c] = (live && c < nbp) ? A[tid + (size_t)(k0 + c) * lda] : T(0);
         int pos = (tid < m) ? tid : INT_MAX / 2;
         int my_ipiv = 0;
-        lu_panel_steps<T, NB, NW>(a, m, nbp, nbp, k0, tid, pos, my_ipiv, info, sh.lu, ipiv == nullptr);
+        lu_panel_steps<T, NB, NW>(a, m, nbp, nbp, k0, tid, pos, my_ipiv, info, sh.lu, ipiv == nullptr, sync);
         if (ipiv && tid >= k0 && tid < k0 + nbp) ipiv[tid] = my_ipiv;
         const bool pivot_row = live && pos < k0 + nbp;
         const bool displaced = live && pos != tid;
@@ -196,10 +198,10 @@ __device__ void blocked_getrf(T* __restrict__ A, int m, int n, int lda, int* __r
             const int slot = pivot_row ? (pos - k0) : (nbp + tid - k0);
             for (int j0 = 0; j0 < k0; j0 += LW) {
                 const int w = min(LW, k0 - j0);
-                __syncthreads();
+                team.sync();
                 if (displaced)
                     for (int c = 0; c < w; ++c) stage[slot * LW + c] = A[tid + (size_t)(j0 + c) * lda];
-                __syncthreads();
+                team.sync();
                 if (displaced)
                     for (int c = 0; c < w; ++c) A[pos + (size_t)(j0 + c) * lda] = stage[slot * LW + c];
             }
@@ -243,23 +245,23 @@ __device__ void blocked_getrf(T* __restrict__ A, int m, int n, int lda, int* __r
         prefetch(k0 + nbp);
         for (int j0 = k0 + nbp; j0 < n; j0 += CW) {
             const int cw = min(CW, n - j0);
-            __syncthreads();   // sU / L11 / src ready; previous chunk's readers done
+            team.sync();   // sU / L11 / src ready; previous chunk's readers done
             for (int idx = tid; idx < nbp * cw; idx += NT) {
                 const int r = idx % nbp, c = idx / nbp;
                 sh.U[r][c] = A[sh.src[r] + (size_t)(j0 + c) * lda];
             }
-            __syncthreads();
+            team.sync();
             // U12 = L11^-1 A12, one thread per column, in two halves of H rows held in
             // registers; each entry gets its fma's in ascending step order.
             for (int c = tid; c < cw; c += NT) blocked_trsm_column<T, NB, NT, CW, DMMA>(sh, c);
-            __syncthreads();
+            team.sync();
             // A22 -= L21 U12 for the non-pivot live rows, stored at their new positions.
             // A row only ever overwrites the old row of a pivot (already gathered above),
             // so no barrier is needed between these loads and stores.
             if constexpr (kDmma) {
                 blocked_update_dmma<NB, NT, CW>(reinterpret_cast<double*>(A), lda, k0, j0, cw, nbp, rpos, rupd,
                                                 reinterpret_cast<const double(&)[NB][CW + 1]>(sh.U),
-                                                reinterpret_cast<const double(&)[4][NB / 4][32]>(sh.af[tid >> 5]));
+                                                reinterpret_cast<const double(&)[4][NB / 4][32]>(sh.af[tid >> 5]), tid);
             } else if (upd) {
                 for (int c0 = 0; c0 < cw; c0 += CB) {
                     T acc[CB];
@@ -279,13 +281,13 @@ __device__ void blocked_getrf(T* __restrict__ A, int m, int n, int lda, int* __r
                         if (c0 + c < cw) A[pos + (size_t)(j0 + c0 + c) * lda] = acc[c];
                 }
             }
-            __syncthreads();   // every displaced row has read its old row before U12 lands there
+            team.sync();   // every displaced row has read its old row before U12 lands there
             for (int idx = tid; idx < nbp * cw; idx += NT) {
                 const int r = idx % nbp, c = idx / nbp;
                 A[k0 + r + (size_t)(j0 + c) * lda] = sh.U[r][c];
             }
         }
-        __syncthreads();   // panel k0 complete before the next panel reads rows
+        team.sync();   // panel k0 complete before the next panel reads rows
     }
 }
 

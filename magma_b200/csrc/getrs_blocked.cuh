@@ -41,14 +41,15 @@ __device__ __forceinline__ int laswp_target(const int* s_ipiv, int n, int t, boo
     return idx;
 }
 
-template <typename T, int NT, int R>
-__device__ __forceinline__ void permute_rows(T (&b)[R], int n, int t, int idx, BlockedRsShared<T, NT, R>& sh) {
-    __syncthreads();
+template <typename T, int NT, int R, typename Team>
+__device__ __forceinline__ void permute_rows(T (&b)[R], int n, int t, int idx, BlockedRsShared<T, NT, R>& sh,
+                                             const Team& team) {
+    team.sync();
     if (t < n) {
 #pragma unroll
         for (int r = 0; r < R; ++r) sh.x[idx][r] = b[r];
     }
-    __syncthreads();
+    team.sync();
     if (t < n) {
 #pragma unroll
         for (int r = 0; r < R; ++r) b[r] = sh.x[t][r];
@@ -76,12 +77,13 @@ __device__ __forceinline__ void stage_diag(const T* __restrict__ A, int lda, int
 }
 
 // op(A) X = B for one matrix; A holds the getrf factors, B is overwritten.
-template <typename T, int NT, int R>
+template <typename T, int NT, int R, typename Team = BlockTeam>
 __device__ void blocked_getrs(bool trans, const T* __restrict__ A, int n, int lda, const int* __restrict__ ipiv,
-                              T* __restrict__ B, int nrhs, int ldb, BlockedRsShared<T, NT, R>& sh) {
-    const int t = threadIdx.x;
+                              T* __restrict__ B, int nrhs, int ldb, BlockedRsShared<T, NT, R>& sh,
+                              const Team& team = Team{}) {
+    const int t = team.tid();
     for (int k = t; k < n; k += NT) sh.ipiv[k] = ipiv ? ipiv[k] : k + 1;   // no pivots: identity
-    __syncthreads();
+    team.sync();
     const int fwd_idx = (t < n) ? laswp_target(sh.ipiv, n, t, false) : t;
     const int inv_idx = (t < n) ? laswp_target(sh.ipiv, n, t, true) : t;
     const int nblk = (n + 31) / 32;
@@ -90,11 +92,11 @@ __device__ void blocked_getrs(bool trans, const T* __restrict__ A, int n, int ld
 #pragma unroll
         for (int r = 0; r < R; ++r) b[r] = (t < n && c0 + r < nrhs) ? B[t + (size_t)(c0 + r) * ldb] : T(0);
         if (!trans) {
-            permute_rows<T, NT, R>(b, n, t, fwd_idx, sh);
+            permute_rows<T, NT, R>(b, n, t, fwd_idx, sh, team);
             // ---- L (unit lower), blocks ascending ----
             for (int J = 0; J < nblk; ++J) {
                 const int j0 = J * 32, j1 = min(n, j0 + 32);
-                __syncthreads();
+                team.sync();
                 if ((t >> 5) == J) {   // the warp that owns rows j0..j1-1 solves the diagonal block
                     stage_diag<T, NT, R>(A, lda, j0, j1, t, sh);
                     const int lane = t & 31, cnt = j1 - j0;
@@ -113,7 +115,7 @@ __device__ void blocked_getrs(bool trans, const T* __restrict__ A, int n, int ld
                         }
                     });
                 }
-                __syncthreads();
+                team.sync();
                 if (t >= j1 && t < n) {
 #pragma unroll
                     for (int kk = 0; kk < 32; ++kk) {
@@ -128,7 +130,7 @@ __device__ void blocked_getrs(bool trans, const T* __restrict__ A, int n, int ld
             // ---- U (non-unit upper), blocks descending ----
             for (int J = nblk - 1; J >= 0; --J) {
                 const int j0 = J * 32, j1 = min(n, j0 + 32);
-                __syncthreads();
+                team.sync();
                 if ((t >> 5) == J) {
                     stage_diag<T, NT, R>(A, lda, j0, j1, t, sh);
                     const int lane = t & 31, cnt = j1 - j0;
@@ -151,7 +153,7 @@ __device__ void blocked_getrs(bool trans, const T* __restrict__ A, int n, int ld
                         }
                     });
                 }
-                __syncthreads();
+                team.sync();
                 if (t < j0) {
 #pragma unroll
                     for (int kk = 31; kk >= 0; --kk) {
@@ -167,7 +169,7 @@ __device__ void blocked_getrs(bool trans, const T* __restrict__ A, int n, int ld
             // ---- U^T (non-unit lower), blocks ascending: y_k = b_k / U(k,k), b_i -= U(k,i) y_k ----
             for (int J = 0; J < nblk; ++J) {
                 const int j0 = J * 32, j1 = min(n, j0 + 32);
-                __syncthreads();
+                team.sync();
                 if ((t >> 5) == J) {
                     stage_diag<T, NT, R>(A, lda, j0, j1, t, sh);
                     const int lane = t & 31, cnt = j1 - j0;
@@ -190,7 +192,7 @@ __device__ void blocked_getrs(bool trans, const T* __restrict__ A, int n, int ld
                         }
                     });
                 }
-                __syncthreads();
+                team.sync();
                 if (t >= j1 && t < n) {
 #pragma unroll
                     for (int kk = 0; kk < 32; ++kk) {
@@ -205,7 +207,7 @@ __device__ void blocked_getrs(bool trans, const T* __restrict__ A, int n, int ld
             // ---- L^T (unit upper), blocks descending ----
             for (int J = nblk - 1; J >= 0; --J) {
                 const int j0 = J * 32, j1 = min(n, j0 + 32);
-                __syncthreads();
+                team.sync();
                 if ((t >> 5) == J) {
                     stage_diag<T, NT, R>(A, lda, j0, j1, t, sh);
                     const int lane = t & 31, cnt = j1 - j0;
@@ -224,7 +226,7 @@ __device__ void blocked_getrs(bool trans, const T* __restrict__ A, int n, int ld
                         }
                     });
                 }
-                __syncthreads();
+                team.sync();
                 if (t < j0) {
 #pragma unroll
                     for (int kk = 31; kk >= 0; --kk) {
@@ -236,14 +238,14 @@ __device__ void blocked_getrs(bool trans, const T* __restrict__ A, int n, int ld
                     }
                 }
             }
-            permute_rows<T, NT, R>(b, n, t, inv_idx, sh);
+            permute_rows<T, NT, R>(b, n, t, inv_idx, sh, team);
         }
         if (t < n) {
 #pragma unroll
             for (int r = 0; r < R; ++r)
                 if (c0 + r < nrhs) B[t + (size_t)(c0 + r) * ldb] = b[r];
         }
-        __syncthreads();
+        team.sync();
     }
 }
 

@@ -9,7 +9,9 @@
 #include "internal.h"
 #include "batched_kernels.h"
 #include "vbatched.h"
+#include "tuning.h"
 #include <algorithm>
+#include <type_traits>
 
 namespace mb200 {
 
@@ -42,6 +44,27 @@ static magma_int_t lu_var(LuOp op, bool trans, const int* m, const int* n, const
                                lists, ws + bw);
     if (rc) return rc;
     const LuSizes sz{0, 0, 0, 0, 0, m, n, lda, ldb, nrhs};
+    if constexpr (std::is_same<T, double>::value) {
+        if (op != LuOp::Getrs && tuning().lu_queue) {
+            // orders <= 512: one persistent launch over all buckets, largest first; the
+            // 1024-thread bucket (512 < max(m, n) <= 1024) beside it on an auxiliary stream
+            const bool solve = op == LuOp::Gesv;
+            int* head = counts + kLuBuckets;
+            if (top < kLuBuckets - 1) {
+                lu_queue<T>(solve, counts, lists, batch, top, head, sz, A, ipiv, B, info, max_nrhs, queue->stream);
+                return launch_status();
+            }
+            if ((rc = queue_fork(queue))) return rc;
+            const int b = kLuBuckets - 1;
+            const WorkList wl{lists + (size_t)b * batch, counts + b, 0};
+            cudaStream_t s0 = queue_aux(queue, 0);
+            rc = getrf_blocked<T>(wl, batch, true, sz, kLuEdges[b], A, ipiv, info, s0);
+            if (!rc && solve) rc = getrs_blocked<T>(wl, batch, true, false, sz, kLuEdges[b], max_nrhs, A, ipiv, B, s0);
+            lu_queue<T>(solve, counts, lists, batch, top, head, sz, A, ipiv, B, info, max_nrhs, queue_aux(queue, 1));
+            queue_join(queue);
+            return rc ? rc : launch_status();
+        }
+    }
     // buckets are independent: each runs on its own auxiliary stream
     if ((rc = queue_fork(queue))) return rc;
     for (int b = top; b >= 0; --b) {

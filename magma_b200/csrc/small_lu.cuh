@@ -189,10 +189,11 @@ struct SmallLuShared {
 // ipiv(g) (1-based) in `my_ipiv`, and `info` is g+1 of the first zero pivot.
 // With nopiv the row at position g is step g's pivot (getrf_nopiv): no search,
 // rows never change position.
-template <typename T, int NC, int NW>
+template <typename T, int NC, int NW, typename Sync = MatSync<NW>>
 __device__ __forceinline__ void lu_panel_steps(T (&a)[NC], int m, int nsteps, int ncols, int k0, int tid, int& pos,
                                                int& my_ipiv, int& info,
-                                               SmallLuShared<T, NC, NW>& sh, bool nopiv = false) {
+                                               SmallLuShared<T, NC, NW>& sh, bool nopiv = false,
+                                               const Sync& sync = Sync{}) {
     (void)ncols;   // columns >= ncols hold zeros in every row, so their updates are no-ops
     const int lane = tid & 31;
     const int warp = tid >> 5;
@@ -211,7 +212,7 @@ __device__ __forceinline__ void lu_panel_steps(T (&a)[NC], int m, int nsteps, in
         s = warp_argmax(key, p, lane) + warp * 32;
         if (NW > 1) {
             if (lane == 0) { sh.red_hi[buf][warp] = key.hi; sh.red_lo[buf][warp] = key.lo; sh.red_p[buf][warp] = p; sh.red_s[buf][warp] = s; }
-            __syncthreads();
+            sync();
             // every warp reduces the NW warp winners lane-parallel (lane w = warp w's winner)
             const bool v = lane < NW;
             key = PivotKey{v ? sh.red_hi[buf][lane] : 0u, v ? sh.red_lo[buf][lane] : 0u};
@@ -226,7 +227,7 @@ __device__ __forceinline__ void lu_panel_steps(T (&a)[NC], int m, int nsteps, in
 #pragma unroll
             for (int j = jw; j < NC; j += 2) row2[j / 2] = make_vec2<T>(a[j], a[j + 1]);
         }
-        mat_sync<NW>();
+        sync();
         const T piv = sh.row[buf][k];
         // ---- LAPACK swap bookkeeping: ipiv(g) = current position of the pivot row ----
         if (tid == g) my_ipiv = p + 1;

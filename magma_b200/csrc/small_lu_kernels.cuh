@@ -35,58 +35,43 @@ __device__ __forceinline__ void store_rows(const T (&a)[NC], T* __restrict__ A, 
 }
 
 // ---------------------------------------------------------------------------
-// getrf
+// One instance of getrf on the matrix's threads (tid = row). n <= 0 or m <= 0 writes info 0.
 template <typename T, int NC, int NW>
-__global__ void __launch_bounds__(32 * NW * BlockShape<NW>::MPB, MinBlocks<NC, NW>::value)
-getrf_small_kernel(WorkList wl, LuSizes sz, T** dA_array, int** ipiv_array, int* info_array) {
-    constexpr int MPB = BlockShape<NW>::MPB;
-    __shared__ SmallLuShared<T, NC, NW> shm[MPB];
-    const int local = (NW == 1) ? (threadIdx.x >> 5) : 0;
-    const int tid = (NW == 1) ? (threadIdx.x & 31) : threadIdx.x;
-    // NW == 1: each warp walks its own items; NW > 1: the block walks them together
-    for (int w = blockIdx.x * MPB + local; w < wl.size(); w += gridDim.x * MPB) {
-        const int id = wl.at(w);
-        const int m = sz.get_m(id), n = sz.get_n(id), lda = sz.get_lda(id);
-        if (m <= 0 || n <= 0) {
-            if (tid == 0) info_array[id] = 0;
-            continue;
-        }
-        T* A = dA_array[id];
-        T a[NC];
-        load_rows<T, NC, NW>(a, A, m, n, lda, tid);
-        int pos, my_ipiv, info;
-        // a null pivot array selects LU without pivoting (getrf_nopiv)
-        small_lu_factor<T, NC, NW>(a, m, n, tid, pos, my_ipiv, info, shm[local], ipiv_array == nullptr);
-        store_rows<T, NC>(a, A, m, n, lda, tid, pos);
-        if (ipiv_array && tid < min(m, n)) ipiv_array[id][tid] = my_ipiv;
-        if (tid == 0) info_array[id] = info;
-        mat_sync<NW>();
+__device__ __forceinline__ void getrf_small_instance(int id, const LuSizes& sz, T** dA_array, int** ipiv_array,
+                                                     int* info_array, int tid, SmallLuShared<T, NC, NW>& sh) {
+    const int m = sz.get_m(id), n = sz.get_n(id), lda = sz.get_lda(id);
+    if (m <= 0 || n <= 0) {
+        if (tid == 0) info_array[id] = 0;
+        return;
     }
+    T* A = dA_array[id];
+    T a[NC];
+    load_rows<T, NC, NW>(a, A, m, n, lda, tid);
+    int pos, my_ipiv, info;
+    // a null pivot array selects LU without pivoting (getrf_nopiv)
+    small_lu_factor<T, NC, NW>(a, m, n, tid, pos, my_ipiv, info, sh, ipiv_array == nullptr);
+    store_rows<T, NC>(a, A, m, n, lda, tid, pos);
+    if (ipiv_array && tid < min(m, n)) ipiv_array[id][tid] = my_ipiv;
+    if (tid == 0) info_array[id] = info;
 }
 
-// ---------------------------------------------------------------------------
-// gesv: getrf + getrs(NoTrans) in one pass. R = RHS columns solved together.
+// One instance of gesv: getrf + getrs(NoTrans) in one pass, R RHS columns solved together.
 template <typename T, int NC, int NW, int R>
-__global__ void __launch_bounds__(32 * NW * BlockShape<NW>::MPB, MinBlocks<NC, NW>::value)
-gesv_small_kernel(WorkList wl, LuSizes sz, T** dA_array, int** ipiv_array, T** dB_array, int* info_array) {
+__device__ __forceinline__ void gesv_small_instance(int id, const LuSizes& sz, T** dA_array, int** ipiv_array,
+                                                    T** dB_array, int* info_array, int tid,
+                                                    SmallLuShared<T, NC, NW>& sh) {
     static_assert(R <= 4, "the shared rhs buffer holds 4 right-hand sides a group");
-    constexpr int MPB = BlockShape<NW>::MPB;
-    __shared__ SmallLuShared<T, NC, NW> shm[MPB];
-    const int local = (NW == 1) ? (threadIdx.x >> 5) : 0;
-    const int tid = (NW == 1) ? (threadIdx.x & 31) : threadIdx.x;
-    for (int w = blockIdx.x * MPB + local; w < wl.size(); w += gridDim.x * MPB) {
-    const int id = wl.at(w);
     const int n = sz.get_n(id), lda = sz.get_lda(id), ldb = sz.get_ldb(id), nrhs = sz.get_nrhs(id);
     if (n <= 0) {
         if (tid == 0) info_array[id] = 0;
-        continue;
+        return;
     }
     T* A = dA_array[id];
     T* B = dB_array[id];
     T a[NC];
     load_rows<T, NC, NW>(a, A, n, n, lda, tid);
     int pos, my_ipiv, info;
-    small_lu_factor<T, NC, NW>(a, n, n, tid, pos, my_ipiv, info, shm[local], ipiv_array == nullptr);
+    small_lu_factor<T, NC, NW>(a, n, n, tid, pos, my_ipiv, info, sh, ipiv_array == nullptr);
     store_rows<T, NC>(a, A, n, n, lda, tid, pos);
     if (ipiv_array && tid < n) ipiv_array[id][tid] = my_ipiv;
     if (tid == 0) info_array[id] = info;
@@ -99,14 +84,44 @@ gesv_small_kernel(WorkList wl, LuSizes sz, T** dA_array, int** ipiv_array, T** d
 #pragma unroll
         for (int r = 0; r < R; ++r)
             b[r] = (tid < n && c0 + r < nrhs) ? B[tid + (size_t)(c0 + r) * ldb] : T(0);
-        small_lu_solve<T, NC, NW, R>(a, n, pos, b, shm[local]);
+        small_lu_solve<T, NC, NW, R>(a, n, pos, b, sh);
         if (tid < n) {
 #pragma unroll
             for (int r = 0; r < R; ++r)
                 if (c0 + r < nrhs) B[pos + (size_t)(c0 + r) * ldb] = b[r];
         }
     }
-    mat_sync<NW>();
+}
+
+// ---------------------------------------------------------------------------
+// getrf
+template <typename T, int NC, int NW>
+__global__ void __launch_bounds__(32 * NW * BlockShape<NW>::MPB, MinBlocks<NC, NW>::value)
+getrf_small_kernel(WorkList wl, LuSizes sz, T** dA_array, int** ipiv_array, int* info_array) {
+    constexpr int MPB = BlockShape<NW>::MPB;
+    __shared__ SmallLuShared<T, NC, NW> shm[MPB];
+    const int local = (NW == 1) ? (threadIdx.x >> 5) : 0;
+    const int tid = (NW == 1) ? (threadIdx.x & 31) : threadIdx.x;
+    // NW == 1: each warp walks its own items; NW > 1: the block walks them together
+    for (int w = blockIdx.x * MPB + local; w < wl.size(); w += gridDim.x * MPB) {
+        getrf_small_instance<T, NC, NW>(wl.at(w), sz, dA_array, ipiv_array, info_array, tid, shm[local]);
+        mat_sync<NW>();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// gesv: getrf + getrs(NoTrans) in one pass. R = RHS columns solved together.
+template <typename T, int NC, int NW, int R>
+__global__ void __launch_bounds__(32 * NW * BlockShape<NW>::MPB, MinBlocks<NC, NW>::value)
+gesv_small_kernel(WorkList wl, LuSizes sz, T** dA_array, int** ipiv_array, T** dB_array, int* info_array) {
+    constexpr int MPB = BlockShape<NW>::MPB;
+    __shared__ SmallLuShared<T, NC, NW> shm[MPB];
+    const int local = (NW == 1) ? (threadIdx.x >> 5) : 0;
+    const int tid = (NW == 1) ? (threadIdx.x & 31) : threadIdx.x;
+    for (int w = blockIdx.x * MPB + local; w < wl.size(); w += gridDim.x * MPB) {
+        gesv_small_instance<T, NC, NW, R>(wl.at(w), sz, dA_array, ipiv_array, dB_array, info_array, tid,
+                                          shm[local]);
+        mat_sync<NW>();
     }
 }
 

@@ -25,19 +25,23 @@ namespace mb200 {
 static TuningTable g_table;
 static std::once_flag g_once;
 
-// Built-in defaults: the table magma_b200_autotune measured on a B200.
+// Built-in defaults: what magma_b200_autotune picked on B200s (the same picks in three
+// runs), except the GEMM tile of the 33-64 bucket, where the 32x32 tile ran the C2
+// workload (20,000 instances, M, N, K in 8..128) faster than the autotuner's 64x64 pick
+// (6.71 against 6.64 TF/s in FP64).
 static void set_defaults(TuningTable& t) {
     const int gemm[2][kGemmBuckets] = {{2, 1, 1, 1}, {2, 1, 1, 1}};
     for (int p = 0; p < 2; ++p)
         for (int b = 0; b < kGemmBuckets; ++b) t.gemm_variant[p][b] = gemm[p][b];
     const char* e = std::getenv("MAGMA_B200_TENSOR_CORE_LU");
     t.mixed_tc_lu = (e && e[0] == '0') ? 0 : 1;
-    // measured on a B200 (uniform[-1,1] batches of 1 GB): the FMA update is faster up to
-    // m = 512 (n = 256: 4.58 against 4.74 ms), DMMA at m = 1,024 (23.4 against 23.9 ms)
-    const int dmma[kLuBlockedBuckets] = {0, 0, 0, 1};
-    for (int b = 0; b < kLuBlockedBuckets; ++b) t.lu_dmma[b] = dmma[b];
-    for (int i = 0; i < kMixedTcOrders; ++i) t.mixed_tc_n[i] = 1;
-    t.chol_queue = 1;
+    // the FP64 pipe's update in every bucket (DMMA is slower at each size: n = 256
+    // 684 against 734 us in ncu, 1,024 within noise)
+    for (int b = 0; b < kLuBlockedBuckets; ++b) t.lu_dmma[b] = 0;
+    // tensor-core LU from n = 160 on; the CUDA-core FP32 LU is faster at n = 96 and 128
+    for (int i = 0; i < kMixedTcOrders; ++i) t.mixed_tc_n[i] = (i >= 2);
+    t.chol_queue = 1;   // one launch for the variable-size Cholesky
+    t.lu_queue = 0;     // one launch per size bucket for the variable-size LU
 }
 
 static void to_values(const TuningTable& t, int* v) {
@@ -48,13 +52,14 @@ static void to_values(const TuningTable& t, int* v) {
     for (int b = 0; b < kLuBlockedBuckets; ++b) v[i++] = t.lu_dmma[b];
     for (int k = 0; k < kMixedTcOrders; ++k) v[i++] = t.mixed_tc_n[k];
     v[i++] = t.chol_queue;
+    v[i++] = t.lu_queue;
 }
 
-// count kTuningValues, or kTuningValuesV1 / V2 / V3 (tables saved before the later
+// count kTuningValues, or kTuningValuesV1 / V2 / V3 / V4 (tables saved before the later
 // entries existed: those keep their current values).
 static bool from_values(const int* v, int count, TuningTable& t) {
     if (count != kTuningValues && count != kTuningValuesV1 && count != kTuningValuesV2 &&
-        count != kTuningValuesV3)
+        count != kTuningValuesV3 && count != kTuningValuesV4)
         return false;
     for (int i = 0; i < 2 * kGemmBuckets; ++i)
         if (v[i] < 0 || v[i] > (i < kGemmBuckets ? 3 : 2)) return false;   // 3: FP64 tensor-core tile
@@ -68,7 +73,8 @@ static bool from_values(const int* v, int count, TuningTable& t) {
         for (int b = 0; b < kLuBlockedBuckets; ++b) t.lu_dmma[b] = v[i++];
     if (count >= kTuningValuesV3)
         for (int k = 0; k < kMixedTcOrders; ++k) t.mixed_tc_n[k] = v[i++];
-    if (count >= kTuningValues) t.chol_queue = v[i++];
+    if (count >= kTuningValuesV4) t.chol_queue = v[i++];
+    if (count >= kTuningValues) t.lu_queue = v[i++];
     return true;
 }
 
@@ -78,7 +84,8 @@ static bool load_file(const char* path, TuningTable& t) {
     char magic[64] = {0};
     int v[kTuningValues];
     bool ok = std::fscanf(f, "%63s", magic) == 1;
-    const int count = !ok ? 0 : std::strcmp(magic, "magma_b200_tuning_v4") == 0 ? kTuningValues
+    const int count = !ok ? 0 : std::strcmp(magic, "magma_b200_tuning_v5") == 0 ? kTuningValues
+                             : std::strcmp(magic, "magma_b200_tuning_v4") == 0 ? kTuningValuesV4
                              : std::strcmp(magic, "magma_b200_tuning_v3") == 0 ? kTuningValuesV3
                              : std::strcmp(magic, "magma_b200_tuning_v2") == 0 ? kTuningValuesV2
                              : std::strcmp(magic, "magma_b200_tuning_v1") == 0 ? kTuningValuesV1 : 0;
@@ -382,6 +389,73 @@ static magma_int_t tune_chol_queue(magma_queue_t q, unsigned seed) {
     return MAGMA_SUCCESS;
 }
 
+// Variable-size LU: one persistent launch against one launch per size bucket, on 8,192
+// diagonally dominant systems with n on [4, 512] (density ~ n^-1.5) and 1-8 right-hand
+// sides, through magma_dgesv_vbatched_max_nocheck (both give bit-identical results).
+static magma_int_t tune_lu_queue(magma_queue_t q, unsigned seed) {
+    const int count = 8192;
+    std::vector<int> n(count + 1), r(count + 1);
+    std::vector<long long> offA(count), offB(count), offP(count);
+    unsigned long long st = seed * 1000003ull;
+    auto unit = [&] {
+        st = st * 6364136223846793005ull + 1442695040888963407ull;
+        return double(st >> 11) * (1.0 / 9007199254740992.0);
+    };
+    const double a = 0.5, b = 1.0 / std::sqrt(512.0);
+    long long na = 0, nb = 0, np = 0;
+    int max_n = 0;
+    for (int i = 0; i < count; ++i) {
+        const double x = a - unit() * (a - b);
+        n[i] = std::min(512, std::max(4, (int)std::lround(1.0 / (x * x))));
+        r[i] = 1 + (int)(unit() * 8.0) % 8;
+        offA[i] = na;
+        offB[i] = nb;
+        offP[i] = np;
+        na += (long long)n[i] * n[i];
+        nb += (long long)n[i] * r[i];
+        np += n[i];
+        max_n = std::max(max_n, n[i]);
+    }
+    n[count] = r[count] = 0;
+    DevBuf dA, dA0, dB, dP, dI, dO, dV;
+    if (!dA.alloc(8 * na) || !dA0.alloc(8 * na) || !dB.alloc(8 * nb) || !dP.alloc(sizeof(void*) * 3 * count) ||
+        !dI.alloc(sizeof(int) * 3 * (count + 1)) || !dO.alloc(sizeof(long long) * count) ||
+        !dV.alloc(sizeof(int) * np))
+        return MAGMA_ERR_DEVICE_ALLOC;
+    std::vector<void*> ptr(3 * count);
+    for (int i = 0; i < count; ++i) {
+        ptr[i] = (double*)dA.p + offA[i];
+        ptr[count + i] = (double*)dB.p + offB[i];
+        ptr[2 * count + i] = (int*)dV.p + offP[i];
+    }
+    int* dn = (int*)dI.p;
+    int* dr = dn + count + 1;
+    int* dinfo = dr + count + 1;
+    cudaMemcpyAsync(dP.p, ptr.data(), sizeof(void*) * 3 * count, cudaMemcpyHostToDevice, q->stream);
+    cudaMemcpyAsync(dn, n.data(), sizeof(int) * (count + 1), cudaMemcpyHostToDevice, q->stream);
+    cudaMemcpyAsync(dr, r.data(), sizeof(int) * (count + 1), cudaMemcpyHostToDevice, q->stream);
+    cudaMemcpyAsync(dO.p, offA.data(), sizeof(long long) * count, cudaMemcpyHostToDevice, q->stream);
+    tune_fill_kernel<double><<<1024, 256, 0, q->stream>>>((double*)dA0.p, (size_t)na, seed + 1);
+    tune_spd_diag_kernel<<<1024, 128, 0, q->stream>>>((double*)dA0.p, (const long long*)dO.p, dn, count);
+    tune_fill_kernel<double><<<1024, 256, 0, q->stream>>>((double*)dB.p, (size_t)nb, seed + 2);
+    cudaStreamSynchronize(q->stream);
+    void** p = (void**)dP.p;
+    float best = 1e30f;
+    int best_v = tuning().lu_queue;
+    for (int v = 0; v < 2; ++v) {
+        tuning_mut().lu_queue = v;
+        const float ms = time_ms(q->stream, [&] {
+            cudaMemcpyAsync(dA.p, dA0.p, 8 * na, cudaMemcpyDeviceToDevice, q->stream);
+            magma_dgesv_vbatched_max_nocheck(dn, dr, (double**)p, dn, (int**)(p + 2 * count), (double**)(p + count),
+                                             dn, dinfo, count, max_n, 8, q);
+        }, 3);
+        if (cudaGetLastError() != cudaSuccess) return MAGMA_ERR_UNKNOWN;
+        if (ms < best) { best = ms; best_v = v; }
+    }
+    tuning_mut().lu_queue = best_v;
+    return MAGMA_SUCCESS;
+}
+
 }  // namespace mb200
 
 using namespace mb200;
@@ -396,6 +470,7 @@ magma_int_t magma_b200_autotune(magma_queue_t queue) {
     if (!rc) rc = tune_mixed(queue, 29);
     if (!rc) rc = tune_lu_update(queue, 31);
     if (!rc) rc = tune_chol_queue(queue, 37);
+    if (!rc) rc = tune_lu_queue(queue, 41);
     cudaStreamSynchronize(queue->stream);
     return rc;
 }
@@ -419,7 +494,7 @@ magma_int_t magma_b200_tuning_save(const char* path) {
     if (!f) return MAGMA_ERR_UNKNOWN;
     int v[kTuningValues];
     to_values(tuning(), v);
-    std::fprintf(f, "magma_b200_tuning_v4\n");
+    std::fprintf(f, "magma_b200_tuning_v5\n");
     for (int i = 0; i < kTuningValues; ++i) std::fprintf(f, "%d%c", v[i], i + 1 < kTuningValues ? ' ' : '\n');
     return std::fclose(f) == 0 ? MAGMA_SUCCESS : MAGMA_ERR_UNKNOWN;
 }

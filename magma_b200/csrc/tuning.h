@@ -21,6 +21,7 @@ struct TuningTable {
                                          // 0 CUDA-core FP32 LU + separate refinement
     int chol_queue;                      // variable-size FP64 Cholesky: 1 one persistent launch over all
                                          // sizes <= 512 (largest first), 0 one launch per size bucket
+    int lu_queue;                        // variable-size FP64 getrf / gesv: the same choice
 };
 
 const TuningTable& tuning();   // defaults, or the file named by MAGMA_B200_TUNING, or the last autotune/set
@@ -28,6 +29,7 @@ TuningTable& tuning_mut();
 constexpr int kTuningValuesV1 = 2 * kGemmBuckets + 1;
 constexpr int kTuningValuesV2 = kTuningValuesV1 + kLuBlockedBuckets;
 constexpr int kTuningValuesV3 = kTuningValuesV2 + kMixedTcOrders;
-constexpr int kTuningValues = kTuningValuesV3 + 1;
+constexpr int kTuningValuesV4 = kTuningValuesV3 + 1;
+constexpr int kTuningValues = kTuningValuesV4 + 1;
 
 }  // namespace mb200

@@ -16,7 +16,7 @@ from magma_b200 import _lib
 from magma_b200 import testing as T
 
 pytestmark = pytest.mark.gpu
-N_VALUES = 20
+N_VALUES = 21
 QUEUE = 19   # index of the queue switch in the tuning table
 
 

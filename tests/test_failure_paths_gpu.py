@@ -100,7 +100,7 @@ def test_tensor_core_wait_timeout_falls_back_to_fp64(cuda):
     import magma_b200 as mb
     from magma_b200 import _lib
     lib = _lib.load()
-    n, batch = 128, 20
+    n, batch = 256, 20   # an order the built-in table runs on the tensor-core LU
     A_np, B_np, _ = T.svd_logrand(batch, n, 1e2, 1e6, nrhs=4, seed=31)
     lib.magma_b200_debug_tc_wait_limit(100000)
     try:

@@ -18,6 +18,26 @@ def dev(a, cuda):
     return torch.from_numpy(np.ascontiguousarray(a)).to(cuda)
 
 
+@pytest.fixture
+def tensor_core_lu():
+    """Every order n = 96..256 on the tensor-core LU (the built-in table keeps the
+    CUDA-core LU at 96 and 128, where it measured faster), restored afterwards."""
+    import ctypes as C
+
+    from magma_b200 import _lib
+    lib = _lib.load()
+    count = lib.magma_b200_tuning_get(None, 0)
+    vals = (C.c_int * count)()
+    assert lib.magma_b200_tuning_get(vals, count) == count
+    old = list(vals)
+    vals[8] = 1                      # the tensor-core LU as a whole
+    for i in range(13, 19):          # per order n = 96 + 32 (i - 13)
+        vals[i] = 1
+    assert lib.magma_b200_tuning_set(vals, count) == 0
+    yield
+    assert lib.magma_b200_tuning_set((C.c_int * count)(*old), count) == 0
+
+
 @pytest.mark.parametrize("n,batch", [(16, 64), (48, 64), (64, 48), (100, 32), (256, 24), (400, 6)])
 def test_dsgesv_svd_logrand(cuda, n, batch):
     import magma_b200 as mb
@@ -72,7 +92,7 @@ def test_dsgesv_rhs_counts(cuda, n, nrhs):
 
 
 @pytest.mark.parametrize("n", [96, 128, 160, 224, 256])
-def test_dsgesv_tensor_core_lu(cuda, n):
+def test_dsgesv_tensor_core_lu(cuda, tensor_core_lu, n):
     """Orders 96..256 in steps of 32 factor on the tensor cores (TMEM-resident LU, split
     TF32): with kappa up to 1e6 the refinement must converge as from an FP32 LU, and
     where it does the single-precision pivots are LAPACK's on all but rare near-ties."""
@@ -92,7 +112,7 @@ def test_dsgesv_tensor_core_lu(cuda, n):
     assert np.mean(same) >= 0.8, np.mean(same)
 
 
-def test_dsgesv_tensor_core_lu_fallbacks(cuda):
+def test_dsgesv_tensor_core_lu_fallbacks(cuda, tensor_core_lu):
     """The tensor-core path (n = 128) hands overflowing, NaN and singular instances to the
     FP64 fallback exactly as the CUDA-core path does."""
     import magma_b200 as mb

@@ -10,7 +10,7 @@ import pytest
 
 from magma_b200 import _lib
 
-N_VALUES = 20
+N_VALUES = 21
 
 
 def _get(lib):
@@ -29,34 +29,39 @@ def test_tuning_roundtrip(tmp_path):
     assert lib.magma_b200_tuning_get(None, 0) == N_VALUES           # size query
     orig = _get(lib)
     try:
-        new = [0, 1, 2, 0, 2, 1, 0, 0, 0, 1, 0, 1, 1, 1, 0, 1, 1, 0, 1, 0]
+        new = [0, 1, 2, 0, 2, 1, 0, 0, 0, 1, 0, 1, 1, 1, 0, 1, 1, 0, 1, 0, 0]
         assert _set(lib, new) == 0 and _get(lib) == new
         f = tmp_path / "tune.txt"
         assert lib.magma_b200_tuning_save(str(f).encode()) == 0
-        assert f.read_text().split()[0] == "magma_b200_tuning_v4"
+        assert f.read_text().split()[0] == "magma_b200_tuning_v5"
         assert _set(lib, orig) == 0 and _get(lib) == orig
         assert lib.magma_b200_tuning_load(str(f).encode()) == 0 and _get(lib) == new
         # rejected: wrong count, out-of-range values, unreadable or malformed files
-        assert _set(lib, new[:-2]) == _lib.MAGMA_ERR_ILLEGAL_VALUE   # 18: no table has that size
+        assert _set(lib, new[:-3]) == _lib.MAGMA_ERR_ILLEGAL_VALUE   # 18: no table has that size
         assert _set(lib, [4] + new[1:]) == _lib.MAGMA_ERR_ILLEGAL_VALUE      # FP64 tiles: 0..3
         assert _set(lib, new[:4] + [3] + new[5:]) == _lib.MAGMA_ERR_ILLEGAL_VALUE   # FP32 tiles: 0..2
         assert _set(lib, [3] + new[1:]) == 0 and _get(lib)[0] == 3
         assert _set(lib, new) == 0
         assert _set(lib, new[:-1] + [2]) == _lib.MAGMA_ERR_ILLEGAL_VALUE
-        # 9-, 13- and 19-value tables (saved before the later entries existed) set their part only
+        # 9-, 13-, 19- and 20-value tables (saved before the later entries existed) set their part only
         assert _set(lib, orig[:9]) == 0 and _get(lib) == orig[:9] + new[9:]
         assert _set(lib, orig[:13]) == 0 and _get(lib) == orig[:13] + new[13:]
         assert _set(lib, orig[:19]) == 0 and _get(lib) == orig[:19] + new[19:]
+        assert _set(lib, orig[:20]) == 0 and _get(lib) == orig[:20] + new[20:]
         v1 = tmp_path / "v1.txt"
         v1.write_text("magma_b200_tuning_v1\n" + " ".join(map(str, new[:9])) + "\n")
-        assert lib.magma_b200_tuning_load(str(v1).encode()) == 0 and _get(lib) == new[:9] + orig[9:19] + new[19:]
+        assert lib.magma_b200_tuning_load(str(v1).encode()) == 0 and _get(lib) == new[:9] + orig[9:20] + new[20:]
         v2 = tmp_path / "v2.txt"
         v2.write_text("magma_b200_tuning_v2\n" + " ".join(map(str, new[:13])) + "\n")
-        assert lib.magma_b200_tuning_load(str(v2).encode()) == 0 and _get(lib) == new[:13] + orig[13:19] + new[19:]
+        assert lib.magma_b200_tuning_load(str(v2).encode()) == 0 and _get(lib) == new[:13] + orig[13:20] + new[20:]
         assert _set(lib, new) == 0
         v3 = tmp_path / "v3.txt"
         v3.write_text("magma_b200_tuning_v3\n" + " ".join(map(str, orig[:19])) + "\n")
         assert lib.magma_b200_tuning_load(str(v3).encode()) == 0 and _get(lib) == orig[:19] + new[19:]
+        assert _set(lib, new) == 0
+        v4 = tmp_path / "v4.txt"
+        v4.write_text("magma_b200_tuning_v4\n" + " ".join(map(str, orig[:20])) + "\n")
+        assert lib.magma_b200_tuning_load(str(v4).encode()) == 0 and _get(lib) == orig[:20] + new[20:]
         assert _set(lib, new) == 0
         assert lib.magma_b200_tuning_load(str(tmp_path / "missing").encode()) == _lib.MAGMA_ERR_ILLEGAL_VALUE
         bad = tmp_path / "bad.txt"
