@@ -399,7 +399,9 @@ magma_int_t magma_b200_host_solver_destroy(magma_b200_host_solver_t solver);
  * Kernel-variant tuning (no reference counterpart; takes the role of the
  * reference's static tables control/batched_kernel_param.h and the headers
  * under magmablas/gemm_config/). The table holds 21 values: the GEMM tile variant
- * (0: 64x64, 1: 32x32, 2: 16x16; for FP64 also 3: 64x64 on the tensor cores) for
+ * (0: 64x64, 1: 32x32, 2: 16x16; 3: on the tensor cores, FP64 64x64 with mma.sync
+ * .f64 (bit-identical to 0-2) and FP32 128x128 with tcgen05 split TF32 (within the
+ * reference tester's 30 eps bound, not bit-identical to 0-2)) for
  * max(M,N) <= 16, <= 32, <= 64 and larger, first for FP64 then FP32; 1/0 for the
  * tensor-core LU in magma_dsgesv_batched (n = 96..256, step 32) as a whole; 1/0 for
  * the FP64 blocked LU's trailing update on the tensor cores (DMMA) instead of the
@@ -411,7 +413,8 @@ magma_int_t magma_b200_host_solver_destroy(magma_b200_host_solver_t solver);
  * 13, 19 or 20 values (saved before the later entries existed) are accepted and leave
  * the rest unchanged. Defaults are built in;
  * MAGMA_B200_TUNING=<file> loads a saved table at first use. Variants of one
- * family compute bit-identical results; tuning changes speed only. Not to be
+ * family compute bit-identical results (except the FP32 tensor-core tile, noted above);
+ * tuning changes speed only. Not to be
  * called while other calls of this library are in flight.
  * magma_b200_autotune times every variant on the queue's device with synthetic
  * problems and keeps the fastest (synchronises the queue). tuning_get returns

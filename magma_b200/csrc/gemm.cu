@@ -22,6 +22,7 @@
 #include "vbatched.h"
 #include "tuning.h"
 #include "lu_sizes.h"
+#include "tc_ptx.cuh"
 #include <algorithm>
 
 namespace mb200 {
@@ -370,6 +371,189 @@ gemm_dmma_kernel(GemmSizes g, double alpha, const double* const* __restrict__ A_
     }
 }
 
+// FP32 tile on the tcgen05 tensor cores (FP32 variant 3): a 128x128 tile of C per
+// 128-thread block, accumulated in tensor memory (128 lanes x 128 FP32 columns; thread t
+// owns lane t = row t of the tile). K runs in chunks of 32: the threads stage op(A) and
+// op(B) as split TF32 pairs (hi = x rounded to TF32, lo = x - hi) in the no-swizzle K-major
+// layout of 8x4 core matrices, then one thread issues the chunk's four K = 8 steps as three
+// MMAs each (lo*hi, hi*lo, hi*hi: ~21-bit products accumulated in FP32, the lo*lo term
+// dropped) and commits them to an mbarrier the block waits on, bounded. Thread t stages
+// row t of op(A) and of op(B)^T, its 32 loads issued together. B is staged for N rounded
+// up to 16 columns (the MMA's N), zero past N; rows of A past M are left as they are (they
+// only reach accumulator rows that are never stored); the K tail is zero in both operands. Unlike the CUDA-core tiles this is not the same
+// fma chain: the results differ in the last bits and are held to the reference tester's
+// bound ||C - C_ref|| / (sqrt(k+2) |alpha| ||A|| ||B|| + 2 |beta| ||C||) < 30 eps
+// (testing/testing_sgemm_vbatched.cpp). A wait that runs out (about a second) leaves the
+// tile unwritten and counts in g_gemm_tc_timeouts.
+__device__ int g_gemm_tc_timeouts;
+constexpr int kTcGemmKc = 32;
+constexpr long long kTcGemmWaitCycles = 2000000000LL;
+
+__device__ __forceinline__ int tc_kmajor(int row, int k) {   // float index of (row, k) in a 32-wide K chunk
+    return (((row >> 3) * 8 + (k >> 2)) * 8 + (row & 7)) * 4 + (k & 3);
+}
+
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(128, 3)
+gemm_tc_kernel(GemmSizes g, float alpha, const float* const* __restrict__ A_arr,
+               const float* const* __restrict__ B_arr, float beta, float** __restrict__ C_arr, int tiles_m,
+               int tiles_n, WorkList wl) {
+    constexpr int BM = 128, BN = 128, KC = kTcGemmKc;
+    extern __shared__ __align__(1024) unsigned char gemm_tc_smem[];
+    float* sA = reinterpret_cast<float*>(gemm_tc_smem);   // [hi, lo][BM * KC]
+    float* sB = sA + 2 * BM * KC;                          // [hi, lo][BN * KC]
+    __shared__ unsigned long long mbar_word;
+    __shared__ uint32_t tmem_base;
+    const int tiles = tiles_m * tiles_n;
+    const int w = blockIdx.x / tiles;
+    if (w >= wl.size()) return;
+    const int id = wl.at(w);
+    const int tt = blockIdx.x - w * tiles;
+    const int i0 = (tt / tiles_n) * BM, j0 = (tt % tiles_n) * BN;
+    const int m = g.M(id), n = g.N(id), k = g.K(id);
+    if (i0 >= m || j0 >= n) return;
+    if ((g.tri == 1 && j0 > i0 + BM - 1) || (g.tri == 2 && i0 > j0 + BN - 1)) return;
+    const int lda = g.LDA(id), ldb = g.LDB(id), ldc = g.LDC(id);
+    const float* A = A_arr[id];
+    const float* B = B_arr[id];
+    float* C = C_arr[id];
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int mrows = min(BM, m - i0), ncols = min(BN, n - j0);
+    const int npad = (ncols + 15) & ~15;
+    const uint32_t mbar = tc::smem_addr(&mbar_word);
+    if (warp == 0) {
+        tc::tmem_alloc(tc::smem_addr(&tmem_base), BN);
+        tc::tmem_relinquish();
+    }
+    if (tid == 0) {
+        tc::mbar_init(mbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tbase = tmem_base;
+    const uint32_t idesc = tc::idesc_tf32(BM, npad, false);
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int k0 = 0; k0 < k; k0 += KC) {
+        // thread t stages row t of op(A) (rows < mrows) and row t of the N x K operand
+        // op(B)^T (rows < npad): 32 values of the chunk each, all loads issued before
+        // any is used, zero past K (and past N for B); rows of A past M stay unwritten
+        float xa[KC], xb[KC];
+        const int gi = i0 + tid, gj = j0 + tid;
+#pragma unroll
+        for (int q = 0; q < KC; ++q) {
+            const int gk = k0 + q;
+            xa[q] = (tid < mrows && gk < k) ? (TA ? A[gk + (size_t)gi * lda] : A[gi + (size_t)gk * lda]) : 0.0f;
+            xb[q] = (tid < ncols && gk < k) ? (TB ? B[gj + (size_t)gk * ldb] : B[gk + (size_t)gj * ldb]) : 0.0f;
+        }
+        if (tid < mrows) {
+#pragma unroll
+            for (int q = 0; q < KC; q += 4) {
+                float4 h, l;
+                tc::split_tf32(xa[q], h.x, l.x);
+                tc::split_tf32(xa[q + 1], h.y, l.y);
+                tc::split_tf32(xa[q + 2], h.z, l.z);
+                tc::split_tf32(xa[q + 3], h.w, l.w);
+                *reinterpret_cast<float4*>(sA + tc_kmajor(tid, q)) = h;
+                *reinterpret_cast<float4*>(sA + BM * KC + tc_kmajor(tid, q)) = l;
+            }
+        }
+        if (tid < npad) {
+#pragma unroll
+            for (int q = 0; q < KC; q += 4) {
+                float4 h, l;
+                tc::split_tf32(xb[q], h.x, l.x);
+                tc::split_tf32(xb[q + 1], h.y, l.y);
+                tc::split_tf32(xb[q + 2], h.z, l.z);
+                tc::split_tf32(xb[q + 3], h.w, l.w);
+                *reinterpret_cast<float4*>(sB + tc_kmajor(tid, q)) = h;
+                *reinterpret_cast<float4*>(sB + BN * KC + tc_kmajor(tid, q)) = l;
+            }
+        }
+        tc::fence_proxy_async_smem();
+        tc::fence_before_sync();
+        __syncthreads();
+        if (tid == 0) {
+            tc::fence_after_sync();
+#pragma unroll
+            for (int s4 = 0; s4 < KC / 8; ++s4) {   // K = 8 per MMA: two core matrices
+                const uint64_t ah = tc::smem_desc(tc::smem_addr(sA + s4 * 64), 128, 1024);
+                const uint64_t al = tc::smem_desc(tc::smem_addr(sA + BM * KC + s4 * 64), 128, 1024);
+                const uint64_t bh = tc::smem_desc(tc::smem_addr(sB + s4 * 64), 128, 1024);
+                const uint64_t bl = tc::smem_desc(tc::smem_addr(sB + BN * KC + s4 * 64), 128, 1024);
+                tc::mma_tf32(tbase, al, bh, idesc, k0 > 0 || s4 > 0);
+                tc::mma_tf32(tbase, ah, bl, idesc, true);
+                tc::mma_tf32(tbase, ah, bh, idesc, true);
+            }
+            tc::commit(mbar);
+        }
+        bool done = false;
+        const long long t0 = clock64();
+        while (!(done = tc::mbar_try_wait(mbar, phase)) && clock64() - t0 < kTcGemmWaitCycles) {
+        }
+        phase ^= 1u;
+        if (__syncthreads_or(!done)) {   // every thread leaves the loop; the tile stays unwritten
+            if (tid == 0) atomicAdd(&g_gemm_tc_timeouts, 1);
+            ok = false;
+            break;
+        }
+        tc::fence_after_sync();
+    }
+    if (ok) {
+        const int gi = i0 + tid;
+        const uint32_t trow = tbase + (uint32_t(32 * warp) << 16);
+        for (int c0 = 0; c0 < ncols; c0 += 32) {
+            float v[32];
+            if (k > 0) {
+                tc::tmem_ld32(trow + uint32_t(c0), v);
+                tc::wait_ld();
+            } else {
+#pragma unroll
+                for (int c = 0; c < 32; ++c) v[c] = 0.0f;
+            }
+            if (tid < mrows) {
+#pragma unroll
+                for (int c = 0; c < 32; ++c) {
+                    const int gj = j0 + c0 + c;
+                    if (c0 + c >= ncols || (g.tri == 1 && gj > gi) || (g.tri == 2 && gi > gj)) continue;
+                    float* cp = C + gi + (size_t)gj * ldc;
+                    *cp = (beta == 0.0f) ? alpha * v[c] : alpha * v[c] + beta * (*cp);
+                }
+            }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (warp == 0) tc::tmem_dealloc(tbase, BN);
+}
+
+constexpr int kTcGemmSmem = 4 * 128 * kTcGemmKc * (int)sizeof(float);   // A and B, hi and lo
+
+template <typename T>
+static magma_int_t gemm_launch_tc(bool TA, bool TB, const GemmSizes& g, T alpha, const T* const* A, const T* const* B,
+                                  T beta, T** C, const WorkList& wl, int bound, int max_m, int max_n, cudaStream_t s) {
+    if constexpr (sizeof(T) != 4) {
+        return MAGMA_ERR_NOT_SUPPORTED;
+    } else {
+        const int tiles_m = ceildiv(max_m, 128), tiles_n = ceildiv(max_n, 128);
+        const long blocks = (long)bound * tiles_m * tiles_n;
+        if (blocks > 0x7fffffffL) return MAGMA_ERR_NOT_SUPPORTED;
+        const dim3 grid((unsigned)blocks);
+        auto launch = [&](auto kern) {
+            ensure_dynamic_smem((const void*)kern, kTcGemmSmem);
+            kern<<<grid, 128, kTcGemmSmem, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n, wl);
+        };
+        if (!TA && !TB) launch(gemm_tc_kernel<false, false>);
+        else if (!TA && TB) launch(gemm_tc_kernel<false, true>);
+        else if (TA && !TB) launch(gemm_tc_kernel<true, false>);
+        else launch(gemm_tc_kernel<true, true>);
+        return 0;
+    }
+}
+
 template <typename T>
 static magma_int_t gemm_launch_dmma(bool TA, bool TB, const GemmSizes& g, T alpha, const T* const* A,
                                     const T* const* B, T beta, T** C, const WorkList& wl, int bound, int max_m,
@@ -418,9 +602,9 @@ static magma_int_t gemm_launch_variant(int variant, magma_trans_t ta, magma_tran
     switch (variant) {
         case 1: return gemm_launch_tile<T, GemmTile1>(TA, TB, g, alpha, A, B, beta, C, wl, bound, max_m, max_n, s);
         case 2: return gemm_launch_tile<T, GemmTile2>(TA, TB, g, alpha, A, B, beta, C, wl, bound, max_m, max_n, s);
-        case 3:   // FP64 tensor cores; FP32 has no such variant and takes the 64x64 tile
+        case 3:   // the tensor cores: FP64 mma.sync (DMMA) tile, FP32 tcgen05 split-TF32 tile
             if (sizeof(T) == 8) return gemm_launch_dmma<T>(TA, TB, g, alpha, A, B, beta, C, wl, bound, max_m, max_n, s);
-            return gemm_launch_tile<T, GemmTile0>(TA, TB, g, alpha, A, B, beta, C, wl, bound, max_m, max_n, s);
+            return gemm_launch_tc<T>(TA, TB, g, alpha, A, B, beta, C, wl, bound, max_m, max_n, s);
         default: return gemm_launch_tile<T, GemmTile0>(TA, TB, g, alpha, A, B, beta, C, wl, bound, max_m, max_n, s);
     }
 }

@@ -7,7 +7,8 @@
 // saved table at first use; magma_b200_autotune() measures every variant on the
 // queue's device with synthetic problems of each bucket and keeps the fastest.
 // Every variant of a family computes bit-identical results (same fma order per
-// output element), so tuning changes speed only.
+// output element), so tuning changes speed only; the one exception is the FP32 GEMM
+// tile on the tcgen05 tensor cores (split TF32), held to the reference tester's bound.
 #include "internal.h"
 #include "tuning.h"
 #include "../../include/magma_b200.h"
@@ -62,7 +63,7 @@ static bool from_values(const int* v, int count, TuningTable& t) {
         count != kTuningValuesV3 && count != kTuningValuesV4)
         return false;
     for (int i = 0; i < 2 * kGemmBuckets; ++i)
-        if (v[i] < 0 || v[i] > (i < kGemmBuckets ? 3 : 2)) return false;   // 3: FP64 tensor-core tile
+        if (v[i] < 0 || v[i] > 3) return false;   // 3: the tensor-core tile (FP64 DMMA, FP32 tcgen05)
     for (int i = 2 * kGemmBuckets; i < count; ++i)
         if (v[i] != 0 && v[i] != 1) return false;
     int i = 0;
@@ -209,7 +210,7 @@ static magma_int_t tune_gemm(int prec, magma_queue_t q, unsigned seed) {
         T** pA = (T**)dP.p; T** pB = pA + count; T** pC = pB + count;
         float best = 1e30f;
         int best_v = tuning().gemm_variant[prec][b];
-        for (int v = 0; v < (sizeof(T) == 8 ? 4 : 3); ++v) {
+        for (int v = 0; v < 4; ++v) {
             tuning_mut().gemm_variant[prec][b] = v;
             const float ms = time_ms(q->stream, [&] {
                 if (sizeof(T) == 8)

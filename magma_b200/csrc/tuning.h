@@ -14,7 +14,7 @@ constexpr int kMixedTcOrders = 6;      // the tensor-core LU's orders: n = 96, 1
 
 struct TuningTable {
     int gemm_variant[2][kGemmBuckets];   // [FP64, FP32][bucket]: tile variant (0: 64x64, 1: 32x32, 2: 16x16,
-                                         // 3: FP64 only, 64x64 on the tensor cores)
+                                         // 3: the tensor cores, FP64 64x64 DMMA or FP32 128x128 tcgen05)
     int mixed_tc_lu;                     // 1: tensor-core LU in the mixed solve (where mixed_tc_n allows it)
     int lu_dmma[kLuBlockedBuckets];      // 1: FP64 blocked LU trailing update on the tensor cores (DMMA)
     int mixed_tc_n[kMixedTcOrders];      // per order n = 96 + 32 i: 1 tensor-core LU (+ fused refinement),
