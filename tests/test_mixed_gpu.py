@@ -109,7 +109,8 @@ def test_dsgesv_tensor_core_lu(cuda, tensor_core_lu, n):
     O = A_np.copy()
     oip, _ = oracle.dgetrf_batched(O, n)
     same = [np.array_equal(ipiv[i], oip[i]) for i in range(batch) if it[i] >= 0]
-    assert np.mean(same) >= 0.8, np.mean(same)
+    # measured on B200: 92.5-97.5% of these instances (90.4% of a 512-instance C3 sample)
+    assert np.mean(same) >= 0.9, np.mean(same)
 
 
 def test_dsgesv_tensor_core_lu_fallbacks(cuda, tensor_core_lu):
