@@ -317,7 +317,7 @@ class C3Mixed:
         if acc[1] < 0.05 * acc[0]:
             # one kernel factors on the tensor cores and refines in FP64: quoted against HBM
             # with the algorithm's compulsory bytes, A read by the factorisation and again by
-            # every refinement pass (SURVEY's (1 + k) 8 n^2 per solve), B read and X written
+            # every refinement pass ((1 + k) 8 n^2 bytes per solve after k passes), B read and X written
             stages = {"lu_and_refine_ms": acc[0], "fallback_ms": acc[2]}
             return {"kernel": "lu_tf32x3_kernel (tcgen05 split-TF32 LU + FP64 refinement, one block per instance)",
                     "ms": acc[0], "alg_bytes": (batch + passes) * 8.0 * n * n + batch * 16.0 * n * r,
