@@ -52,6 +52,36 @@ using GemmTile0 = GemmTile<64, 64, 4, 4, 2, 3>;     // 256 threads
 using GemmTile1 = GemmTile<32, 32, 4, 4, 10, 16>;   // 64 threads
 using GemmTile2 = GemmTile<16, 16, 2, 2, 16, 16>;   // 64 threads
 
+// C = alpha acc + beta C for a thread's TM x TN outputs (rows tx + (BM/TM) i, columns
+// ty TN + j of the tile). Every read of C goes out before the first write: interleaved,
+// each read would wait for the previous write (the compiler cannot rule out aliasing).
+template <typename T, int BM, int TM, int TN>
+__device__ __forceinline__ void gemm_tile_epilogue(const GemmSizes& g, T alpha, T beta, T* C, int ldc, int m, int n,
+                                                   int i0, int j0, int tx, int ty, const T (&acc)[TM][TN]) {
+    T cv[TM][TN];
+    bool in[TM][TN];
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+        const int gj = j0 + ty * TN + j;
+#pragma unroll
+        for (int i = 0; i < TM; ++i) {
+            const int gi = i0 + tx + (BM / TM) * i;
+            in[i][j] = gj < n && gi < m && !(g.tri == 1 && gj > gi) && !(g.tri == 2 && gi > gj);
+            cv[i][j] = (in[i][j] && beta != T(0)) ? C[gi + (size_t)gj * ldc] : T(0);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+        const int gj = j0 + ty * TN + j;
+#pragma unroll
+        for (int i = 0; i < TM; ++i) {
+            const int gi = i0 + tx + (BM / TM) * i;
+            if (in[i][j])
+                C[gi + (size_t)gj * ldc] = (beta == T(0)) ? alpha * acc[i][j] : alpha * acc[i][j] + beta * cv[i][j];
+        }
+    }
+}
+
 template <typename T, bool TA, bool TB, typename S>
 __global__ void __launch_bounds__(S::NT, (sizeof(T) == 8 ? S::MINB_D : S::MINB_F))
 gemm_tile_kernel(GemmSizes g, T alpha, const T* const* __restrict__ A_arr, const T* const* __restrict__ B_arr, T beta,
@@ -141,18 +171,7 @@ gemm_tile_kernel(GemmSizes g, T alpha, const T* const* __restrict__ A_arr, const
                 for (int j = 0; j < TN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
         }
     }
-#pragma unroll
-    for (int j = 0; j < TN; ++j) {
-        const int gj = j0 + ty * TN + j;
-        if (gj >= n) continue;
-#pragma unroll
-        for (int i = 0; i < TM; ++i) {
-            const int gi = i0 + tx + (BM / TM) * i;
-            if (gi >= m || (g.tri == 1 && gj > gi) || (g.tri == 2 && gi > gj)) continue;
-            T* c = C + gi + (size_t)gj * ldc;
-            *c = (beta == T(0)) ? alpha * acc[i][j] : alpha * acc[i][j] + beta * (*c);
-        }
-    }
+    gemm_tile_epilogue<T, BM, TM, TN>(g, alpha, beta, C, ldc, m, n, i0, j0, tx, ty, acc);
 }
 
 // NN form of the CUDA-core tiles with an asynchronous operand pipeline: each K chunk
@@ -242,18 +261,7 @@ gemm_async_kernel(GemmSizes g, T alpha, const T* const* __restrict__ A_arr, cons
         }
     }
     asm volatile("cp.async.wait_group 0;" ::: "memory");
-#pragma unroll
-    for (int j = 0; j < TN; ++j) {
-        const int gj = j0 + ty * TN + j;
-        if (gj >= n) continue;
-#pragma unroll
-        for (int i = 0; i < TM; ++i) {
-            const int gi = i0 + tx + (BM / TM) * i;
-            if (gi >= m || (g.tri == 1 && gj > gi) || (g.tri == 2 && gi > gj)) continue;
-            T* cp = C + gi + (size_t)gj * ldc;
-            *cp = (beta == T(0)) ? alpha * acc[i][j] : alpha * acc[i][j] + beta * (*cp);
-        }
-    }
+    gemm_tile_epilogue<T, BM, TM, TN>(g, alpha, beta, C, ldc, m, n, i0, j0, tx, ty, acc);
 }
 
 // FP64 tile on the tensor cores (variant 3): a 64x64 tile of C per 256-thread block,
@@ -354,18 +362,33 @@ gemm_dmma_kernel(GemmSizes g, double alpha, const double* const* __restrict__ A_
                 for (int j = 0; j < 2; ++j) gemm_dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
         }
     }
+    // every read of C before the first write (as gemm_tile_epilogue)
+    double cv[4][2][2];
+    bool in[4][2][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const int gi = i0 + wm + 8 * i + r8;
-        if (gi >= m) continue;
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int gj = j0 + wn + 8 * j + 2 * q + h;
-                if (gj >= n || (g.tri == 1 && gj > gi) || (g.tri == 2 && gi > gj)) continue;
-                double* c = C + gi + (size_t)gj * ldc;
-                *c = (beta == 0.0) ? alpha * acc[i][j][h] : alpha * acc[i][j][h] + beta * (*c);
+                in[i][j][h] = gi < m && gj < n && !(g.tri == 1 && gj > gi) && !(g.tri == 2 && gi > gj);
+                cv[i][j][h] = (in[i][j][h] && beta != 0.0) ? C[gi + (size_t)gj * ldc] : 0.0;
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int gi = i0 + wm + 8 * i + r8;
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int gj = j0 + wn + 8 * j + 2 * q + h;
+                if (in[i][j][h])
+                    C[gi + (size_t)gj * ldc] =
+                        (beta == 0.0) ? alpha * acc[i][j][h] : alpha * acc[i][j][h] + beta * cv[i][j][h];
             }
         }
     }
@@ -514,12 +537,20 @@ gemm_tc_kernel(GemmSizes g, float alpha, const float* const* __restrict__ A_arr,
                 for (int c = 0; c < 32; ++c) v[c] = 0.0f;
             }
             if (tid < mrows) {
+                // all 32 reads of C before any write (the writes could alias later reads, so
+                // interleaved they would wait for each other)
+                float cv[32];
+#pragma unroll
+                for (int c = 0; c < 32; ++c) {
+                    const int gj = j0 + c0 + c;
+                    const bool in = c0 + c < ncols && !(g.tri == 1 && gj > gi) && !(g.tri == 2 && gi > gj);
+                    cv[c] = (in && beta != 0.0f) ? C[gi + (size_t)gj * ldc] : 0.0f;
+                }
 #pragma unroll
                 for (int c = 0; c < 32; ++c) {
                     const int gj = j0 + c0 + c;
                     if (c0 + c >= ncols || (g.tri == 1 && gj > gi) || (g.tri == 2 && gi > gj)) continue;
-                    float* cp = C + gi + (size_t)gj * ldc;
-                    *cp = (beta == 0.0f) ? alpha * v[c] : alpha * v[c] + beta * (*cp);
+                    C[gi + (size_t)gj * ldc] = (beta == 0.0f) ? alpha * v[c] : alpha * v[c] + beta * cv[c];
                 }
             }
         }
