@@ -26,12 +26,13 @@ namespace mb200 {
 static TuningTable g_table;
 static std::once_flag g_once;
 
-// Built-in defaults: what magma_b200_autotune picked on B200s (the same picks in three
-// runs), except the GEMM tile of the 33-64 bucket, where the 32x32 tile ran the C2
-// workload (20,000 instances, M, N, K in 8..128) faster than the autotuner's 64x64 pick
-// (6.71 against 6.64 TF/s in FP64).
+// Built-in defaults: what magma_b200_autotune picked on B200s, with the GEMM tiles
+// checked on the C2 workload (20,000 instances, M, N, K in 8..128): FP64 16x16 / 32x32
+// CUDA-core tiles up to max(M, N) = 32 and the DMMA tile above (7.38 TF/s, against 6.94
+// with CUDA-core tiles throughout); FP32 CUDA-core tiles up to 64 and the tcgen05 tile
+// above (14.6 TF/s, against 10.7).
 static void set_defaults(TuningTable& t) {
-    const int gemm[2][kGemmBuckets] = {{2, 1, 1, 1}, {2, 1, 1, 1}};
+    const int gemm[2][kGemmBuckets] = {{2, 1, 3, 3}, {2, 1, 1, 3}};
     for (int p = 0; p < 2; ++p)
         for (int b = 0; b < kGemmBuckets; ++b) t.gemm_variant[p][b] = gemm[p][b];
     const char* e = std::getenv("MAGMA_B200_TENSOR_CORE_LU");
