@@ -139,10 +139,16 @@ tri_panel_kernel(TriArgs<T> g, int panels, int batch) {
 #pragma unroll
                 for (int u = 0; u < EPR; ++u) put(u, rt[u], rx[u]);
             } else {
-                for (int u = 0; u < EPT; ++u) {
-                    T tv, xv;
-                    chunk_vals(kc, u, tv, xv);
-                    put(u, tv, xv);
+                // all the chunk's loads before its shared-memory stores: interleaved, each
+                // load would wait for the store before it (a generic pointer could alias it)
+                constexpr int H = EPT / 2;   // in two halves: the registers stay under the solve's
+#pragma unroll
+                for (int u0 = 0; u0 < EPT; u0 += H) {
+                    T tv[H], xv[H];
+#pragma unroll
+                    for (int u = 0; u < H; ++u) chunk_vals(kc, u0 + u, tv[u], xv[u]);
+#pragma unroll
+                    for (int u = 0; u < H; ++u) put(u0 + u, tv[u], xv[u]);
                 }
             }
             __syncthreads();
