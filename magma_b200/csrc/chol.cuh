@@ -204,6 +204,15 @@ __device__ __forceinline__ void chol_small_instance(int id, const LuSizes& sz, b
     T a[NC];
 #pragma unroll
     for (int j = 0; j < NC; ++j) a[j] = (tid < n && j <= tid) ? tri(A, lda, upper, tid, j) : T(0);
+    // the first group of right-hand sides is loaded with A, so its latency hides behind
+    // the factorisation (after the stores of A the compiler could not move it earlier)
+    T b0[R];
+    if constexpr (SOLVE) {
+        const int nrhs0 = sz.get_nrhs(id), ldb0 = sz.get_ldb(id);
+        const T* B0 = dB_array[id];
+#pragma unroll
+        for (int r = 0; r < R; ++r) b0[r] = (tid < n && r < nrhs0) ? B0[tid + (size_t)r * ldb0] : T(0);
+    }
     const int info = chol_panel_steps<T, NC, NW>(a, n, n, 0, tid, sh, sync);
     if (tid < n) {
         // on failure the rows stay as the steps left them, like LAPACK's partial factor
@@ -219,7 +228,8 @@ __device__ __forceinline__ void chol_small_instance(int id, const LuSizes& sz, b
         for (int c0 = 0; c0 < nrhs; c0 += R) {
             T b[R];
 #pragma unroll
-            for (int r = 0; r < R; ++r) b[r] = (tid < n && c0 + r < nrhs) ? B[tid + (size_t)(c0 + r) * ldb] : T(0);
+            for (int r = 0; r < R; ++r)
+                b[r] = (c0 == 0) ? b0[r] : (tid < n && c0 + r < nrhs) ? B[tid + (size_t)(c0 + r) * ldb] : T(0);
             chol_solve<T, NC, NW, R>(a, n, tid, b, sh, sync);
             if (tid < n) {
 #pragma unroll

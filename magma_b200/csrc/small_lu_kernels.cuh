@@ -70,6 +70,11 @@ __device__ __forceinline__ void gesv_small_instance(int id, const LuSizes& sz, T
     T* B = dB_array[id];
     T a[NC];
     load_rows<T, NC, NW>(a, A, n, n, lda, tid);
+    // the first group of right-hand sides is loaded with A, so its latency hides behind
+    // the factorisation (after the stores of A the compiler could not move it earlier)
+    T b0[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) b0[r] = (tid < n && r < nrhs) ? B[tid + (size_t)r * ldb] : T(0);
     int pos, my_ipiv, info;
     small_lu_factor<T, NC, NW>(a, n, n, tid, pos, my_ipiv, info, sh, ipiv_array == nullptr);
     store_rows<T, NC>(a, A, n, n, lda, tid, pos);
@@ -83,7 +88,7 @@ __device__ __forceinline__ void gesv_small_instance(int id, const LuSizes& sz, T
         T b[R];
 #pragma unroll
         for (int r = 0; r < R; ++r)
-            b[r] = (tid < n && c0 + r < nrhs) ? B[tid + (size_t)(c0 + r) * ldb] : T(0);
+            b[r] = (c0 == 0) ? b0[r] : (tid < n && c0 + r < nrhs) ? B[tid + (size_t)(c0 + r) * ldb] : T(0);
         small_lu_solve<T, NC, NW, R>(a, n, pos, b, sh);
         if (tid < n) {
 #pragma unroll
