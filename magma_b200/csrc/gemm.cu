@@ -585,6 +585,114 @@ static magma_int_t gemm_launch_tc(bool TA, bool TB, const GemmSizes& g, T alpha,
     }
 }
 
+// NN form of the FP64 tensor-core tile fed by the cp.async pipeline of gemm_async_kernel:
+// three K chunks of 16 in flight (element-sized copies, zero-filled past the edges) into
+// rows padded to 68 doubles, the same fragments, k-steps and epilogue as gemm_dmma_kernel,
+// so the same bits.
+struct GemmDmmaAsyncSmem {
+    double a[3][16][68];
+    double b[3][16][68];
+};
+
+__global__ void __launch_bounds__(256, 2)
+gemm_dmma_async_kernel(GemmSizes g, double alpha, const double* const* __restrict__ A_arr,
+                       const double* const* __restrict__ B_arr, double beta, double** __restrict__ C_arr,
+                       int tiles_m, int tiles_n, WorkList wl) {
+    constexpr int BM = 64, BN = 64, BK = 16, NT = 256, ST = 3;
+    constexpr int EA = BM * BK / NT, EB = BK * BN / NT;
+    extern __shared__ __align__(16) unsigned char gemm_dmma_async_raw[];
+    GemmDmmaAsyncSmem& sm = *reinterpret_cast<GemmDmmaAsyncSmem*>(gemm_dmma_async_raw);
+    const int tiles = tiles_m * tiles_n;
+    const int w = blockIdx.x / tiles;
+    if (w >= wl.size()) return;
+    const int id = wl.at(w);
+    const int t = blockIdx.x - w * tiles;
+    const int i0 = (t / tiles_n) * BM, j0 = (t % tiles_n) * BN;
+    const int m = g.M(id), n = g.N(id), k = g.K(id);
+    if (i0 >= m || j0 >= n) return;
+    if ((g.tri == 1 && j0 > i0 + BM - 1) || (g.tri == 2 && i0 > j0 + BN - 1)) return;
+    const int lda = g.LDA(id), ldb = g.LDB(id), ldc = g.LDC(id);
+    const double* A = A_arr[id];
+    const double* B = B_arr[id];
+    double* C = C_arr[id];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;   // warp's sub-tile
+    const int q = lane & 3, r8 = lane >> 2;
+    double acc[4][2][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    auto issue = [&](int chunk) {
+        const int st = chunk % ST, k0 = chunk * BK;
+#pragma unroll
+        for (int e = 0; e < EA; ++e) {   // A (M x K, column-major): rows fastest, contiguous
+            const int idx = tid + e * NT, r = idx % BM, c = idx / BM;
+            const bool v = (i0 + r < m) && (k0 + c < k);
+            cp_async_elem(&sm.a[st][c][r], v ? A + (i0 + r) + (size_t)(k0 + c) * lda : A, v, 8);
+        }
+#pragma unroll
+        for (int e = 0; e < EB; ++e) {   // B (K x N, column-major): k fastest, contiguous
+            const int idx = tid + e * NT, c = idx % BK, j = idx / BK;
+            const bool v = (k0 + c < k) && (j0 + j < n);
+            cp_async_elem(&sm.b[st][c][j], v ? B + (k0 + c) + (size_t)(j0 + j) * ldb : B, v, 8);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    const int nchunks = (k + BK - 1) / BK;
+    if (nchunks > 0) issue(0);
+    if (nchunks > 1) issue(1); else asm volatile("cp.async.commit_group;" ::: "memory");
+    for (int c = 0; c < nchunks; ++c) {
+        asm volatile("cp.async.wait_group 1;" ::: "memory");   // chunk c has landed (c+1 may be in flight)
+        __syncthreads();                                         // ... for every thread; stage (c+2)%3 is free
+        if (c + 2 < nchunks) issue(c + 2); else asm volatile("cp.async.commit_group;" ::: "memory");
+        const int st = c % ST;
+#pragma unroll
+        for (int s4 = 0; s4 < BK / 4; ++s4) {
+            double af[4], bf[2];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) af[i] = sm.a[st][4 * s4 + q][wm + 8 * i + r8];
+#pragma unroll
+            for (int j = 0; j < 2; ++j) bf[j] = sm.b[st][4 * s4 + q][wn + 8 * j + r8];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) gemm_dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+        }
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    // every read of C before the first write (as gemm_tile_epilogue)
+    double cv[4][2][2];
+    bool in[4][2][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int gi = i0 + wm + 8 * i + r8;
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int gj = j0 + wn + 8 * j + 2 * q + h;
+                in[i][j][h] = gi < m && gj < n && !(g.tri == 1 && gj > gi) && !(g.tri == 2 && gi > gj);
+                cv[i][j][h] = (in[i][j][h] && beta != 0.0) ? C[gi + (size_t)gj * ldc] : 0.0;
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int gi = i0 + wm + 8 * i + r8;
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int gj = j0 + wn + 8 * j + 2 * q + h;
+                if (in[i][j][h])
+                    C[gi + (size_t)gj * ldc] =
+                        (beta == 0.0) ? alpha * acc[i][j][h] : alpha * acc[i][j][h] + beta * cv[i][j][h];
+            }
+        }
+    }
+}
+
 template <typename T>
 static magma_int_t gemm_launch_dmma(bool TA, bool TB, const GemmSizes& g, T alpha, const T* const* A,
                                     const T* const* B, T beta, T** C, const WorkList& wl, int bound, int max_m,
@@ -596,7 +704,11 @@ static magma_int_t gemm_launch_dmma(bool TA, bool TB, const GemmSizes& g, T alph
         const long blocks = (long)bound * tiles_m * tiles_n;
         if (blocks > 0x7fffffffL) return MAGMA_ERR_NOT_SUPPORTED;
         const dim3 grid((unsigned)blocks);
-        if (!TA && !TB) gemm_dmma_kernel<false, false><<<grid, 256, 0, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n, wl);
+        if (!TA && !TB) {   // NN: the cp.async-fed form
+            const int smem = (int)sizeof(GemmDmmaAsyncSmem);
+            ensure_dynamic_smem((const void*)gemm_dmma_async_kernel, smem);
+            gemm_dmma_async_kernel<<<grid, 256, smem, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n, wl);
+        }
         else if (!TA && TB) gemm_dmma_kernel<false, true><<<grid, 256, 0, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n, wl);
         else if (TA && !TB) gemm_dmma_kernel<true, false><<<grid, 256, 0, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n, wl);
         else gemm_dmma_kernel<true, true><<<grid, 256, 0, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n, wl);
