@@ -553,7 +553,7 @@ class C2GemmVbatched:
                 "alpha": 1.0, "beta": 0.5, "gflop_per_step": self.flops / 1e9}
 
     def launches_per_step(self):
-        return 1
+        return 1 + 4   # bucketize by max(M, N), then one launch per size bucket (four below 128)
 
     def _call(self, q, tag):
         b = self.bufs[tag]
