@@ -605,16 +605,22 @@ static magma_int_t gemm_launch_tc(bool TA, bool TB, const GemmSizes& g, T alpha,
 // three K chunks of 16 in flight (element-sized copies, zero-filled past the edges) into
 // rows padded to 68 doubles, the same fragments, k-steps and epilogue as gemm_dmma_kernel,
 // so the same bits.
+#ifndef MB200_DMMA_WARP_N
+#define MB200_DMMA_WARP_N 32
+#endif
+constexpr int kDmmaWarpN = MB200_DMMA_WARP_N;
 struct GemmDmmaAsyncSmem {
     double a[3][16][68];
     double b[3][16][68];
 };
 
-__global__ void __launch_bounds__(256, 2)
+// WN: each warp's tile is 32 x WN (4 x WN/8 tiles of 8x8); 64 x 64 / (32 WN) warps.
+template <int WN>
+__global__ void __launch_bounds__(64 * 64 / (32 * WN) * 32, (WN == 16 ? 2 : 3))
 gemm_dmma_async_kernel(GemmSizes g, double alpha, const double* const* __restrict__ A_arr,
                        const double* const* __restrict__ B_arr, double beta, double** __restrict__ C_arr,
                        int tiles_m, int tiles_n, WorkList wl) {
-    constexpr int BM = 64, BN = 64, BK = 16, NT = 256, ST = 3;
+    constexpr int BM = 64, BN = 64, BK = 16, NT = 64 * 64 / (32 * WN) * 32, ST = 3, TJ = WN / 8;
     constexpr int EA = BM * BK / NT, EB = BK * BN / NT;
     extern __shared__ __align__(16) unsigned char gemm_dmma_async_raw[];
     GemmDmmaAsyncSmem& sm = *reinterpret_cast<GemmDmmaAsyncSmem*>(gemm_dmma_async_raw);
@@ -632,13 +638,13 @@ gemm_dmma_async_kernel(GemmSizes g, double alpha, const double* const* __restric
     const double* B = B_arr[id];
     double* C = C_arr[id];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;   // warp's sub-tile
+    const int wm = (warp & 1) * 32, wn = (warp >> 1) * WN;   // warp's sub-tile
     const int q = lane & 3, r8 = lane >> 2;
-    double acc[4][2][2];
+    double acc[4][TJ][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+        for (int j = 0; j < TJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
     auto issue = [&](int chunk) {
         const int st = chunk % ST, k0 = chunk * BK;
 #pragma unroll
@@ -665,26 +671,26 @@ gemm_dmma_async_kernel(GemmSizes g, double alpha, const double* const* __restric
         const int st = c % ST;
 #pragma unroll
         for (int s4 = 0; s4 < BK / 4; ++s4) {
-            double af[4], bf[2];
+            double af[4], bf[TJ];
 #pragma unroll
             for (int i = 0; i < 4; ++i) af[i] = sm.a[st][4 * s4 + q][wm + 8 * i + r8];
 #pragma unroll
-            for (int j = 0; j < 2; ++j) bf[j] = sm.b[st][4 * s4 + q][wn + 8 * j + r8];
+            for (int j = 0; j < TJ; ++j) bf[j] = sm.b[st][4 * s4 + q][wn + 8 * j + r8];
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int j = 0; j < 2; ++j) gemm_dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+                for (int j = 0; j < TJ; ++j) gemm_dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
         }
     }
     asm volatile("cp.async.wait_group 0;" ::: "memory");
     // every read of C before the first write (as gemm_tile_epilogue)
-    double cv[4][2][2];
-    bool in[4][2][2];
+    double cv[4][TJ][2];
+    bool in[4][TJ][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const int gi = i0 + wm + 8 * i + r8;
 #pragma unroll
-        for (int j = 0; j < 2; ++j) {
+        for (int j = 0; j < TJ; ++j) {
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int gj = j0 + wn + 8 * j + 2 * q + h;
@@ -697,7 +703,7 @@ gemm_dmma_async_kernel(GemmSizes g, double alpha, const double* const* __restric
     for (int i = 0; i < 4; ++i) {
         const int gi = i0 + wm + 8 * i + r8;
 #pragma unroll
-        for (int j = 0; j < 2; ++j) {
+        for (int j = 0; j < TJ; ++j) {
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int gj = j0 + wn + 8 * j + 2 * q + h;
@@ -721,9 +727,11 @@ static magma_int_t gemm_launch_dmma(bool TA, bool TB, const GemmSizes& g, T alph
         if (blocks > 0x7fffffffL) return MAGMA_ERR_NOT_SUPPORTED;
         const dim3 grid((unsigned)blocks);
         if (!TA && !TB) {   // NN: the cp.async-fed form
+            constexpr int WN = kDmmaWarpN;
+            auto kern = gemm_dmma_async_kernel<WN>;
             const int smem = (int)sizeof(GemmDmmaAsyncSmem);
-            ensure_dynamic_smem((const void*)gemm_dmma_async_kernel, smem);
-            gemm_dmma_async_kernel<<<grid, 256, smem, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n, wl);
+            ensure_dynamic_smem((const void*)kern, smem);
+            kern<<<grid, 64 * 64 / (32 * WN) * 32, smem, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n, wl);
         }
         else if (!TA && TB) gemm_dmma_kernel<false, true><<<grid, 256, 0, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n, wl);
         else if (TA && !TB) gemm_dmma_kernel<true, false><<<grid, 256, 0, s>>>(g, alpha, A, B, beta, C, tiles_m, tiles_n, wl);
