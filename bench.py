@@ -604,7 +604,7 @@ class C2GemmVbatched:
 
     def dominant_kernel(self, q, stream, reps=20):
         ms = timed_restore(stream, lambda i: self.step(q, i), self.restore, reps) / reps
-        return {"kernel": "gemm_dmma_kernel (magmablas_dgemm_vbatched_max_nocheck: the FP64 tensor-core tile for "
+        return {"kernel": "gemm_dmma_async_kernel (magmablas_dgemm_vbatched_max_nocheck: the FP64 tensor-core tile for "
                           "max(M,N) > 32, CUDA-core tiles below)", "ms": ms,
                 "alg_bytes": self.bytes64, "tflops": self.flops / ms / 1e9}
 
