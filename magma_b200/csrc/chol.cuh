@@ -279,7 +279,95 @@ struct BlockedCholShared {
     T P[NT][NB + 1];     // panel entries of every row
 };
 
-template <typename T, int NB, int NT, int CW, int CB, typename Team = BlockTeam>
+// One FP64 tensor-core step D = A B + D on an 8x8 tile (mma.sync m8n8k4: lane l holds
+// A(l/4, l%4), B(l%4, l/4) and D(l/4, 2(l%4) .. +1)); each element of D receives its four
+// products as fma's in ascending k, rounded after each (the unblocked order).
+__device__ __forceinline__ void chol_dmma(double& d0, double& d1, double a, double b) {
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+        : "+d"(d0), "+d"(d1)
+        : "d"(a), "d"(b));
+}
+
+// Trailing update of one panel on the FP64 tensor cores: A22 -= P P^T on the lower
+// triangle from row/column m0 on, in jobs of 32 rows x 8 columns per warp (four 8x8
+// accumulator tiles, so four independent MMA chains). The multipliers come from the
+// panel rows in shared memory (A fragment negated: (-l_i) l_j + a is the fma of the
+// CUDA-core update), steps past the panel's nbp are zero, and each element receives its
+// nbp updates in ascending order, exactly as in the CUDA-core update. The next job's
+// entries are loaded before the current job's products.
+template <int NB, int NT, int CW, typename Team>
+__device__ __forceinline__ void chol_update_dmma(double* __restrict__ A, int n, int lda, bool upper, int m0,
+                                                 int nbp, const BlockedCholShared<double, NB, NT, CW>& sh,
+                                                 const Team& team) {
+    constexpr int NW = NT / 32;
+    const int tid = team.tid(), lane = tid & 31, warp = tid >> 5;
+    const int q = lane & 3, r8 = lane >> 2;
+    const int T8 = (n - m0 + 7) / 8;   // 8-column tiles of the trailing triangle
+    // element (i, j) of the stored triangle at A + i * si + j * sj (lower: A(i, j); upper: A(j, i))
+    const size_t si = upper ? (size_t)lda : 1, sj = upper ? 1 : (size_t)lda;
+    auto load_c = [&](int bj, int rb, double (&c)[4][2]) {
+        const int j0 = m0 + 8 * bj, ib = j0 + 32 * rb;
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+            const int i = ib + 8 * g + r8;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int j = j0 + 2 * q + h;
+                c[g][h] = (i < n && j <= i) ? A[i * si + j * sj] : 0.0;
+            }
+        }
+    };
+    int job = 0;
+    double cn[4][2];
+    // the warp's jobs in order: (bj, rb) with rb < ceil((T8 - bj) / 4), every NW-th job
+    auto next_job = [&](int& bj, int& rb) {
+        while (bj < T8) {
+            const int nrb = (T8 - bj + 3) / 4;
+            while (rb < nrb) {
+                if (job++ % NW == warp) return true;
+                ++rb;
+            }
+            ++bj;
+            rb = 0;
+        }
+        return false;
+    };
+    int bj = 0, rb = 0;
+    bool have = next_job(bj, rb);
+    if (have) load_c(bj, rb, cn);
+    while (have) {
+        double cc[4][2];
+#pragma unroll
+        for (int g = 0; g < 4; ++g) { cc[g][0] = cn[g][0]; cc[g][1] = cn[g][1]; }
+        const int cbj = bj, crb = rb;
+        ++rb;
+        have = next_job(bj, rb);
+        if (have) load_c(bj, rb, cn);   // in flight while the current job computes
+        const int j0 = m0 + 8 * cbj, ib = j0 + 32 * crb;
+#pragma unroll
+        for (int s4 = 0; s4 < NB / 4; ++s4) {
+            const int kk = 4 * s4 + q;
+            const bool kv = kk < nbp;
+            const double b = kv ? sh.P[min(j0 + r8, NT - 1)][kk] : 0.0;
+            double af[4];
+#pragma unroll
+            for (int g = 0; g < 4; ++g) af[g] = kv ? -sh.P[min(ib + 8 * g + r8, NT - 1)][kk] : 0.0;
+#pragma unroll
+            for (int g = 0; g < 4; ++g) chol_dmma(cc[g][0], cc[g][1], af[g], b);
+        }
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+            const int i = ib + 8 * g + r8;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int j = j0 + 2 * q + h;
+                if (i < n && j <= i) A[i * si + j * sj] = cc[g][h];
+            }
+        }
+    }
+}
+
+template <typename T, int NB, int NT, int CW, int CB, typename Team = BlockTeam, bool DMMA = false>
 __device__ int blocked_potrf(T* __restrict__ A, int n, int lda, bool upper, BlockedCholShared<T, NB, NT, CW>& sh,
                              const Team& team = Team{}) {
     constexpr int NW = NT / 32;
@@ -307,6 +395,11 @@ __device__ int blocked_potrf(T* __restrict__ A, int n, int lda, bool upper, Bloc
         // trailing lower triangle: rows/columns m0..n-1, square 8x8 blocks (bj <= bi),
         // each split into G work items of TR rows
         const int m0 = k0 + nbp;
+        if constexpr (DMMA && std::is_same<T, double>::value) {
+            chol_update_dmma<NB, NT, CW>(A, n, lda, upper, m0, nbp, sh, team);
+            team.sync();   // trailing entries visible before the next panel loads them
+            continue;
+        }
         const int T8 = (n - m0 + 7) / 8;
         const int items = G * T8 * (T8 + 1) / 2;
         for (int w = tid; w < items; w += NT) {
