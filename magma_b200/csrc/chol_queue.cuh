@@ -78,9 +78,10 @@ __device__ __forceinline__ void queue_blocked(int id, const LuSizes& sz, bool up
     const int n = sz.get_n(id), lda = sz.get_lda(id);
     if constexpr (FACTOR) {
         auto& sh = *reinterpret_cast<BlockedCholShared<T, 32, S, 64>*>(base);
-        // FP64 and 512 threads: the trailing updates on the tensor cores (the same bits as
-        // the CUDA-core form, which the smaller teams keep)
-        constexpr bool kDmma = std::is_same<T, double>::value && S == 512;
+        // FP64 teams of 256 and 512 threads: the trailing updates on the tensor cores (the same
+        // bits as the CUDA-core form, which the smaller teams keep: with them as well the
+        // kernel spills heavily under its 128 registers)
+        constexpr bool kDmma = std::is_same<T, double>::value && S >= 256;
         const int inf = blocked_potrf<T, 32, S, 64, 8, WarpRangeTeam, kDmma>(dA[id], n, lda, upper, sh, team);
         if (team.tid() == 0 && info) info[id] = inf;
         team.sync();   // the solve's shared memory overlays the factor's
