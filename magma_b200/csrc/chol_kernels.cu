@@ -49,7 +49,9 @@ potrf_blocked_kernel(WorkList wl, LuSizes sz, bool upper, T** dA_array, int* inf
         const int id = wl.at(w);
         const int n = sz.get_n(id), lda = sz.get_lda(id);
         int info = 0;
-        if (n > 0) info = blocked_potrf<T, NB, NT, CW, CB>(dA_array[id], n, lda, upper, sh);
+        // FP64: the trailing updates on the tensor cores (the same bits as the CUDA-core form)
+        if (n > 0) info = blocked_potrf<T, NB, NT, CW, CB, BlockTeam, std::is_same<T, double>::value>(
+                       dA_array[id], n, lda, upper, sh);
         if (threadIdx.x == 0 && info_array) info_array[id] = info;
         __syncthreads();
     }
