@@ -1,6 +1,7 @@
 """GPU parity tests of the one-launch variable-size LU (the persistent queue kernel).
 
-With the tuning switch on (the default), magma_dgetrf_vbatched and magma_dgesv_vbatched
+With the tuning switch on (it is off by default: the per-bucket launches measured
+faster on the size mix tried), magma_dgetrf_vbatched and magma_dgesv_vbatched
 run every instance with max(m, n) <= 512 from one device queue in a single launch; with
 it off, one launch per size bucket. Both must give the oracle's bits: factors, pivots,
 info and NoTrans solutions, for square and rectangular instances in every size class,
