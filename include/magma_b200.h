@@ -242,7 +242,7 @@ magma_int_t magma_dgesv_rbt_batched(magma_int_t n, magma_int_t nrhs, double** dA
 /* Householder QR: src/zgeqrf_batched.cpp:89-119 (info_array zeroed first; m -1, n -2,
  * ldda -4). LAPACK's representation: R on and above the diagonal, the reflectors'
  * vectors below it (unit leading entry implied), tau_i (min(m,n) entries) per
- * instance. m <= 256, n <= 64 (MAGMA_ERR_NOT_SUPPORTED otherwise). */
+ * instance. m <= 1024 (MAGMA_ERR_NOT_SUPPORTED otherwise), any n. */
 magma_int_t magma_dgeqrf_batched(magma_int_t m, magma_int_t n, double** dA_array, magma_int_t ldda,
                                  double** dtau_array, magma_int_t* info_array, magma_int_t batchCount,
                                  magma_queue_t queue);

@@ -3,12 +3,12 @@
 // LAPACK dgeqr2 order: for each column k, dlarfg on A(k:m, k), then dlarf on the
 // trailing columns. One thread block per matrix; P consecutive lanes per column
 // (P = 1, 2, 4, 8 for m <= 16, 32, 64, 128; P = 8 with 32 rows a lane for m <= 256,
-// with 64 rows a lane for m <= 512);
+// with 64 rows a lane for m <= 512; P = 16 with 64 rows a lane for m <= 1024);
 // lane p of column j holds rows r = i*P + p (i < S) in registers, so a warp's
 // load or store of element i touches P consecutive rows of each of its columns
 // (sector-coalesced without staging). Rows >= m are zero.
 //
-// More columns than a panel holds (64; 32 for m > 256): the columns are processed in panels (one panel's
+// More columns than a panel holds (64; 32 for m > 256, 16 for m > 512): the columns are processed in panels (one panel's
 // columns in registers); a panel first replays, in order, the reflectors the
 // earlier panels formed (read back from A and tau), then forms its own. Every
 // column receives the same operations in the same order either way.
@@ -172,12 +172,16 @@ geqrf_lanes_kernel(int m, int n, double** dA_array, int lda, double** dtau_array
 template <int S, int P>
 static void launch_geqrf(int m, int n, double** A, int lda, double** tau, int batch, cudaStream_t s) {
     const int grid = std::min(batch, 65535);
-    if (n <= 16 && P * 16 >= 32 && S <= 32) geqrf_lanes_kernel<S, P, 16><<<grid, P * 16, 0, s>>>(m, n, A, lda, tau, batch);
-    else if (n <= 32 || S > 32) geqrf_lanes_kernel<S, P, 32><<<grid, P * 32, 0, s>>>(m, n, A, lda, tau, batch);
-    else geqrf_lanes_kernel<S, P, 64><<<grid, P * 64, 0, s>>>(m, n, A, lda, tau, batch);
+    if constexpr (P == 16) {   // 256 threads
+        geqrf_lanes_kernel<S, P, 16><<<grid, P * 16, 0, s>>>(m, n, A, lda, tau, batch);
+    } else {
+        if (n <= 16 && P * 16 >= 32 && S <= 32) geqrf_lanes_kernel<S, P, 16><<<grid, P * 16, 0, s>>>(m, n, A, lda, tau, batch);
+        else if (n <= 32 || S > 32) geqrf_lanes_kernel<S, P, 32><<<grid, P * 32, 0, s>>>(m, n, A, lda, tau, batch);
+        else geqrf_lanes_kernel<S, P, 64><<<grid, P * 64, 0, s>>>(m, n, A, lda, tau, batch);
+    }
 }
 
-bool geqrf_supported(int m, int n) { return m <= 512 && n >= 0; }
+bool geqrf_supported(int m, int n) { return m <= 1024 && n >= 0; }
 
 magma_int_t geqrf_small(int m, int n, double** A, int lda, double** tau, int batch, cudaStream_t s) {
     if (!geqrf_supported(m, n)) return MAGMA_ERR_NOT_SUPPORTED;
@@ -186,7 +190,8 @@ magma_int_t geqrf_small(int m, int n, double** A, int lda, double** tau, int bat
     else if (m <= 64) launch_geqrf<16, 4>(m, n, A, lda, tau, batch, s);
     else if (m <= 128) launch_geqrf<16, 8>(m, n, A, lda, tau, batch, s);
     else if (m <= 256) launch_geqrf<32, 8>(m, n, A, lda, tau, batch, s);
-    else launch_geqrf<64, 8>(m, n, A, lda, tau, batch, s);   // panels of 32 columns, 64 rows a lane
+    else if (m <= 512) launch_geqrf<64, 8>(m, n, A, lda, tau, batch, s);   // panels of 32 columns, 64 rows a lane
+    else launch_geqrf<64, 16>(m, n, A, lda, tau, batch, s);                // panels of 16 columns, 64 rows a lane
     return launch_status();
 }
 
@@ -197,7 +202,7 @@ using namespace mb200;
 extern "C" {
 
 // src/zgeqrf_batched.cpp:89-119: info_array zeroed first; m -1, n -2, ldda < max(1,m) -4;
-// quick return when m or n is 0. m <= 512 (MAGMA_ERR_NOT_SUPPORTED otherwise), any n.
+// quick return when m or n is 0. m <= 1024 (MAGMA_ERR_NOT_SUPPORTED otherwise), any n.
 magma_int_t magma_dgeqrf_batched(magma_int_t m, magma_int_t n, double** dA_array, magma_int_t ldda,
                                  double** dtau_array, magma_int_t* info_array, magma_int_t batchCount,
                                  magma_queue_t queue) {

@@ -97,7 +97,7 @@ void oracle_dgetrf_nopiv_batched(int m, int n, double* A, int lda, long strideA,
  * instance at a time (testing/testing_zgeqrf_batched.cpp:224).
  * LAPACK 3.x dgeqr2 (Householder QR: dlarfg, then dlarf on the trailing columns), with
  * the summation order of the batched path written out: the rows of a column are dealt
- * to P lanes (row r to lane r mod P, P = 1, 2, 4, 8 for m <= 16, 32, 64, 256); each
+ * to P lanes (row r to lane r mod P, P = 1, 2, 4, 8, 16 for m <= 16, 32, 64, 512, 1024); each
  * lane sums its rows in ascending order with fma, and the P partial sums are added as
  * a pairwise tree ((x0+x1)+(x2+x3))+... . For column k:
  *   xs = ||A(k+1:m, k)||^2 in that order, beta = -sign(alpha) sqrt(fma(alpha, alpha, xs)),
@@ -107,7 +107,7 @@ void oracle_dgetrf_nopiv_batched(int m, int n, double* A, int lda, long strideA,
  *   A(r,j) = fma(t_r, w, A(r,j)) for all m rows (rows above k change by an exact zero).
  * Against LAPACK this differs by rounding only (and the sign of exact zeros); dnrm2's
  * scaling and dlapy2's guard are omitted (entries far inside [1e-150, 1e150]). */
-static int qr_lanes(int m) { return m <= 16 ? 1 : m <= 32 ? 2 : m <= 64 ? 4 : 8; }
+static int qr_lanes(int m) { return m <= 16 ? 1 : m <= 32 ? 2 : m <= 64 ? 4 : m <= 512 ? 8 : 16; }
 
 static double tree_sum(double* x, int P) {
     for (int h = 1; h < P; h *= 2)

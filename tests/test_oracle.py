@@ -141,7 +141,8 @@ def test_oracle_cholesky_upper_is_transpose():
     assert np.array_equal(np.tril(lo[0].T), np.triu(up[0].T).T)
 
 
-@pytest.mark.parametrize("m,n", [(1, 1), (8, 8), (40, 17), (64, 64), (200, 50), (10, 30), (16, 33), (33, 40), (256, 64)])
+@pytest.mark.parametrize("m,n", [(1, 1), (8, 8), (40, 17), (64, 64), (200, 50), (10, 30), (16, 33), (33, 40), (256, 64),
+                                 (700, 20), (1024, 9)])
 def test_oracle_geqr2_matches_lapack(m, n):
     """The restated dgeqr2 agrees with LAPACK dgeqrf (numpy's qr, mode 'raw') to rounding:
     same reflectors, same signs of R's diagonal, same tau."""

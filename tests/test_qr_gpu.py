@@ -51,7 +51,10 @@ def qr_errors(A0, h, tau, m, n):
                                            (100, 256, 3, 101), (30, 200, 4, 30), (256, 300, 2, 260),
                                            (200, 129, 4, 200),
                                            # 257..512 rows: 64 rows a lane, panels of 32 columns
-                                           (300, 40, 3, 300), (512, 70, 2, 512), (400, 400, 2, 401), (257, 3, 4, 257)])
+                                           (300, 40, 3, 300), (512, 70, 2, 512), (400, 400, 2, 401), (257, 3, 4, 257),
+                                           # 513..1024 rows: 16 lanes a column, 64 rows a lane, panels of 16 columns
+                                           (513, 5, 3, 513), (700, 40, 2, 703), (1024, 33, 2, 1024),
+                                           (600, 600, 1, 600), (1000, 1100, 1, 1001)])
 def test_geqrf_matches_oracle(cuda, m, n, batch, lda):
     import magma_b200 as mb
     rng = np.random.default_rng(1000 * m + n)
@@ -116,6 +119,6 @@ def test_geqrf_argument_errors(cuda):
     torch.cuda.synchronize()
     assert info.cpu().tolist() == [0, 0]                            # zeroed before the checks
     assert f(8, 0, vp(pA), 8, vp(pT), vp(info), 2, q.handle) == 0  # quick return
-    # more than 512 rows is refused before any work (the arrays here are far too small for
+    # more than 1024 rows is refused before any work (the arrays here are far too small for
     # such a matrix, and nothing reads them)
-    assert f(513, 4, vp(pA), 513, vp(pT), vp(info), 2, q.handle) == _lib.MAGMA_ERR_NOT_SUPPORTED
+    assert f(1025, 4, vp(pA), 1025, vp(pT), vp(info), 2, q.handle) == _lib.MAGMA_ERR_NOT_SUPPORTED
