@@ -293,9 +293,11 @@ __device__ __forceinline__ void chol_dmma(double& d0, double& d1, double a, doub
 // accumulator tiles, so four independent MMA chains). The multipliers come from the
 // panel rows in shared memory (A fragment negated: (-l_i) l_j + a is the fma of the
 // CUDA-core update), steps past the panel's nbp are zero, and each element receives its
-// nbp updates in ascending order, exactly as in the CUDA-core update. The next job's
-// entries are loaded before the current job's products.
-template <int NB, int NT, int CW, typename Team>
+// nbp updates in ascending order, exactly as in the CUDA-core update. With PREFETCH the
+// next job's entries are loaded before the current job's products (16 more registers a
+// thread; the persistent queue kernel, whose every path shares one 128-register budget,
+// spills with it and loads each job's entries in turn instead).
+template <int NB, int NT, int CW, bool PREFETCH, typename Team>
 __device__ __forceinline__ void chol_update_dmma(double* __restrict__ A, int n, int lda, bool upper, int m0,
                                                  int nbp, const BlockedCholShared<double, NB, NT, CW>& sh,
                                                  const Team& team) {
@@ -334,15 +336,19 @@ __device__ __forceinline__ void chol_update_dmma(double* __restrict__ A, int n, 
     };
     int bj = 0, rb = 0;
     bool have = next_job(bj, rb);
-    if (have) load_c(bj, rb, cn);
+    if (PREFETCH && have) load_c(bj, rb, cn);
     while (have) {
         double cc[4][2];
+        if constexpr (PREFETCH) {
 #pragma unroll
-        for (int g = 0; g < 4; ++g) { cc[g][0] = cn[g][0]; cc[g][1] = cn[g][1]; }
+            for (int g = 0; g < 4; ++g) { cc[g][0] = cn[g][0]; cc[g][1] = cn[g][1]; }
+        } else {
+            load_c(bj, rb, cc);
+        }
         const int cbj = bj, crb = rb;
         ++rb;
         have = next_job(bj, rb);
-        if (have) load_c(bj, rb, cn);   // in flight while the current job computes
+        if (PREFETCH && have) load_c(bj, rb, cn);   // in flight while the current job computes
         const int j0 = m0 + 8 * cbj, ib = j0 + 32 * crb;
 #pragma unroll
         for (int s4 = 0; s4 < NB / 4; ++s4) {
@@ -367,7 +373,8 @@ __device__ __forceinline__ void chol_update_dmma(double* __restrict__ A, int n, 
     }
 }
 
-template <typename T, int NB, int NT, int CW, int CB, typename Team = BlockTeam, bool DMMA = false>
+template <typename T, int NB, int NT, int CW, int CB, typename Team = BlockTeam, bool DMMA = false,
+          bool PREFETCH = true>
 __device__ int blocked_potrf(T* __restrict__ A, int n, int lda, bool upper, BlockedCholShared<T, NB, NT, CW>& sh,
                              const Team& team = Team{}) {
     constexpr int NW = NT / 32;
@@ -396,7 +403,7 @@ __device__ int blocked_potrf(T* __restrict__ A, int n, int lda, bool upper, Bloc
         // each split into G work items of TR rows
         const int m0 = k0 + nbp;
         if constexpr (DMMA && std::is_same<T, double>::value) {
-            chol_update_dmma<NB, NT, CW>(A, n, lda, upper, m0, nbp, sh, team);
+            chol_update_dmma<NB, NT, CW, PREFETCH>(A, n, lda, upper, m0, nbp, sh, team);
             team.sync();   // trailing entries visible before the next panel loads them
             continue;
         }

@@ -82,7 +82,7 @@ __device__ __forceinline__ void queue_blocked(int id, const LuSizes& sz, bool up
         // bits as the CUDA-core form, which the smaller teams keep: with them as well the
         // kernel spills heavily under its 128 registers)
         constexpr bool kDmma = std::is_same<T, double>::value && S >= 256;
-        const int inf = blocked_potrf<T, 32, S, 64, 8, WarpRangeTeam, kDmma>(dA[id], n, lda, upper, sh, team);
+        const int inf = blocked_potrf<T, 32, S, 64, 8, WarpRangeTeam, kDmma, false>(dA[id], n, lda, upper, sh, team);
         if (team.tid() == 0 && info) info[id] = inf;
         team.sync();   // the solve's shared memory overlays the factor's
     }
